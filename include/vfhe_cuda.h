@@ -1,0 +1,335 @@
+/*
+ * vfhe_cuda.h -- C ABI of the B200 `cuda` engine for vfhe's RNS polynomial hot path.
+ *
+ * Part 1 is the drop-in surface: the functions and struct prefixes that vfhe's
+ * cffi layer binds for every engine.  Names, argument order and meaning follow the
+ * reference cdefs line by line:
+ *   modules/arith/python/cdef/arith.cdef   (cited as arith.cdef:<line>)
+ *   modules/misc/python/cdef/misc.cdef     (misc.cdef:<line>)
+ *   modules/misc/python/cdef/vfhe_cpu.cdef (vfhe_cpu.cdef:<line>)
+ *   modules/mlwe/python/cdef/mlwe.cdef     (mlwe.cdef:<line>)
+ *   modules/fhe/python/cdef/fhe.cdef       (fhe.cdef:<line>)
+ * Handles are `void *`; outputs are caller-allocated out-params, first.  Calls are
+ * synchronous: when a function returns, its results are readable from the host
+ * through the coefficient pointers (coefficient rows live in CUDA managed memory).
+ *
+ * Part 2 is new: a batched device API over plain device pointers and a CUDA
+ * stream, for callers that keep ciphertexts and keys resident in HBM.
+ *
+ * Errors: the reference aborts on contract violations.  This engine records the
+ * first error instead (vfhe_cuda_last_error) and returns; batched entry points
+ * also return a nonzero status.
+ *
+ * This header is also the cffi cdef source: keep it free of macros other than the
+ * include guard and the extern "C" block.
+ */
+#ifndef VFHE_CUDA_H
+#define VFHE_CUDA_H
+
+#include <stdbool.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ===================================================================== *
+ * Part 1: drop-in surface                                                *
+ * ===================================================================== */
+
+/* Opaque per-prime transform descriptor (arith.cdef:8; modules/arith/c/include/arith.h:29-46).
+ * Its first two fields are the transform size n and the prime q, as in the reference. */
+typedef struct _NTT_proc *NTT_proc;
+
+/* Pool of primes for one (N, split_degree) (arith.cdef:10-16; arith.h:48-54).
+ * w[i] holds the split-product twist row of prime i (N/split_degree values, host-readable). */
+typedef struct _incNTT {
+  NTT_proc *ntt;
+  uint64_t split_degree;
+  uint64_t **w;
+  uint64_t N;
+  uint64_t l;
+} *incNTT;
+
+/* RNS polynomial (arith.cdef:18-23; arith.h:72-78): one row of N residues per limb of
+ * the pool, rns_mask selects the active limbs.  Rows are host-dereferenceable. */
+typedef struct _RNS_Polynomial {
+  uint64_t **coeffs;
+  incNTT ntt;
+  uint64_t rns_mask;
+  uint64_t allocated_l;
+} *RNS_Polynomial;
+
+/* --- misc --- */
+void *safe_aligned_malloc(uint64_t size);                                            /* arith.cdef:26 */
+
+/* --- ntt / base conversion --- */
+void *new_incomplete_ntt_list(uint64_t *primes, uint64_t split_degree, uint64_t N, uint64_t count); /* arith.cdef:29 */
+void incNTT_extend_with_primes(void *ntt, uint64_t *new_primes, uint64_t count);   /* arith.cdef:30 */
+uint64_t **incNTT_get_rou_matrix(void *ntt);                                       /* arith.cdef:31 */
+void *init_base_conversion_params(void *ntt, uint64_t in_mask, uint64_t out_mask);  /* arith.cdef:32 */
+void free_base_conversion_params(void *params);                                    /* arith.cdef:33 */
+
+/* --- polynomial lifecycle / io --- */
+void *polynomial_new_RNS_polynomial(uint64_t N, uint64_t rns_mask, void *ntt);      /* arith.cdef:36 */
+void polynomial_copy_RNS_polynomial(void *out, void *in);                          /* arith.cdef:37 */
+void free_RNS_polynomial(void *p);                                                 /* arith.cdef:38 */
+void int_array_to_RNS(void *out, uint64_t *in);                                    /* arith.cdef:39 */
+void array_to_RNS(void *out, uint64_t **in);                                       /* arith.cdef:40 */
+
+/* --- sampling (engine-specific random stream, as in the reference) --- */
+void polynomial_gen_random_RNSc_polynomial(void *out);                             /* arith.cdef:43 */
+void polynomial_gen_gaussian_RNSc_polynomial(void *out, double sigma);             /* arith.cdef:44 */
+
+/* --- arithmetic --- */
+void polynomial_mul_RNS_polynomial(void *out, void *in1, void *in2);               /* arith.cdef:47 */
+void polynomial_multo_RNS_polynomial(void *out, void *in);                         /* arith.cdef:48 */
+void polynomial_sub_RNS_polynomial(void *out, void *in1, void *in2);               /* arith.cdef:49 */
+void polynomial_sub_RNSc_polynomial(void *out, void *in1, void *in2);              /* arith.cdef:50 */
+void polynomial_add_RNSc_polynomial(void *out, void *in1, void *in2);              /* arith.cdef:51 */
+void polynomial_add_RNS_polynomial(void *out, void *in1, void *in2);               /* arith.cdef:52 */
+void polynomial_scale_RNSc_polynomial(void *out, void *in1, uint64_t scale);       /* arith.cdef:53 */
+void polynomial_scale_RNS_polynomial_RNS(void *out, void *in1, uint64_t *scale);   /* arith.cdef:54 */
+void polynomial_RNSc_negate(void *out, void *in);                                  /* arith.cdef:55 */
+void polynomial_RNSc_add_integer(void *out, void *in1, uint64_t in2);              /* arith.cdef:56 */
+void polynomial_RNS_add_integer(void *out, void *in1, uint64_t in2);               /* arith.cdef:57 */
+
+/* --- automorphism / domain conversion --- */
+void polynomial_RNSc_permute(void *out, void *in, uint64_t gen);                   /* arith.cdef:60 */
+void polynomial_RNSc_to_RNS(void *out, void *in);                                  /* arith.cdef:61 */
+void polynomial_RNS_to_RNSc(void *out, void *in);                                  /* arith.cdef:62 */
+
+/* --- tower --- */
+void polynomial_base_conversion_RNSc(void *out, void *in, void *params);           /* arith.cdef:65 */
+void polynomial_RNSc_mod_reduce(void *out, void *in);                              /* arith.cdef:66 */
+void polynomial_RNSc_mod_reduce_lifted(void *out, void *in, uint64_t idx);         /* arith.cdef:67 */
+void polynomial_round_division_RNSc_wo_free(void *out, uint64_t divide_mask);      /* arith.cdef:68 */
+void polynomial_floor_division_RNSc_wo_free(void *out, uint64_t divide_mask);      /* arith.cdef:69 */
+void polynomial_RNSc_scaled_lift(void *out, void *in, uint64_t *delta);            /* arith.cdef:70 */
+
+/* --- slots / inverse / eq --- */
+int polynomial_RNS_inverse(void *out, void *in);                                   /* arith.cdef:73 */
+bool polynomial_eq(void *a, void *b);                                              /* arith.cdef:74 */
+void polynomial_RNS_broadcast_slot(void *out, void *in, uint64_t slot_idx);        /* arith.cdef:75 */
+void polynomial_RNS_rotate_slot(void *out, void *in, uint64_t rot);                /* arith.cdef:76 */
+void polynomial_RNS_copy_slot(void *out, uint64_t dst, void *in, uint64_t src);    /* arith.cdef:77 */
+
+/* --- hashing: BLAKE3 is not part of this engine; these record an error --- */
+void polynomial_RNS_get_hash(uint64_t *out, void *p);                              /* arith.cdef:80 */
+uint64_t *polynomial_RNS_get_hash_p(void *p);                                      /* arith.cdef:81 */
+
+/* --- complex FFT (CKKS encoding) --- */
+void *load_rous_CT(double *rous_real, double *rous_imag, uint64_t size);           /* arith.cdef:84 */
+void *load_rous_GS(double *rous_real, double *rous_imag, uint64_t size);           /* arith.cdef:85 */
+void CT_NR(double *x, void *ws, uint64_t n);                                       /* arith.cdef:86 */
+void GS_RN(double *x, void *ws, uint64_t n);                                       /* arith.cdef:87 */
+void bit_reverse_array(double *v, uint64_t N, uint32_t prec);                      /* arith.cdef:88 */
+void complex_poly_scale_double(double *v, double scale, uint64_t N);               /* arith.cdef:89 */
+void complex_poly_round_to_RNS(void *out, double *in, uint64_t N);                 /* arith.cdef:90 */
+void complex_polys_ifft_scale_round_to_RNS_batch(void **rows_in, void **outs_rns, uint64_t count,
+                                                 uint64_t n_complex, uint32_t log_prec, void *gs_ws,
+                                                 double temp_delta);                /* arith.cdef:91-93 */
+
+/* --- multiprecision (outside the hot path; present so the surface links) --- */
+typedef struct _mp_vector mp_vector_t;                                             /* arith.cdef:101 */
+typedef struct _MPScalar { mp_vector_t *digits; uint64_t d; } *MPScalar;           /* arith.cdef:102 */
+typedef struct _MPPolynomial { uint64_t **coeffs; uint64_t N; uint64_t d; } *MPPolynomial; /* arith.cdef:103 */
+int get_mp_vector_size(void);                                                      /* arith.cdef:104 */
+void mp_scale(void *out, void *in, void *m);                                       /* arith.cdef:105 */
+void mp_sub(void *out, void *a, void *b);                                          /* arith.cdef:106 */
+void *mp_load(uint64_t *in, uint64_t d);                                           /* arith.cdef:107 */
+mp_vector_t *load_m512(uint64_t in);                                               /* arith.cdef:108 */
+void *new_mp_polynomial(uint64_t N, uint64_t d);                                   /* arith.cdef:109 */
+void mp_polynomial_from_RNS(void *out, void *in, MPScalar *PW, void *q, mp_vector_t *m, uint64_t k); /* arith.cdef:110 */
+void mp_polynomial_to_RNSc(void *out, void *in);                                   /* arith.cdef:111 */
+
+/* --- field extensions (outside the hot path; present so the surface links) --- */
+void *field_new_proc(uint64_t q);                                                  /* arith.cdef:114 */
+void field_ext_add(uint64_t *c, const uint64_t *a, const uint64_t *b, uint64_t d, uint64_t q); /* arith.cdef:115 */
+void field_ext_sub(uint64_t *c, const uint64_t *a, const uint64_t *b, uint64_t d, uint64_t q); /* arith.cdef:116 */
+void field_ext_neg(uint64_t *c, const uint64_t *a, uint64_t d, uint64_t q);        /* arith.cdef:117 */
+void field_ext_mul(uint64_t *c, const uint64_t *a, const uint64_t *b, uint64_t d, uint64_t w, void *proc); /* arith.cdef:118 */
+void field_ext_pow(uint64_t *res, const uint64_t *base, uint64_t exp_lo, uint64_t exp_hi, uint64_t d, uint64_t w, void *proc); /* arith.cdef:119 */
+int field_ext_inv(uint64_t *ainv, const uint64_t *a, uint64_t d, uint64_t w, void *proc); /* arith.cdef:120 */
+void field_sample_random_element(uint64_t *a, const uint8_t *seed, uint64_t seed_len, uint64_t d, uint64_t mod); /* arith.cdef:121 */
+void field_hash_element(uint8_t *out, const uint64_t *a, uint64_t d);              /* arith.cdef:122 */
+int field_ext_is_equal(const uint64_t *a, const uint64_t *b, uint64_t d);          /* arith.cdef:123 */
+void field_base_conversion(uint64_t *out, const uint64_t *in,
+                           uint64_t source_component, uint64_t target_component,
+                           uint64_t d, uint64_t poly_size, const uint64_t *w_i, void *proc); /* arith.cdef:124-126 */
+void ntt_free_proc(void *proc);                                                    /* arith.cdef:127 */
+uint64_t inverse_mod_eea(uint64_t a, uint64_t p);                                  /* arith.cdef:128 */
+
+/* --- misc.cdef / vfhe_cpu.cdef --- */
+const char *vfhe_engine_active(void);                                              /* misc.cdef:8 */
+void vfhe_prng_set_deterministic_seed(uint64_t seed);                              /* misc.cdef:12 */
+void vfhe_prng_clear_deterministic_seed(void);                                     /* misc.cdef:13 */
+int vfhe_cpu_supports(const char *capability);                                     /* vfhe_cpu.cdef:7 */
+/* misc.cdef:17 binds libc free(); safe_aligned_malloc above returns libc memory. */
+
+/* --- mlwe.cdef --- */
+typedef struct _IntPolynomial *IntPolynomial;                                      /* mlwe.cdef:9 */
+
+typedef struct _LWE_Key {                                                          /* mlwe.cdef:11-17 */
+  uint64_t **s;
+  uint64_t n;
+  uint64_t l;
+  incNTT ntt;
+  double sigma;
+} *LWE_Key;
+
+typedef struct _LWE {                                                              /* mlwe.cdef:19-25 */
+  uint64_t **a;
+  uint64_t *b;
+  uint64_t n;
+  uint64_t l;
+  incNTT ntt;
+} *LWE;
+
+typedef struct _RNS_MLWE {                                                         /* mlwe.cdef:27-31 */
+  RNS_Polynomial *a;
+  RNS_Polynomial b;
+  uint64_t r;
+} *RNS_MLWE;
+
+typedef struct _RNS_MLWE_Key {                                                     /* mlwe.cdef:33-40 */
+  IntPolynomial *s;
+  RNS_Polynomial *s_RNS;
+  uint64_t N;
+  uint64_t l;
+  uint64_t r;
+  double sigma;
+} *RNS_MLWE_Key;
+
+/* lwe */
+void *lwe_alloc_key(uint64_t n, uint64_t l, void *ntt);                            /* mlwe.cdef:43 */
+void *lwe_alloc_sample(uint64_t n, uint64_t l, void *ntt);                         /* mlwe.cdef:44 */
+void free_lwe_sample(void *c);                                                     /* mlwe.cdef:45 */
+void *lwe_new_key(uint64_t n, uint64_t l, void *ntt, double sec_sigma, double err_sigma); /* mlwe.cdef:46 */
+void *lwe_new_sparse_ternary_key(uint64_t n, uint64_t l, void *ntt, uint64_t h, double err_sigma); /* mlwe.cdef:47 */
+void lwe_sample(void *c, uint64_t *m, void *key);                                  /* mlwe.cdef:48 */
+void *lwe_new_sample(uint64_t *m, void *key);                                      /* mlwe.cdef:49 */
+void *lwe_new_trivial_sample(uint64_t *m, uint64_t n, uint64_t l, void *ntt);      /* mlwe.cdef:50 */
+void lwe_phase(uint64_t *out, void *c, void *key);                                 /* mlwe.cdef:51 */
+void lwe_subto(void *out, void *in);                                               /* mlwe.cdef:52 */
+
+/* mlwe (rns) */
+void *mlwe_new_RNS_key_from_array(uint64_t *array, uint64_t N, uint64_t r, uint64_t l, void *ntt, double sigma); /* mlwe.cdef:55 */
+void *mlwe_new_RNS_gaussian_key(uint64_t N, uint64_t r, uint64_t l, double key_sigma, void *ntt, double sigma);  /* mlwe.cdef:56 */
+void *mlwe_alloc_RNS_sample(uint64_t N, uint64_t r, uint64_t mask, void *ntt);     /* mlwe.cdef:57 */
+void *mlwe_alloc_RNS_sample_array(uint64_t size, uint64_t N, uint64_t r, uint64_t mask, void *ntt); /* mlwe.cdef:58 */
+void *mlwe_create_copy_array(void *in, uint64_t size);                             /* mlwe.cdef:59 */
+void free_mlwe_RNS_sample(void *p);                                                /* mlwe.cdef:60 */
+void free_mlwe_RNS_key(void *key);                                                 /* mlwe.cdef:61 */
+
+void mlwe_RNSc_sample(void *out, void *key, void *m);                              /* mlwe.cdef:63 */
+void mlwe_RNS_phase(void *out, void *in, void *key);                               /* mlwe.cdef:64 */
+void mlwe_RNSc_to_RNS(void *out, void *in);                                        /* mlwe.cdef:65 */
+void mlwe_RNS_to_RNSc(void *out, void *in);                                        /* mlwe.cdef:66 */
+void mlwe_copy_RNS_sample(void *out, void *in);                                    /* mlwe.cdef:67 */
+void mlwe_RNS_trivial_sample_of_zero(void *out);                                   /* mlwe.cdef:68 */
+void *mlwe_new_RNSc_sample_of_zero(void *key);                                     /* mlwe.cdef:69 */
+void *mlwe_new_RNS_sample_of_zero(void *key);                                      /* mlwe.cdef:70 */
+void *mlwe_new_RNS_trivial_sample_of_zero(uint64_t N, uint64_t r, uint64_t mask, void *ntt); /* mlwe.cdef:71 */
+
+void mlwe_RNS_mul_addto_by_poly(void *out, void *in, void *poly);                  /* mlwe.cdef:73 */
+void mlwe_RNS_mul_subto_by_poly(void *out, void *in, void *poly);                  /* mlwe.cdef:74 */
+void mlwe_RNS_mul_by_poly(void *out, void *in, void *poly);                        /* mlwe.cdef:75 */
+void mlwe_scale_RNS_mlwe_RNS(void *c, uint64_t *scale);                            /* mlwe.cdef:76 */
+void mlwe_add_RNSc_sample(void *out, void *in1, void *in2);                        /* mlwe.cdef:77 */
+void mlwe_sub_RNSc_sample(void *out, void *in1, void *in2);                        /* mlwe.cdef:78 */
+void mlwe_RNSc_mul_by_xai(void *out, void *in, uint64_t a);                        /* mlwe.cdef:79 */
+void mlwe_RNSc_mul_by_xai_minus1(void *out, void *in, uint64_t a);                 /* mlwe.cdef:80 */
+void mlwe_add_RNSc_polynomial(void *out, void *in1, void *in2);                    /* mlwe.cdef:81 */
+void mlwe_sub_RNSc_polynomial(void *out, void *in1, void *in2);                    /* mlwe.cdef:82 */
+void mlwe_RNS_add_polynomial(void *out, void *in1, void *in2);                     /* mlwe.cdef:83 */
+void mlwe_RNS_sub_polynomial(void *out, void *in1, void *in2);                     /* mlwe.cdef:84 */
+void mlwe_round_division_RNSc(void *out, uint64_t divide_mask);                    /* mlwe.cdef:85 */
+
+void *mlwe_extract_LWE(void *in, uint64_t idx);                                    /* mlwe.cdef:87 */
+void mlwe_full_packing_keyswitch(void *out, void *in, uint64_t size, void *ksk, uint64_t lvl); /* mlwe.cdef:88 */
+void mlwe_full_packing_keyswitch_scaled(void *vec, uint64_t ell, void *ksks, uint64_t lvl);    /* mlwe.cdef:89 */
+void mlwe_RNSc_GHS_hybrid_keyswitch(void *out, void *in, void *ksk, uint64_t lvl); /* mlwe.cdef:90 */
+void mlwe_automorphism_RNSc_GHS(void *out, void *in, uint64_t gen, void *ksk, uint64_t lvl); /* mlwe.cdef:91 */
+void mlwe_partial_trace(void *out, void *in, uint64_t *gens, void *ksks, uint64_t size, uint64_t lvl); /* mlwe.cdef:92 */
+void mlwe_trace(void *out, void *in, void *ksks, uint64_t lvl);                    /* mlwe.cdef:93 */
+uint64_t mlwe_extended_rank(uint64_t r);                                           /* mlwe.cdef:94 */
+void mlwe_tensor_product(void *out, void *in1, void *in2);                         /* mlwe.cdef:95 */
+void mlwe_multiply(void *out, void *in1, void *in2, void *ksk);                    /* mlwe.cdef:96 */
+
+/* mgsw */
+void mgsw_external_product(void *out, void *mgsw, void *in, uint64_t ell, uint64_t special_primes); /* mlwe.cdef:99 */
+void mgsw_CMUX(void *out, void *in1, void *in2, void *mgsw, uint64_t ell, uint64_t special_primes); /* mlwe.cdef:100 */
+void mgsw_NCMUX(void *out, void *in1, void *in2, void *mgsw, void *ksk, uint64_t ell, uint64_t special_primes); /* mlwe.cdef:101 */
+
+/* --- fhe.cdef: GP25 (outside the hot path; present so the surface links) --- */
+void gp25_RGSW_monomial_mul(void *p0, uint64_t in_N, void *e, uint64_t r_prec, void *ksk, uint64_t ell, uint64_t special_primes); /* fhe.cdef:8 */
+void gp25_RGSW_monomial_mul_mt(void *p0, uint64_t in_N, void *e, uint64_t r_prec, void *ksk, uint64_t ell, uint64_t special_primes, uint64_t num_threads); /* fhe.cdef:9 */
+void gp25_sub_a_mt(void *p0, uint64_t in_N, uint64_t *a, void *s_sign, uint64_t ell, uint64_t special_primes, uint64_t N, uint64_t num_threads); /* fhe.cdef:10 */
+
+/* ===================================================================== *
+ * Part 2: batched device API (new; no reference counterpart)             *
+ * ===================================================================== */
+
+/* Engine status: 0 when no error has been recorded since the last clear. */
+int vfhe_cuda_status(void);
+const char *vfhe_cuda_last_error(void);
+void vfhe_cuda_clear_error(void);
+/* Device ordinal this engine runs on, and a sync of its internal stream. */
+int vfhe_cuda_device(void);
+int vfhe_cuda_synchronize(void);
+
+/* Batched negacyclic (incomplete) NTT over a device buffer laid out as
+ * [batch][nlimbs][N] uint64 residues; limb slot k uses pool prime limbs[k] of the
+ * incNTT `ntt` (same split_degree layout as polynomial_RNSc_to_RNS).
+ * inverse = 0: coefficient -> NTT (polynomial_RNSc_to_RNS, rns_polynomial.c:582-597);
+ * inverse = 1: NTT -> coefficient (polynomial_RNS_to_RNSc, rns_polynomial.c:599-614).
+ * d_out may equal d_in.  `stream` is a cudaStream_t (NULL = legacy default stream). */
+int vfhe_cuda_ntt_batch(void *ntt, int inverse, uint64_t *d_out, const uint64_t *d_in,
+                        uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
+
+/* Batched incomplete ring product d_out = d_a * d_b over [batch][nlimbs][N] NTT-domain
+ * buffers (polynomial_mul_RNS_polynomial, rns_polynomial.c:311-356). */
+int vfhe_cuda_poly_mul_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
+                             uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
+
+/* Fused NTT -> incomplete product -> INTT for `batch` pairs of coefficient-domain
+ * polynomials [batch][nlimbs][N]: d_out = INTT(NTT(d_a) * NTT(d_b)). */
+int vfhe_cuda_ntt_mul_intt_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
+                                 uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
+
+/* CKKS evaluation over device-resident ciphertexts.
+ *
+ * A ciphertext at level with L active limbs is [2][L][N] uint64: component 0 is a,
+ * component 1 is b.  limbs[0..L) are the pool indices of the ciphertext primes in
+ * increasing order; `special` is the pool index of the special prime.  A key-switch
+ * key for L digits is [L][2][L+1][N] in the NTT domain: digit j, component (a,b),
+ * extended limbs (limbs[0..L) then `special`) -- the layout of
+ * MLWE_Set(...)->obj[0][j] in the reference (modules/mlwe/python/src/vfhe/mlwe/mlwe.py:145-177).
+ *
+ * vfhe_cuda_ckks_mul_relin_rescale_batch: d_out[i] = rescale(relin(d_ct1[i] x d_ct2[i]))
+ * for NTT-domain inputs, coefficient-domain outputs [2][L-1][N]; equal to
+ * CKKS_Ciphertext.__mul__ (ckks.py:227-241): mlwe_multiply (mlwe.c:711-760) then
+ * the round division of the top prime (mlwe.c:762-772).
+ *
+ * vfhe_cuda_ckks_rotate_batch: d_out[i] = automorphism(d_ct[i], gen) key-switched
+ * with d_gk, coefficient domain in and out (mlwe_automorphism_RNSc_GHS, mlwe.c:314-326).
+ *
+ * Scratch comes from `workspace` (device memory of at least the size returned by the
+ * matching *_workspace_bytes call); pass NULL to let the engine allocate it. */
+uint64_t vfhe_cuda_ckks_mul_workspace_bytes(void *ntt, uint64_t batch, uint32_t nlimbs);
+int vfhe_cuda_ckks_mul_relin_rescale_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct1,
+                                           const uint64_t *d_ct2, uint64_t batch,
+                                           const uint32_t *limbs, uint32_t nlimbs, uint32_t special,
+                                           const uint64_t *d_rlk, void *workspace, void *stream);
+uint64_t vfhe_cuda_ckks_rotate_workspace_bytes(void *ntt, uint64_t batch, uint32_t nlimbs);
+int vfhe_cuda_ckks_rotate_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct, uint64_t batch,
+                                const uint32_t *limbs, uint32_t nlimbs, uint32_t special,
+                                uint64_t gen, const uint64_t *d_gk, void *workspace, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VFHE_CUDA_H */

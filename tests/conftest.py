@@ -1,0 +1,83 @@
+"""Shared fixtures.
+
+``gpu`` marks tests that need a CUDA device (the cuda engine has no CPU path).
+The CPU oracle (oracle/vfhe_oracle.c, built to oracle/_build/) is loaded only here,
+as the checker; the reference libraries under oracle/_ref/ are used when present.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+ORACLE_SRC = ROOT / "oracle" / "vfhe_oracle.c"
+ORACLE_LIB = ROOT / "oracle" / "_build" / "libvfhe_oracle.so"
+REF_DIR = ROOT / "oracle" / "_ref"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built cuda engine")
+
+
+def build_oracle() -> Path:
+    """Compile the C oracle if its library is missing or stale."""
+    if not ORACLE_LIB.exists() or ORACLE_LIB.stat().st_mtime < ORACLE_SRC.stat().st_mtime:
+        ORACLE_LIB.parent.mkdir(exist_ok=True)
+        subprocess.run(
+            ["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-o", str(ORACLE_LIB), str(ORACLE_SRC)],
+            check=True,
+        )
+    return ORACLE_LIB
+
+
+@pytest.fixture(scope="session")
+def oracle_engine():
+    from vfhe_b200.native import Engine
+
+    return Engine(build_oracle(), "oracle")
+
+
+def ref_engine_path(name: str) -> Path | None:
+    p = REF_DIR / f"libvfhe_ref_{name}.so"
+    return p if p.exists() else None
+
+
+@pytest.fixture(scope="session")
+def ref_portable():
+    from vfhe_b200.native import Engine
+
+    p = ref_engine_path("portable")
+    if p is None:
+        pytest.skip("reference library not built (oracle/build_ref.sh)")
+    return Engine(p)
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    from vfhe_b200.native import cuda_engine
+
+    return cuda_engine()
+
+
+@pytest.fixture(autouse=True)
+def _fresh_prime_pools():
+    """Each test starts with empty prime pools, as in the reference's conftest.py:63-85."""
+    from vfhe_b200.arith import reset_registries
+
+    reset_registries()
+    yield
+    reset_registries()
+
+
+def has_ifma() -> bool:
+    try:
+        return "avx512ifma" in Path("/proc/cpuinfo").read_text()
+    except OSError:
+        return False
+
+
+os.environ.setdefault("VFHE_CUDA_QUIET", "1")

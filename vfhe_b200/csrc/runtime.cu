@@ -1,0 +1,440 @@
+// Device context, error recording, memory caches, PRNG state and transform tables.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <map>
+#include <string>
+
+#include "engine.cuh"
+
+namespace vc {
+
+// ---------------------------------------------------------------- context / errors
+Context& ctx() {
+    static Context c;
+    return c;
+}
+
+namespace {
+std::mutex g_err_mu;
+int g_status = 0;
+std::string g_error;
+}  // namespace
+
+void set_error(const char* where, const char* what) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    if (g_status == 0) {
+        g_status = 1;
+        g_error = std::string(where) + ": " + what;
+        if (getenv("VFHE_CUDA_QUIET") == nullptr) fprintf(stderr, "vfhe cuda engine: %s\n", g_error.c_str());
+    }
+}
+
+bool check_cuda(int code, const char* where) {
+    if (code == cudaSuccess) return true;
+    set_error(where, cudaGetErrorString((cudaError_t)code));
+    return false;
+}
+
+bool ensure_ready() {
+    Context& c = ctx();
+    if (c.ready) return true;
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    if (c.ready) return true;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        set_error("init", "no CUDA device is available (the cuda engine has no CPU fallback)");
+        return false;
+    }
+    int dev = 0;
+    if (const char* s = getenv("VFHE_CUDA_DEVICE")) dev = atoi(s);
+    if (!check_cuda(cudaSetDevice(dev), "init: cudaSetDevice")) return false;
+    if (!check_cuda(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "init: stream"))
+        return false;
+    c.device = dev;
+    c.ready = true;
+    return true;
+}
+
+cudaStream_t stream() { return ctx().stream; }
+
+bool sync(const char* where) {
+    cudaError_t e = cudaStreamSynchronize(ctx().stream);
+    if (e != cudaSuccess) return check_cuda(e, where);
+    return true;
+}
+
+// ---------------------------------------------------------------- memory caches
+namespace {
+struct Cache {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks;
+    std::map<void*, size_t> sizes;
+};
+Cache& managed_cache() {
+    static Cache c;
+    return c;
+}
+Cache& device_cache() {
+    static Cache c;
+    return c;
+}
+size_t round_bytes(size_t b) {
+    if (b < 4096) return 4096;
+    // round to 1/8 of the next power of two to bound waste and keep reuse high
+    size_t p = 1;
+    while (p < b) p <<= 1;
+    size_t step = p >> 3;
+    return (b + step - 1) / step * step;
+}
+void* cache_alloc(Cache& c, size_t bytes, bool managed) {
+    size_t rb = round_bytes(bytes);
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.free_blocks.find(rb);
+        if (it != c.free_blocks.end()) {
+            void* p = it->second;
+            c.free_blocks.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = managed ? cudaMallocManaged(&p, rb, cudaMemAttachGlobal) : cudaMalloc(&p, rb);
+    if (e != cudaSuccess) {
+        check_cuda(e, managed ? "cudaMallocManaged" : "cudaMalloc");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.sizes[p] = rb;
+    return p;
+}
+void cache_free(Cache& c, void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(c.mu);
+    auto it = c.sizes.find(p);
+    if (it == c.sizes.end()) return;
+    c.free_blocks.emplace(it->second, p);
+}
+}  // namespace
+
+void* managed_alloc(size_t bytes) {
+    if (!ensure_ready()) return nullptr;
+    return cache_alloc(managed_cache(), bytes, true);
+}
+void managed_free(void* p) { cache_free(managed_cache(), p); }
+void* device_alloc(size_t bytes) {
+    if (!ensure_ready()) return nullptr;
+    return cache_alloc(device_cache(), bytes, false);
+}
+void device_free(void* p) { cache_free(device_cache(), p); }
+
+void prefetch_to_device(const void* p, size_t bytes) {
+    if (!p || bytes == 0) return;
+    static int enabled = -1;
+    if (enabled < 0) {
+        const char* s = getenv("VFHE_CUDA_PREFETCH");
+        enabled = (s == nullptr || atoi(s) != 0) ? 1 : 0;
+    }
+    if (!enabled) return;
+    cudaMemPrefetchAsync(p, bytes, ctx().device, ctx().stream);
+    cudaGetLastError();  // a refused prefetch only costs speed
+}
+
+// ---------------------------------------------------------------- PRNG state
+namespace {
+uint64_t g_seed = 0;
+uint64_t g_counter = 0;
+bool g_seeded = false;
+uint64_t entropy_seed() {
+    uint64_t s = 0;
+    FILE* f = fopen("/dev/urandom", "rb");
+    if (f) {
+        if (fread(&s, sizeof s, 1, f) != 1) s = 0;
+        fclose(f);
+    }
+    return s ^ 0x9e3779b97f4a7c15ULL;
+}
+}  // namespace
+
+uint64_t prng_seed() {
+    if (!g_seeded) {
+        g_seed = entropy_seed();
+        g_counter = 0;
+        g_seeded = true;
+    }
+    return g_seed;
+}
+uint64_t prng_advance(uint64_t count) {
+    prng_seed();
+    uint64_t c = g_counter;
+    g_counter += count;
+    return c;
+}
+void prng_set(uint64_t seed, bool det) {
+    g_seed = det ? seed : entropy_seed();
+    g_counter = 0;
+    g_seeded = true;
+}
+
+// ---------------------------------------------------------------- number theory
+uint64_t host_mul_mod(uint64_t a, uint64_t b, uint64_t q) {
+    return (uint64_t)(((unsigned __int128)a * b) % q);
+}
+uint64_t host_pow_mod(uint64_t b, uint64_t e, uint64_t q) {
+    uint64_t r = 1 % q;
+    b %= q;
+    while (e) {
+        if (e & 1) r = host_mul_mod(r, b, q);
+        b = host_mul_mod(b, b, q);
+        e >>= 1;
+    }
+    return r;
+}
+uint64_t host_inv_mod(uint64_t a, uint64_t q) {
+    // extended Euclid on signed 128-bit to stay exact for q < 2^63
+    __int128 t = 0, nt = 1, r = q, nr = a % q;
+    while (nr != 0) {
+        __int128 quo = r / nr;
+        __int128 tmp = t - quo * nt;
+        t = nt;
+        nt = tmp;
+        tmp = r - quo * nr;
+        r = nr;
+        nr = tmp;
+    }
+    if (t < 0) t += q;
+    return (uint64_t)t;
+}
+uint64_t host_shoup(uint64_t w, uint64_t q) {
+    return (uint64_t)((((unsigned __int128)w) << 64) / q);
+}
+
+static uint64_t brv(uint64_t x, int bits) {
+    uint64_t r = 0;
+    for (int i = 0; i < bits; ++i) {
+        r = (r << 1) | (x & 1);
+        x >>= 1;
+    }
+    return r;
+}
+
+static int bit_length(uint64_t x) {
+    int b = 0;
+    while (x) {
+        ++b;
+        x >>= 1;
+    }
+    return b;
+}
+
+// The reference's deterministic root search (ntt_new_proc, ntt_portable.c:137-154):
+// the first g = 2, 3, ... whose (q-1)/2P power has order exactly 2P.
+static uint64_t find_root(uint64_t P, uint64_t q) {
+    for (uint64_t g = 2; g < q; ++g) {
+        uint64_t c = host_pow_mod(g, (q - 1) / (2 * P), q);
+        if (host_pow_mod(c, P, q) == q - 1) return c;
+    }
+    return 0;
+}
+
+bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
+                 std::vector<uint64_t>& twist_host) {
+    const uint64_t P = t->P;
+    const int logP = t->logP;
+    if (q < 3 || q >= (1ULL << 61) || ((q - 1) % (2 * P)) != 0) {
+        set_error("new_incomplete_ntt_list", "prime must be below 2^61 and congruent to 1 mod 2N/split");
+        return false;
+    }
+    const uint64_t psi = find_root(P, q);
+    const uint64_t psi_inv = host_inv_mod(psi, q);
+    proc->n = P;
+    proc->q = q;
+    proc->root_of_unity = psi;
+    proc->inv_root_of_unity = psi_inv;
+
+    std::vector<uint64_t> fwd(2 * P), inv(2 * P), tw(2 * P);
+    // forward / inverse twiddles: table[brv(i)] = psi^(+-i)   (ntt_portable.c:18-62)
+    uint64_t pf = 1, pi = 1;
+    for (uint64_t i = 0; i < P; ++i) {
+        uint64_t idx = brv(i, logP);
+        fwd[2 * idx] = pf;
+        fwd[2 * idx + 1] = host_shoup(pf, q);
+        inv[2 * idx] = pi;
+        inv[2 * idx + 1] = host_shoup(pi, q);
+        pf = host_mul_mod(pf, psi, q);
+        pi = host_mul_mod(pi, psi_inv, q);
+    }
+    // split-product twist: w[k] = psi^(2 brv(k) + 1)   (rns_polynomial.c:19-27, misc.c:186-192)
+    twist_host.resize(P);
+    for (uint64_t kk = 0; kk < P; ++kk) {
+        uint64_t w = host_pow_mod(psi, 2 * brv(kk, logP) + 1, q);
+        twist_host[kk] = w;
+        tw[2 * kk] = w;
+        tw[2 * kk + 1] = host_shoup(w, q);
+    }
+    void* blk = nullptr;
+    const size_t bytes = sizeof(uint64_t) * 6 * P;
+    if (!check_cuda(cudaMalloc(&blk, bytes), "table alloc")) return false;
+    uint64_t* d = (uint64_t*)blk;
+    if (!check_cuda(cudaMemcpy(d, fwd.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
+        !check_cuda(cudaMemcpy(d + 2 * P, inv.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
+        !check_cuda(cudaMemcpy(d + 4 * P, tw.data(), 16 * P, cudaMemcpyHostToDevice), "table upload"))
+        return false;
+    t->dev_blocks.push_back(blk);
+
+    PrimeInfo& o = *out;
+    memset(&o, 0, sizeof o);
+    o.q = q;
+    o.two_q = 2 * q;
+    const int b = bit_length(q);
+    o.bar_shift = (uint32_t)(b - 2);
+    o.bar_mu = (uint64_t)((((unsigned __int128)1) << (b + 62)) / q);
+    o.log_p = (uint32_t)logP;
+    o.p_inv = host_inv_mod(P % q, q);
+    o.p_inv_sh = host_shoup(o.p_inv, q);
+    const uint64_t last_tw = P >= 2 ? inv[2 * 1] : 1;
+    o.inv_last = host_mul_mod(last_tw, o.p_inv, q);
+    o.inv_last_sh = host_shoup(o.inv_last, q);
+    o.fwd = d;
+    o.inv = d + 2 * P;
+    o.twist = d + 4 * P;
+    o.fwd_f = nullptr;
+    return true;
+}
+
+bool upload_prime_info(IncNtt* t) {
+    const size_t n = t->info.size();
+    if (n > t->d_info_cap) {
+        size_t cap = n < 64 ? 64 : n;
+        PrimeInfo* d = nullptr;
+        if (!check_cuda(cudaMalloc(&d, cap * sizeof(PrimeInfo)), "prime info alloc")) return false;
+        if (t->d_info) {
+            // the old table may still be read by queued kernels: drain first
+            cudaStreamSynchronize(ctx().stream);
+            cudaFree(t->d_info);
+        }
+        t->d_info = d;
+        t->d_info_cap = cap;
+    }
+    return check_cuda(cudaMemcpy(t->d_info, t->info.data(), n * sizeof(PrimeInfo), cudaMemcpyHostToDevice),
+                      "prime info upload");
+}
+
+static bool add_primes(IncNtt* t, const uint64_t* primes, uint64_t count) {
+    const uint64_t P = t->P;
+    for (uint64_t i = 0; i < count; ++i) {
+        PrimeInfo pi;
+        _NTT_proc* proc = (_NTT_proc*)calloc(1, sizeof(_NTT_proc));
+        std::vector<uint64_t> tw;
+        if (!build_prime(t, primes[i], &pi, proc, tw)) {
+            free(proc);
+            return false;
+        }
+        uint64_t* w_row = (uint64_t*)aligned_alloc(64, ((P * 8 + 63) / 64) * 64);
+        memcpy(w_row, tw.data(), P * 8);
+        t->info.push_back(pi);
+        t->procs.push_back(proc);
+        // public arrays are reallocated as the pool grows
+        t->pub.ntt = (NTT_proc*)realloc(t->pub.ntt, sizeof(NTT_proc) * t->procs.size());
+        t->pub.w = (uint64_t**)realloc(t->pub.w, sizeof(uint64_t*) * t->procs.size());
+        t->pub.ntt[t->procs.size() - 1] = proc;
+        t->pub.w[t->procs.size() - 1] = w_row;
+    }
+    t->pub.l = t->procs.size();
+    return upload_prime_info(t);
+}
+
+IncNtt* ntt_create(const uint64_t* primes, uint64_t split, uint64_t N, uint64_t count) {
+    if (!ensure_ready()) return nullptr;
+    if (split == 0 || N == 0 || (N & (N - 1)) || (split & (split - 1)) || split > N) {
+        set_error("new_incomplete_ntt_list", "N and split_degree must be powers of two with split <= N");
+        return nullptr;
+    }
+    IncNtt* t = new IncNtt();
+    t->pub.ntt = nullptr;
+    t->pub.w = nullptr;
+    t->pub.N = N;
+    t->pub.split_degree = split;
+    t->pub.l = 0;
+    t->P = N / split;
+    int lp = 0;
+    while ((1ULL << lp) < t->P) ++lp;
+    t->logP = lp;
+    if (lp > 17) {
+        set_error("new_incomplete_ntt_list", "N/split_degree above 2^17 is not supported");
+        delete t;
+        return nullptr;
+    }
+    if (count > (uint64_t)kMaxLimbs) {
+        set_error("new_incomplete_ntt_list", "at most 64 primes per pool (rns_mask is 64-bit)");
+        delete t;
+        return nullptr;
+    }
+    if (!add_primes(t, primes, count)) {
+        delete t;
+        return nullptr;
+    }
+    return t;
+}
+
+bool ntt_extend(IncNtt* t, const uint64_t* primes, uint64_t count) {
+    if (t->procs.size() + count > (uint64_t)kMaxLimbs) {
+        set_error("incNTT_extend_with_primes", "at most 64 primes per pool (rns_mask is 64-bit)");
+        return false;
+    }
+    return add_primes(t, primes, count);
+}
+
+Poly* poly_create(uint64_t N, uint64_t mask, IncNtt* t) {
+    if (!t) {
+        set_error("polynomial_new_RNS_polynomial", "null incNTT");
+        return nullptr;
+    }
+    Poly* p = new Poly();
+    const uint64_t l = t->pub.l;
+    p->base = (uint64_t*)managed_alloc(sizeof(uint64_t) * l * t->pub.N);
+    p->pub.coeffs = (uint64_t**)malloc(sizeof(uint64_t*) * (l ? l : 1));
+    for (uint64_t i = 0; i < l; ++i) p->pub.coeffs[i] = p->base ? p->base + i * t->pub.N : nullptr;
+    p->pub.ntt = &t->pub;
+    p->pub.rns_mask = mask;
+    p->pub.allocated_l = l;
+    (void)N;
+    return p;
+}
+
+void poly_destroy(Poly* p) {
+    if (!p) return;
+    managed_free(p->base);
+    free(p->pub.coeffs);
+    delete p;
+}
+
+}  // namespace vc
+
+// ---------------------------------------------------------------- status ABI
+extern "C" {
+
+int vfhe_cuda_status(void) { return vc::g_status; }
+
+const char* vfhe_cuda_last_error(void) { return vc::g_error.c_str(); }
+
+void vfhe_cuda_clear_error(void) {
+    std::lock_guard<std::mutex> lk(vc::g_err_mu);
+    vc::g_status = 0;
+    vc::g_error.clear();
+}
+
+int vfhe_cuda_device(void) {
+    if (!vc::ensure_ready()) return -1;
+    return vc::ctx().device;
+}
+
+int vfhe_cuda_synchronize(void) {
+    if (!vc::ensure_ready()) return 1;
+    return vc::sync("vfhe_cuda_synchronize") ? 0 : 1;
+}
+
+}  // extern "C"
