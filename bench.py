@@ -1,0 +1,429 @@
+"""Benchmark: batched CKKS multiply -> relinearise -> rescale -> rotate on B200.
+
+Workload (one "step"): 256 ciphertext pairs in Z_Q[X]/(X^16384 + 1), one 50-bit base
+prime + eight 40-bit primes (L = 9) plus one 50-bit special prime, scale 2^40,
+ternary secret, sigma 3.2 errors, 2^13 slots uniform in the unit disk.  Each pair is
+multiplied, relinearised, rescaled to L = 8 and rotated by a step drawn from
+{1, 2, 4, ..., 2^12} (13 Galois keys resident in HBM).  All inputs are synthetic
+from fixed seeds.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+Prints one JSON line (rank 0).  ``value`` is pairs per second over all ranks with
+ciphertexts already in HBM; ``e2e`` adds the host->device copy of each step's input
+ciphertexts from pinned memory and the device->host copy of its results.  The
+reference arm runs the reference's own CPU library (built from its sources into
+oracle/_ref/) on the same workload, one process per host core.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+N_DEG = 2**14
+PRIME_SIZES = [50] + [40] * 8 + [50]
+PAIRS = 256
+STEPS_SET = [1 << i for i in range(13)]
+SCALE = 2.0**40
+SEED = 20261203
+CONFIG = {
+    "workload": "CKKS mul+relin+rescale+rotate, N=2^14, L=9 (1x50-bit + 8x40-bit) + 1 special 50-bit prime, "
+                "scale 2^40, 256 ciphertext pairs per step, rotation steps 2^0..2^12",
+    "N": N_DEG,
+    "L": 9,
+    "special_primes": 1,
+    "pairs_per_step": PAIRS,
+    "l2_policy": "inputs larger than L2 (1.2 GB of ciphertexts per step)",
+    "parallelism": "replicas, ciphertext pairs sharded by rank (no data-path collective)",
+}
+
+
+# ----------------------------------------------------------------------------- setup
+def build_workload(engine, pairs: int, seed: int, gk_steps=STEPS_SET):
+    """Keys and ciphertexts through the reference API mirror (seeded, engine-independent)."""
+    from vfhe_b200.arith import Ring
+    from vfhe_b200.fhe import CKKS_Scheme
+    from vfhe_b200.native import use_engine
+
+    with use_engine(engine):
+        rng = np.random.default_rng(seed)
+        R = Ring(N_DEG, prime_size=PRIME_SIZES, split_degree=1)
+        s = CKKS_Scheme(R, scaling_factor=SCALE, special_primes=1)
+        key = s.key_gen_uniform_ternary(3.2, rng)
+        rlk = s.gen_rlk(key, key, lvl=0, rng=rng)
+        gks = {k: s.gen_ksk_automorphism(key, key, s.galois_gen(k), lvl=1, rng=rng) for k in gk_steps}
+        steps = [int(v) for v in rng.choice(gk_steps, pairs)]
+        zs, cts = [], []
+        for _ in range(2 * pairs):
+            z = np.sqrt(rng.random(N_DEG // 2)) * np.exp(2j * np.pi * rng.random(N_DEG // 2))
+            zs.append(z)
+            cts.append(s.encrypt(s.encode(list(z)), key, rng=rng))
+        return s, key, rlk, gks, steps, zs, cts
+
+
+def decoded_error(s, key, ct, expect, delta) -> float:
+    dec = np.array(s.decode(s.decrypt(ct, key), scaling_factor=delta))
+    return float(np.max(np.abs(dec - expect)))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self) -> dict:
+        if not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- cpu legs
+def _ref_library() -> tuple[Path, str]:
+    ifma = "avx512ifma" in Path("/proc/cpuinfo").read_text()
+    name = "avx512ifma" if ifma else "portable"
+    return ROOT / "oracle" / "_ref" / f"libvfhe_ref_{name}.so", name
+
+
+def _ref_worker(args) -> dict:
+    """One host core: reference library, a bounded number of pairs, warmup + timed steps."""
+    pairs, warmup, steps, seed, time_budget = args
+    from vfhe_b200.native import Engine
+
+    lib, name = _ref_library()
+    eng = Engine(lib)
+    s, key, rlk, gks, rot, zs, cts = build_workload(eng, pairs, seed, gk_steps=sorted(set(STEPS_SET[:2])))
+
+    def one_step():
+        for p in range(pairs):
+            prod = s.multiply(cts[2 * p], cts[2 * p + 1], rlk)
+            prod.round_division(lvl=1)
+            k = STEPS_SET[p % 2]
+            s.automorphism(prod, s.galois_gen(k), gks[k])
+
+    for _ in range(warmup):
+        one_step()
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(steps):
+        one_step()
+        done += 1
+        if time_budget and time.perf_counter() - t0 > time_budget:
+            break
+    return {"elapsed": time.perf_counter() - t0, "pairs": pairs * done, "engine": name}
+
+
+def cpu_baseline(time_budget: float = 15.0) -> dict:
+    """Reference library, one core, bounded sample of the same workload (pairs/s)."""
+    lib, name = _ref_library()
+    if not lib.exists():
+        return {"value": None, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    r = _ref_worker((1, 1, 50, SEED + 7, time_budget))
+    return {"value": r["pairs"] / r["elapsed"], "unit": "pairs/s", "cores": 1, "kind": "reference",
+            "sample": f"{r['pairs']} pairs of the same workload on the reference's {name} engine, "
+                      f"one thread, {r['elapsed']:.1f} s"}
+
+
+def run_reference_arm(args) -> None:
+    import multiprocessing as mp
+
+    lib, name = _ref_library()
+    if not lib.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/build_ref.sh)"}))
+        return
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    workers = max(1, min(cores, 96))
+    ctx = mp.get_context("spawn")
+    steps = args.steps
+    with ctx.Pool(workers) as pool:
+        res = pool.map(_ref_worker, [(1, args.warmup, steps, SEED + 1000 + w, 0) for w in range(workers)])
+    elapsed = max(r["elapsed"] for r in res)
+    total = sum(r["pairs"] for r in res)
+    value = total / elapsed
+    line = {
+        "impl": "reference", "metric": "CKKS mul+relin+rescale/s", "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (RNS residues < 2^50)",
+        "data": "synthetic (seeded)", "config": dict(CONFIG, pairs_per_step=workers),
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": workers, "kind": "reference",
+                         "sample": f"{workers} processes x 1 pair per step on the reference's {name} engine"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------- gpu arm
+def run_cuda_arm(args) -> None:
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ.setdefault("VFHE_CUDA_DEVICE", str(local))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from vfhe_b200.batch import CkksBatch, ciphertext_rows, key_tensor, to_device
+    from vfhe_b200.native import cuda_engine
+
+    eng = cuda_engine()
+    s, key, rlk, gks, rot_steps, zs, cts = build_workload(eng, PAIRS, SEED + rank)
+    for c in cts:
+        c.to_NTT()
+    host1 = np.stack([ciphertext_rows(c) for c in cts[0::2]])
+    host2 = np.stack([ciphertext_rows(c) for c in cts[1::2]])
+    d1, d2 = to_device(host1), to_device(host2)
+    rlk_t = key_tensor(rlk)
+    gk_t = {k: key_tensor(v) for k, v in gks.items()}
+    special = s.special_rings[0].prime_indices[-1]
+    mul = CkksBatch(s.rings[0], special, eng)
+    rotb = CkksBatch(s.rings[1], special, eng)
+    gens = [s.galois_gen(k) for k in rot_steps]
+    keys = [gk_t[k] for k in rot_steps]
+    prod = torch.empty((PAIRS, 2, 8, N_DEG), dtype=torch.int64, device="cuda")
+    rot = torch.empty_like(prod)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        mul.mul_relin_rescale(d1, d2, rlk_t, out=prod)
+        rotb.rotate(prod, gens, keys, out=rot)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- device-resident throughput
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    launches0 = eng.lib.vfhe_cuda_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        barrier()
+    launches = eng.lib.vfhe_cuda_launch_count() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * PAIRS / (ms * 1e-3)
+
+    # ---- end to end: pinned host inputs in, host results out, every step
+    h1 = torch.from_numpy(host1.view(np.int64)).pin_memory()
+    h2 = torch.from_numpy(host2.view(np.int64)).pin_memory()
+    hout = torch.empty(rot.shape, dtype=torch.int64).pin_memory()
+    e2e_steps = max(2, min(args.steps, 5))
+
+    def e2e_step():
+        d1.copy_(h1, non_blocking=True)
+        d2.copy_(h2, non_blocking=True)
+        step()
+        hout.copy_(rot, non_blocking=True)
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    ev1.record(stream)
+    barrier()
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * PAIRS / (e2e_ms * 1e-3)
+    _ = time.perf_counter() - t0
+
+    # ---- dominant kernel: the digit transforms (B x (L+1) rows of N = 2^14 per launch)
+    ffi = eng.ffi
+    ext = list(s.special_rings[0].prime_indices)
+    ne = len(ext)
+    buf = torch.empty((PAIRS, ne, N_DEG), dtype=torch.int64, device="cuda")
+    for k, idx in enumerate(ext):
+        buf[:, k].random_(0, s.special_rings[0].primes[k])
+    limbs = ffi.new("uint32_t[]", ext)
+    ptr = ffi.cast("uint64_t*", buf.data_ptr())
+    sp = ffi.cast("void*", stream.cuda_stream)
+    for _ in range(3):
+        eng.lib.vfhe_cuda_ntt_batch(s.special_rings[0].NTT, 0, ptr, ptr, PAIRS, limbs, ne, sp)
+    torch.cuda.synchronize()
+    reps = 20
+    ev0.record(stream)
+    for _ in range(reps):
+        eng.lib.vfhe_cuda_ntt_batch(s.special_rings[0].NTT, 0, ptr, ptr, PAIRS, limbs, ne, sp)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ntt_ms = ev0.elapsed_time(ev1) / reps
+    alg_bytes = PAIRS * ne * 16 * N_DEG
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ntt_ms * 1e-3) / 1e9
+    del buf
+
+    # ---- secondary: N = 2^16, L = 24 forward NTT limbs/s (the survey's NTT metric)
+    from vfhe_b200.arith import Ring
+
+    R16 = Ring(2**16, prime_size=[50] * 24, split_degree=1, engine=eng)
+    b16 = torch.empty((8, 24, 2**16), dtype=torch.int64, device="cuda")
+    for k, q in enumerate(R16.primes):
+        b16[:, k].random_(0, q)
+    l16 = ffi.new("uint32_t[]", R16.prime_indices)
+    p16 = ffi.cast("uint64_t*", b16.data_ptr())
+    for _ in range(3):
+        eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, 8, l16, 24, sp)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(reps):
+        eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, 8, l16, 24, sp)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms16 = ev0.elapsed_time(ev1) / reps
+    limbs16 = 8 * 24 / (ms16 * 1e-3)
+    del b16
+    eng.check("bench")
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- decoded error of one pair (host decode)
+    from vfhe_b200.fhe import CKKS_Ciphertext
+    from vfhe_b200.batch import to_host
+
+    out_rows = to_host(rot[:1])[0]
+    c = CKKS_Ciphertext(s, lvl=1)
+    c.set_component_rows(0, out_rows[0])
+    c.set_component_rows(1, out_rows[1])
+    from vfhe_b200.arith import repr as prepr
+
+    c.repr = prepr.coeff
+    delta = SCALE * SCALE / s.rings[0].primes[-1]
+    expect = np.roll(zs[0] * zs[1], -rot_steps[0])
+    err = decoded_error(s, key, c, expect, delta)
+
+    line = {
+        "metric": "CKKS mul+relin+rescale/s",
+        "value": value,
+        "unit": "pairs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": max(3, args.warmup),
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64 (RNS residues < 2^50)",
+        "data": "synthetic (seeded keys, noise and unit-disk slots)",
+        "config": CONFIG,
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
+                "d2h_bytes_per_step": int(hout.numel() * 8), "ms_per_step": e2e_ms},
+        "roofline": {"bound": "hbm", "kernel": "k_ntt_pass (digit transforms, 2560 rows x 2^14)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": None, "launch_ms": ntt_ms,
+                     "algorithmic_bytes": alg_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "decoded_max_error": err,
+        "ntt_2p16_L24": {"limbs_per_s": limbs16, "ms_per_8_polys": ms16,
+                         "frac_hbm": 16 * 2**16 * limbs16 / 1e9 / peak},
+    }
+    if world == 1:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    args = ap.parse_args()
+    sys.path.insert(0, str(ROOT))
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        run_reference_arm(args)
+    else:
+        run_cuda_arm(args)
+
+
+if __name__ == "__main__":
+    main()

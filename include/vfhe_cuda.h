@@ -279,6 +279,8 @@ void vfhe_cuda_clear_error(void);
 /* Device ordinal this engine runs on, and a sync of its internal stream. */
 int vfhe_cuda_device(void);
 int vfhe_cuda_synchronize(void);
+/* Number of transform and batched-CKKS kernels this engine has launched so far. */
+uint64_t vfhe_cuda_launch_count(void);
 
 /* Batched negacyclic (incomplete) NTT over a device buffer laid out as
  * [batch][nlimbs][N] uint64 residues; limb slot k uses pool prime limbs[k] of the
@@ -313,8 +315,10 @@ int vfhe_cuda_ntt_mul_intt_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a
  * CKKS_Ciphertext.__mul__ (ckks.py:227-241): mlwe_multiply (mlwe.c:711-760) then
  * the round division of the top prime (mlwe.c:762-772).
  *
- * vfhe_cuda_ckks_rotate_batch: d_out[i] = automorphism(d_ct[i], gen) key-switched
- * with d_gk, coefficient domain in and out (mlwe_automorphism_RNSc_GHS, mlwe.c:314-326).
+ * vfhe_cuda_ckks_rotate_batch: d_out[i] = automorphism(d_ct[i], gens[i]) key-switched
+ * with the key at d_gks[i], coefficient domain in and out [2][L][N]
+ * (mlwe_automorphism_RNSc_GHS, mlwe.c:314-326).  gens and d_gks are host arrays of
+ * `batch` entries (Galois elements, device key pointers).
  *
  * Scratch comes from `workspace` (device memory of at least the size returned by the
  * matching *_workspace_bytes call); pass NULL to let the engine allocate it. */
@@ -326,7 +330,8 @@ int vfhe_cuda_ckks_mul_relin_rescale_batch(void *ntt, uint64_t *d_out, const uin
 uint64_t vfhe_cuda_ckks_rotate_workspace_bytes(void *ntt, uint64_t batch, uint32_t nlimbs);
 int vfhe_cuda_ckks_rotate_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct, uint64_t batch,
                                 const uint32_t *limbs, uint32_t nlimbs, uint32_t special,
-                                uint64_t gen, const uint64_t *d_gk, void *workspace, void *stream);
+                                const uint64_t *gens, const uint64_t *const *d_gks, void *workspace,
+                                void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,97 @@
+"""Batched device API over torch tensors (vfhe_cuda.h Part 2).
+
+Ciphertexts and keys live in HBM as int64 tensors holding uint64 residues:
+  ciphertext batch   [B][2][L][N]        (component a, b; limbs in ring order)
+  key-switching key  [D][2][L+1][N]      (digit, component, extended limb), NTT domain
+Torch supplies device memory and streams only; every operation is one call into the
+engine library with raw device pointers.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .arith import Ring
+from .mlwe import MLWE, MLWE_Set
+from .native import Engine, EngineError, cuda_engine
+
+
+def _ptr(ffi, t: torch.Tensor):
+    assert t.is_cuda and t.is_contiguous()
+    return ffi.cast("uint64_t*", t.data_ptr())
+
+
+def to_device(a: np.ndarray, device="cuda") -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).to(device)
+
+
+def to_host(t: torch.Tensor) -> np.ndarray:
+    return t.cpu().numpy().view(np.uint64)
+
+
+class CkksBatch:
+    """Batched CKKS evaluation for one level chain of a CKKS scheme."""
+
+    def __init__(self, ring: Ring, special_index: int, engine: Engine | None = None):
+        self.engine = engine or cuda_engine()
+        self.ring = ring
+        self.ffi = self.engine.ffi
+        self.lib = self.engine.lib
+        self.special = special_index
+        self._limbs = self.ffi.new("uint32_t[]", list(ring.prime_indices))
+        self.L = ring.ell
+        self._ws: torch.Tensor | None = None
+
+    def _stream(self, stream: torch.cuda.Stream | None):
+        st = stream or torch.cuda.current_stream()
+        return self.ffi.cast("void*", st.cuda_stream)
+
+    def _workspace(self, nbytes: int) -> torch.Tensor:
+        if self._ws is None or self._ws.numel() * 8 < nbytes:
+            self._ws = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device="cuda")
+        return self._ws
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            self.engine.check(what)
+            raise EngineError(what)
+
+    def mul_relin_rescale(self, ct1: torch.Tensor, ct2: torch.Tensor, rlk: torch.Tensor,
+                          out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        B = ct1.shape[0]
+        N = self.ring.N
+        if out is None:
+            out = torch.empty((B, 2, self.L - 1, N), dtype=torch.int64, device="cuda")
+        ws = self._workspace(self.lib.vfhe_cuda_ckks_mul_workspace_bytes(self.ring.NTT, B, self.L))
+        rc = self.lib.vfhe_cuda_ckks_mul_relin_rescale_batch(
+            self.ring.NTT, _ptr(self.ffi, out), _ptr(self.ffi, ct1), _ptr(self.ffi, ct2), B, self._limbs,
+            self.L, self.special, _ptr(self.ffi, rlk), self.ffi.cast("void*", ws.data_ptr()), self._stream(stream))
+        self._check(rc, "ckks_mul_relin_rescale_batch")
+        return out
+
+    def rotate(self, ct: torch.Tensor, gens: list[int], keys: list[torch.Tensor], out: torch.Tensor | None = None,
+               stream=None) -> torch.Tensor:
+        B = ct.shape[0]
+        if out is None:
+            out = torch.empty_like(ct)
+        ws = self._workspace(self.lib.vfhe_cuda_ckks_rotate_workspace_bytes(self.ring.NTT, B, self.L))
+        g = self.ffi.new("uint64_t[]", [int(x) for x in gens])
+        kp = self.ffi.new("uint64_t*[]", [_ptr(self.ffi, k) for k in keys])
+        rc = self.lib.vfhe_cuda_ckks_rotate_batch(
+            self.ring.NTT, _ptr(self.ffi, out), _ptr(self.ffi, ct), B, self._limbs, self.L, self.special, g, kp,
+            self.ffi.cast("void*", ws.data_ptr()), self._stream(stream))
+        self._check(rc, "ckks_rotate_batch")
+        return out
+
+
+def ciphertext_rows(ct: MLWE) -> np.ndarray:
+    """[2][L][N] raw rows of a rank-1 ciphertext."""
+    return np.stack([ct.component_rows(0), ct.component_rows(1)])
+
+
+def key_tensor(ks: MLWE_Set, component: int = 0) -> torch.Tensor:
+    """Device copy of one component of a key-switching key set, [D][2][L+1][N]."""
+    arr = ks.key_arrays()[component]
+    assert arr is not None
+    return to_device(arr)

@@ -1,5 +1,5 @@
 // Batched device API (Part 2 of vfhe_cuda.h): plain device pointers and a caller
-// stream, no managed memory and no synchronisation.
+// stream, no managed memory, no synchronisation unless the engine has to allocate.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -8,6 +8,16 @@
 using namespace vc;
 
 namespace vc {
+uint64_t ckks_mul_ws_elems(uint64_t N, uint64_t B, uint64_t L);
+uint64_t ckks_rot_ws_elems(uint64_t N, uint64_t B, uint64_t L);
+int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const uint64_t* ct2, uint64_t B,
+                           const uint32_t* limbs, uint32_t L, uint32_t special, const uint64_t* rlk, uint64_t* ws,
+                           cudaStream_t st);
+int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const uint32_t* limbs, uint32_t L,
+                uint32_t special, const uint64_t* gens, const uint64_t* const* gks, uint64_t* ws, cudaStream_t st);
+}  // namespace vc
+
+namespace {
 
 bool batch_rowset(IncNtt* t, uint64_t* d_out, const uint64_t* d_in, uint64_t batch, const uint32_t* limbs,
                   uint32_t nlimbs, RowSet* rs, const char* where) {
@@ -31,10 +41,30 @@ bool batch_rowset(IncNtt* t, uint64_t* d_out, const uint64_t* d_in, uint64_t bat
     rs->logP = t->logP;
     rs->batch = (int)batch;
     rs->batch_stride = (long long)(nlimbs * N);
+    rs->in_batch_stride = rs->batch_stride;
     return true;
 }
 
-}  // namespace vc
+// Scratch owned by the engine when the caller passes no workspace: grown on demand,
+// recycled only after the stream that used it has drained.
+uint64_t* engine_workspace(size_t bytes, cudaStream_t st) {
+    static void* buf = nullptr;
+    static size_t cap = 0;
+    if (bytes > cap) {
+        cudaStreamSynchronize(st);
+        if (buf) cudaFree(buf);
+        buf = nullptr;
+        cap = 0;
+        if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+            set_error("workspace", "cudaMalloc failed");
+            return nullptr;
+        }
+        cap = bytes;
+    }
+    return (uint64_t*)buf;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -51,13 +81,17 @@ int vfhe_cuda_poly_mul_batch(void* ntt, uint64_t* d_out, const uint64_t* d_a, co
                              uint64_t batch, const uint32_t* limbs, uint32_t nlimbs, void* stream_) {
     if (!vc::ensure_ready()) return 1;
     IncNtt* t = as_ntt(ntt);
-    if (!t || nlimbs == 0 || nlimbs > (uint32_t)kMaxLimbs) {
+    if (!t || !limbs || nlimbs == 0 || nlimbs > (uint32_t)kMaxLimbs) {
         set_error("vfhe_cuda_poly_mul_batch", "bad pool or limb list");
         return 1;
     }
     const uint64_t N = t->pub.N;
     EwSet s = empty_set((long long)N);
     for (uint32_t k = 0; k < nlimbs; ++k) {
+        if (limbs[k] >= t->pub.l) {
+            set_error("vfhe_cuda_poly_mul_batch", "limb index outside the pool");
+            return 1;
+        }
         s.out[k] = d_out + (uint64_t)k * N;
         s.a[k] = d_a + (uint64_t)k * N;
         s.b[k] = d_b + (uint64_t)k * N;
@@ -75,47 +109,49 @@ int vfhe_cuda_ntt_mul_intt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_a
     if (!vc::ensure_ready()) return 1;
     IncNtt* t = as_ntt(ntt);
     if (!t) return 1;
-    const uint64_t elems = batch * nlimbs * t->pub.N;
-    uint64_t* tmp = (uint64_t*)device_alloc(elems * 8);
-    if (!tmp) return 1;
     cudaStream_t st = (cudaStream_t)stream_;
+    uint64_t* tmp = engine_workspace(batch * nlimbs * t->pub.N * 8, st);
+    if (!tmp) return 1;
     int rc = vfhe_cuda_ntt_batch(ntt, 0, tmp, d_b, batch, limbs, nlimbs, stream_);
     if (!rc) rc = vfhe_cuda_ntt_batch(ntt, 0, d_out, d_a, batch, limbs, nlimbs, stream_);
     if (!rc) rc = vfhe_cuda_poly_mul_batch(ntt, d_out, d_out, tmp, batch, limbs, nlimbs, stream_);
     if (!rc) rc = vfhe_cuda_ntt_batch(ntt, 1, d_out, d_out, batch, limbs, nlimbs, stream_);
-    // the scratch may only be recycled once the stream has consumed it
-    cudaStreamSynchronize(st);
-    device_free(tmp);
     return rc;
 }
 
 uint64_t vfhe_cuda_ckks_mul_workspace_bytes(void* ntt, uint64_t batch, uint32_t nlimbs) {
-    (void)ntt; (void)batch; (void)nlimbs;
-    return 0;
+    IncNtt* t = as_ntt(ntt);
+    return t ? 8 * ckks_mul_ws_elems(t->pub.N, batch, nlimbs) : 0;
 }
 
 int vfhe_cuda_ckks_mul_relin_rescale_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct1, const uint64_t* d_ct2,
                                            uint64_t batch, const uint32_t* limbs, uint32_t nlimbs,
                                            uint32_t special, const uint64_t* d_rlk, void* workspace,
                                            void* stream_) {
-    (void)ntt; (void)d_out; (void)d_ct1; (void)d_ct2; (void)batch; (void)limbs; (void)nlimbs; (void)special;
-    (void)d_rlk; (void)workspace; (void)stream_;
-    set_error("vfhe_cuda_ckks_mul_relin_rescale_batch", "not built yet");
-    return 1;
+    if (!vc::ensure_ready()) return 1;
+    IncNtt* t = as_ntt(ntt);
+    cudaStream_t st = (cudaStream_t)stream_;
+    uint64_t* ws = (uint64_t*)workspace;
+    if (!ws) ws = engine_workspace(vfhe_cuda_ckks_mul_workspace_bytes(ntt, batch, nlimbs), st);
+    if (!ws) return 1;
+    return ckks_mul_relin_rescale(t, d_out, d_ct1, d_ct2, batch, limbs, nlimbs, special, d_rlk, ws, st);
 }
 
 uint64_t vfhe_cuda_ckks_rotate_workspace_bytes(void* ntt, uint64_t batch, uint32_t nlimbs) {
-    (void)ntt; (void)batch; (void)nlimbs;
-    return 0;
+    IncNtt* t = as_ntt(ntt);
+    return t ? 8 * ckks_rot_ws_elems(t->pub.N, batch, nlimbs) : 0;
 }
 
 int vfhe_cuda_ckks_rotate_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct, uint64_t batch,
-                                const uint32_t* limbs, uint32_t nlimbs, uint32_t special, uint64_t gen,
-                                const uint64_t* d_gk, void* workspace, void* stream_) {
-    (void)ntt; (void)d_out; (void)d_ct; (void)batch; (void)limbs; (void)nlimbs; (void)special; (void)gen;
-    (void)d_gk; (void)workspace; (void)stream_;
-    set_error("vfhe_cuda_ckks_rotate_batch", "not built yet");
-    return 1;
+                                const uint32_t* limbs, uint32_t nlimbs, uint32_t special, const uint64_t* gens,
+                                const uint64_t* const* d_gks, void* workspace, void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    IncNtt* t = as_ntt(ntt);
+    cudaStream_t st = (cudaStream_t)stream_;
+    uint64_t* ws = (uint64_t*)workspace;
+    if (!ws) ws = engine_workspace(vfhe_cuda_ckks_rotate_workspace_bytes(ntt, batch, nlimbs), st);
+    if (!ws) return 1;
+    return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, gens, d_gks, ws, st);
 }
 
 }  // extern "C"

@@ -1,0 +1,357 @@
+// Batched CKKS evaluation over device-resident ciphertexts: multiply + relinearise +
+// rescale, and rotate (Galois automorphism + key switch).
+//
+// The steps are the reference's (mlwe_multiply, mlwe.c:711-760; GHS key switch,
+// mlwe.c:557-598; gadget product, gadget.c:5-36; round division,
+// rns_polynomial.c:939-976; permutation, rns_polynomial.c:996-1035), batched over
+// ciphertexts and fused where the data allows:
+//   * the tensor product writes all three components in one pass;
+//   * the digit broadcast (limb j reduced modulo every extended prime) happens in
+//     the load of the forward transform, so the broadcast rows are never stored;
+//   * the special-prime round division, the pass-through additions and the CKKS
+//     rescale (division by the top prime) are one kernel per coefficient;
+//   * the forward transform at the end of the reference's mlwe_multiply and the
+//     inverse transform at the start of its rescale are both skipped: they are
+//     inverse bijections on canonical residues, so skipping them changes no bit.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <vector>
+
+#include "abi_common.cuh"
+
+namespace vc {
+
+namespace {
+
+struct LimbPrimes {
+    uint32_t p[kMaxLimbs];
+};
+
+// d0 = a1 a2, d1 = a1 b2 + b1 a2, d2 = b1 b2 per NTT slot (mlwe.c:665-709 at rank 1).
+__global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ c1,
+                         const uint64_t* __restrict__ c2, const __grid_constant__ LimbPrimes lp,
+                         const PrimeInfo* __restrict__ primes, int L, long long N) {
+    const int by = blockIdx.y;
+    const int b = by / L, k = by - b * L;
+    const PrimeInfo pi = primes[lp.p[k]];
+    const long long cs = (long long)2 * L * N, ts = (long long)3 * L * N, LN = (long long)L * N;
+    const uint64_t* a1 = c1 + b * cs + k * N;
+    const uint64_t* b1 = a1 + LN;
+    const uint64_t* a2 = c2 + b * cs + k * N;
+    const uint64_t* b2 = a2 + LN;
+    uint64_t* t0 = T + b * ts + k * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+         x += (long long)gridDim.x * blockDim.x) {
+        const uint64_t va1 = a1[x], vb1 = b1[x], va2 = a2[x], vb2 = b2[x];
+        t0[x] = mul_mod(va1, va2, pi);
+        t0[x + LN] = add_mod(mul_mod(va1, vb2, pi), mul_mod(vb1, va2, pi), pi.q);
+        t0[x + 2 * LN] = mul_mod(vb1, vb2, pi);
+    }
+}
+
+// acc[b][c][i] = -sum_j D[b][j][i] * K_b[j][c][i]   (gadget_mul_subto_polynomial, gadget.c:22-36)
+// D: [B][nd][ne][N]; K_b: [digits][2][ne][N] (only the first nd digits are used);
+// acc: [B][2][ne][N].
+__global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
+                      const uint64_t* const* __restrict__ keys, const __grid_constant__ LimbPrimes lp,
+                      const PrimeInfo* __restrict__ primes, int nd, int ne, long long N) {
+    const int by = blockIdx.y;
+    const int b = by / ne, i = by - b * ne;
+    const PrimeInfo pi = primes[lp.p[i]];
+    const uint64_t* key = keys[b];
+    const long long dstride = (long long)ne * N;       // between digits of D
+    const long long kstride = (long long)2 * ne * N;   // between digits of K
+    const uint64_t* d = D + (long long)b * nd * dstride + (long long)i * N;
+    const uint64_t* ka = key + (long long)i * N;
+    const uint64_t* kb = ka + dstride;
+    uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
+    uint64_t* ob = oa + dstride;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+         x += (long long)gridDim.x * blockDim.x) {
+        uint64_t sa = 0, sb = 0;
+        for (int j = 0; j < nd; ++j) {
+            const uint64_t v = d[j * dstride + x];
+            sa = add_mod(sa, mul_mod(v, ka[j * kstride + x], pi), pi.q);
+            sb = add_mod(sb, mul_mod(v, kb[j * kstride + x], pi), pi.q);
+        }
+        oa[x] = neg_mod(sa, pi.q);
+        ob[x] = neg_mod(sb, pi.q);
+    }
+}
+
+struct ModDownConsts {
+    uint32_t prime[kMaxLimbs];      // pool index of output limb i (i < nl)
+    uint64_t half_sp[kMaxLimbs];    // floor(p/2) mod q_i, p the special prime
+    uint64_t inv_sp[kMaxLimbs];     // p^-1 mod q_i
+    uint64_t inv_sp_sh[kMaxLimbs];
+    uint64_t half_r[kMaxLimbs];     // floor(q_top/2) mod q_i
+    uint64_t inv_r[kMaxLimbs];      // q_top^-1 mod q_i
+    uint64_t inv_r_sh[kMaxLimbs];
+    uint32_t special;               // pool index of the special prime
+    uint64_t p, half_p;             // special prime and floor(p/2)
+    uint64_t q_top, half_top;       // top prime dropped by the rescale
+};
+
+// Per coefficient: divide the key-switch accumulator by the special prime with
+// rounding, add the pass-through component, and optionally rescale by the top prime.
+// acc: [B][2][nl+1][N] coefficient domain; pass_c: [B][..][nl][N] rows at pass_off[c]
+// (null = nothing to add); out: [B][2][nl or nl-1][N].
+__global__ void k_moddown(uint64_t* __restrict__ out, const uint64_t* __restrict__ acc,
+                          const uint64_t* __restrict__ pass, long long pass_stride, long long pass_off_a,
+                          long long pass_off_b, int use_pass_a, int use_pass_b, const __grid_constant__ ModDownConsts mc,
+                          const PrimeInfo* __restrict__ primes, int nl, int rescale, long long N) {
+    const int by = blockIdx.y;
+    const int b = by >> 1, c = by & 1;
+    const int ne = nl + 1;
+    const int nout = rescale ? nl - 1 : nl;
+    const uint64_t* a = acc + ((long long)b * 2 + c) * ne * N;
+    uint64_t* o = out + ((long long)b * 2 + c) * nout * N;
+    const int use_pass = c == 0 ? use_pass_a : use_pass_b;
+    const uint64_t* ps = use_pass ? pass + (long long)b * pass_stride + (c == 0 ? pass_off_a : pass_off_b) : nullptr;
+    const PrimeInfo psp = primes[mc.special];
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+         x += (long long)gridDim.x * blockDim.x) {
+        const uint64_t t = add_mod(a[(long long)nl * N + x], mc.half_p, mc.p);
+        // value of limb i after the special-prime division and the pass-through add
+        auto limb = [&](int i) -> uint64_t {
+            const PrimeInfo& pi = primes[mc.prime[i]];
+            uint64_t v = add_mod(a[(long long)i * N + x], mc.half_sp[i], pi.q);
+            v = sub_mod(v, reduce64(t, pi), pi.q);
+            v = shoup(v, mc.inv_sp[i], mc.inv_sp_sh[i], pi.q);
+            if (ps) v = add_mod(v, ps[(long long)i * N + x], pi.q);
+            return v;
+        };
+        if (!rescale) {
+            for (int i = 0; i < nl; ++i) o[(long long)i * N + x] = limb(i);
+        } else {
+            const uint64_t t2 = add_mod(limb(nl - 1), mc.half_top, mc.q_top);
+            for (int i = 0; i < nl - 1; ++i) {
+                const PrimeInfo& pi = primes[mc.prime[i]];
+                uint64_t v = add_mod(limb(i), mc.half_r[i], pi.q);
+                v = sub_mod(v, reduce64(t2, pi), pi.q);
+                o[(long long)i * N + x] = shoup(v, mc.inv_r[i], mc.inv_r_sh[i], pi.q);
+            }
+        }
+    }
+    (void)psp;
+}
+
+// Galois permutation of both components, per-ciphertext generator (rns_polynomial.c:996-1035).
+__global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __restrict__ in,
+                                const uint64_t* __restrict__ gens, const __grid_constant__ LimbPrimes lp,
+                                const PrimeInfo* __restrict__ primes, int L, long long N, int log_split) {
+    const int by = blockIdx.y;  // (b, c, k)
+    const int k = by % L;
+    const int bc = by / L;
+    const int b = bc >> 1;
+    const uint64_t q = primes[lp.p[k]].q;
+    const uint64_t gen = gens[b];
+    const uint64_t* src = in + ((long long)bc * L + k) * N;
+    uint64_t* dst = out + ((long long)bc * L + k) * N;
+    const uint64_t split = 1ULL << log_split;
+    const uint64_t P = (uint64_t)N >> log_split;
+    for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < N;
+         pos += (long long)gridDim.x * blockDim.x) {
+        const uint64_t i = (uint64_t)pos / P, i2 = (uint64_t)pos % P;
+        const uint64_t idx = (i + (i2 << log_split)) * gen;
+        const uint64_t d = (idx & (split - 1)) * P + ((idx & ((uint64_t)N - 1)) >> log_split);
+        const uint64_t v = src[pos];
+        dst[d] = (idx & (uint64_t)N) ? neg_mod(v, q) : v;
+    }
+}
+
+// Grid for one launch of a per-coefficient kernel; every call site launches exactly
+// one kernel with it, so it also counts the launch.
+dim3 grid_xy(long long n, long long y) {
+    note_launch();
+    long long blocks = (n + 255) / 256;
+    if (blocks > 64) blocks = 64;
+    if (blocks < 1) blocks = 1;
+    return dim3((unsigned)blocks, (unsigned)y, 1);
+}
+
+bool check_shape(IncNtt* t, const uint32_t* limbs, uint32_t L, uint32_t special, const char* where) {
+    if (!t || !limbs || L == 0 || L + 1 > (uint32_t)kMaxLimbs) {
+        set_error(where, "bad pool or limb list (1 <= nlimbs <= 63)");
+        return false;
+    }
+    for (uint32_t k = 0; k < L; ++k)
+        if (limbs[k] >= t->pub.l) {
+            set_error(where, "limb index outside the pool");
+            return false;
+        }
+    if (special >= t->pub.l) {
+        set_error(where, "special prime outside the pool");
+        return false;
+    }
+    return true;
+}
+
+// Forward transforms of every digit: D[b][j][i] = NTT(d_j mod q_i), reading digit
+// rows from src (limb j at src + j N, polynomials src_stride apart).
+int digits_forward(IncNtt* t, uint64_t* D, const uint64_t* src, long long src_stride, uint64_t B,
+                   const uint32_t* ext, int nd, int ne, cudaStream_t st) {
+    const long long N = (long long)t->pub.N;
+    for (int j = 0; j < nd; ++j) {
+        RowSet rs;
+        memset(&rs, 0, sizeof rs);
+        for (int i = 0; i < ne; ++i) {
+            rs.in[i] = src + (long long)j * N;
+            rs.out[i] = D + ((long long)j * ne + i) * N;
+            rs.prime[i] = ext[i];
+        }
+        rs.nlimbs = ne;
+        rs.split = (int)t->pub.split_degree;
+        rs.logP = t->logP;
+        rs.batch = (int)B;
+        rs.batch_stride = (long long)nd * ne * N;
+        rs.in_batch_stride = src_stride;
+        rs.reduce_input = 1;
+        const int e = launch_ntt(rs, t->d_info, false, st);
+        if (e) return e;
+    }
+    return 0;
+}
+
+// In-place transform of `count` consecutive [nl][N] blocks with the given limb primes.
+int blocks_transform(IncNtt* t, uint64_t* data, uint64_t count, const uint32_t* lim, int nl, bool inverse,
+                     cudaStream_t st) {
+    const long long N = (long long)t->pub.N;
+    RowSet rs;
+    memset(&rs, 0, sizeof rs);
+    for (int i = 0; i < nl; ++i) {
+        rs.in[i] = data + (long long)i * N;
+        rs.out[i] = data + (long long)i * N;
+        rs.prime[i] = lim[i];
+    }
+    rs.nlimbs = nl;
+    rs.split = (int)t->pub.split_degree;
+    rs.logP = t->logP;
+    rs.batch = (int)count;
+    rs.batch_stride = (long long)nl * N;
+    rs.in_batch_stride = rs.batch_stride;
+    return launch_ntt(rs, t->d_info, inverse, st);
+}
+
+ModDownConsts moddown_consts(IncNtt* t, const uint32_t* limbs, int nl, uint32_t special) {
+    ModDownConsts mc;
+    memset(&mc, 0, sizeof mc);
+    const uint64_t p = t->info[special].q;
+    mc.special = special;
+    mc.p = p;
+    mc.half_p = p / 2;
+    const uint64_t qt = t->info[limbs[nl - 1]].q;
+    mc.q_top = qt;
+    mc.half_top = qt / 2;
+    for (int i = 0; i < nl; ++i) {
+        const uint64_t q = t->info[limbs[i]].q;
+        mc.prime[i] = limbs[i];
+        mc.half_sp[i] = (p / 2) % q;
+        mc.inv_sp[i] = host_inv_mod(p % q, q);
+        mc.inv_sp_sh[i] = host_shoup(mc.inv_sp[i], q);
+        mc.half_r[i] = (qt / 2) % q;
+        mc.inv_r[i] = host_inv_mod(qt % q, q);
+        mc.inv_r_sh[i] = host_shoup(mc.inv_r[i], q);
+    }
+    return mc;
+}
+
+}  // namespace
+
+uint64_t ckks_mul_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
+    const uint64_t ne = L + 1;
+    return B * N * (3 * L + L * ne + 2 * ne) + 2 * B + 64;
+}
+
+uint64_t ckks_rot_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
+    const uint64_t ne = L + 1;
+    return B * N * (2 * L + L * ne + 2 * ne) + 2 * B + 64;
+}
+
+int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const uint64_t* ct2, uint64_t B,
+                           const uint32_t* limbs, uint32_t L, uint32_t special, const uint64_t* rlk,
+                           uint64_t* ws, cudaStream_t st) {
+    const char* where = "vfhe_cuda_ckks_mul_relin_rescale_batch";
+    if (!check_shape(t, limbs, L, special, where)) return 1;
+    if (L < 2) {
+        set_error(where, "rescaling needs at least two limbs");
+        return 1;
+    }
+    const long long N = (long long)t->pub.N;
+    const int nl = (int)L, ne = nl + 1;
+    uint32_t ext[kMaxLimbs];
+    for (int i = 0; i < nl; ++i) ext[i] = limbs[i];
+    ext[nl] = special;
+    LimbPrimes lp, lpe;
+    memset(&lp, 0, sizeof lp);
+    memset(&lpe, 0, sizeof lpe);
+    for (int i = 0; i < nl; ++i) lp.p[i] = limbs[i];
+    for (int i = 0; i < ne; ++i) lpe.p[i] = ext[i];
+
+    uint64_t* T = ws;                                   // [B][3][L][N]
+    uint64_t* D = T + B * 3 * nl * N;                   // [B][L][ne][N]
+    uint64_t* acc = D + B * (uint64_t)nl * ne * N;      // [B][2][ne][N]
+    uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
+
+    std::vector<const uint64_t*> kp(B, rlk);
+    if (!check_cuda(cudaMemcpyAsync(keyptrs, kp.data(), B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where))
+        return 1;
+    k_tensor<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
+    if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
+    k_mac<<<grid_xy(N, (long long)B * ne), 256, 0, st>>>(acc, D, (const uint64_t* const*)keyptrs, lpe, t->d_info,
+                                                          nl, ne, N);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
+    const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
+    k_moddown<<<grid_xy(N, (long long)B * 2), 256, 0, st>>>(out, acc, T, 3LL * nl * N, (long long)nl * N,
+                                                            2LL * nl * N, 1, 1, mc, t->d_info, nl, 1, N);
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const uint32_t* limbs, uint32_t L,
+                uint32_t special, const uint64_t* gens, const uint64_t* const* gks, uint64_t* ws, cudaStream_t st) {
+    const char* where = "vfhe_cuda_ckks_rotate_batch";
+    if (!check_shape(t, limbs, L, special, where)) return 1;
+    const long long N = (long long)t->pub.N;
+    for (uint64_t b = 0; b < B; ++b)
+        if ((gens[b] & 1) == 0 || gens[b] >= 2 * (uint64_t)N) {
+            set_error(where, "Galois elements must be odd and below 2N");
+            return 1;
+        }
+    const int nl = (int)L, ne = nl + 1;
+    uint32_t ext[kMaxLimbs];
+    for (int i = 0; i < nl; ++i) ext[i] = limbs[i];
+    ext[nl] = special;
+    LimbPrimes lp, lpe;
+    memset(&lp, 0, sizeof lp);
+    memset(&lpe, 0, sizeof lpe);
+    for (int i = 0; i < nl; ++i) lp.p[i] = limbs[i];
+    for (int i = 0; i < ne; ++i) lpe.p[i] = ext[i];
+    int ls = 0;
+    while ((1ULL << ls) < t->pub.split_degree) ++ls;
+
+    uint64_t* Pm = ws;                                  // [B][2][L][N]
+    uint64_t* D = Pm + B * 2 * nl * N;                  // [B][L][ne][N]
+    uint64_t* acc = D + B * (uint64_t)nl * ne * N;      // [B][2][ne][N]
+    uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
+    uint64_t* d_gens = keyptrs + B;                     // [B]
+    if (!check_cuda(cudaMemcpyAsync(keyptrs, gks, B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where) ||
+        !check_cuda(cudaMemcpyAsync(d_gens, gens, B * sizeof(uint64_t), cudaMemcpyHostToDevice, st), where))
+        return 1;
+    k_permute_batch<<<grid_xy(N, (long long)B * 2 * nl), 256, 0, st>>>(Pm, ct, d_gens, lp, t->d_info, nl, N, ls);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(digits_forward(t, D, Pm, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
+    k_mac<<<grid_xy(N, (long long)B * ne), 256, 0, st>>>(acc, D, (const uint64_t* const*)keyptrs, lpe, t->d_info,
+                                                          nl, ne, N);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
+    const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
+    k_moddown<<<grid_xy(N, (long long)B * 2), 256, 0, st>>>(out, acc, Pm, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
+                                                            mc, t->d_info, nl, 0, N);
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+}  // namespace vc

@@ -37,13 +37,18 @@ __global__ void __launch_bounds__(1024) k_ntt_pass(const __grid_constant__ RowSe
     const PrimeInfo* pi = primes + rows.prime[slot];
     const uint64_t q = pi->q;
     const uint64_t q2 = pi->two_q;
-    const long long off = b * rows.batch_stride + (long long)blk * P;
-    const uint64_t* __restrict__ src = rows.in[slot] + off;
-    uint64_t* __restrict__ dst = rows.out[slot] + off;
+    const long long off = (long long)blk * P;
+    const uint64_t* __restrict__ src = rows.in[slot] + b * rows.in_batch_stride + off;
+    uint64_t* __restrict__ dst = rows.out[slot] + b * rows.batch_stride + off;
 
     const int base = (hi << (bit_lo + k)) + (cb << logC);
-    for (int e = threadIdx.x; e < T; e += blockDim.x) {
-        tile[e] = src[base + ((e >> logC) << bit_lo) + (e & (C - 1))];
+    if (rows.reduce_input && !INV) {
+        const PrimeInfo pr = *pi;
+        for (int e = threadIdx.x; e < T; e += blockDim.x)
+            tile[e] = reduce64(src[base + ((e >> logC) << bit_lo) + (e & (C - 1))], pr);
+    } else {
+        for (int e = threadIdx.x; e < T; e += blockDim.x)
+            tile[e] = src[base + ((e >> logC) << bit_lo) + (e & (C - 1))];
     }
     __syncthreads();
 
@@ -115,6 +120,7 @@ int run_pass(const RowSet& rows, const PrimeInfo* d_primes, int bit_lo, int k, i
     if (threads < 32) threads = 32;
     k_ntt_pass<INV><<<(unsigned)grid, threads, smem, stream>>>(rows, d_primes, bit_lo, k, logC,
                                                               last ? 1 : 0);
+    note_launch();
     return (int)cudaGetLastError();
 }
 
@@ -132,9 +138,11 @@ int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cuda
     const int k_lo = 12;
     const int k_hi = logP - k_lo;
     const int logC = k_lo - k_hi;
+    // the second pass works in place on the first pass's output
     RowSet second = rows;
-    second.in[0] = nullptr;  // placeholder; fixed up below
     for (int i = 0; i < rows.nlimbs; ++i) second.in[i] = rows.out[i];
+    second.in_batch_stride = rows.batch_stride;
+    second.reduce_input = 0;
     int err;
     if (!inverse) {
         err = run_pass<false>(rows, d_primes, k_lo, k_hi, logC, false, stream);

@@ -26,8 +26,11 @@ constexpr int kMaxLimbs = 64;
 // A set of rows (one row = one P-point transform) described compactly.
 // Row r of the launch maps to (poly b, limb slot k, block blk):
 //   r = (b * nlimbs + k) * split + blk
-//   in  = in_base[k]  + b * batch_stride + blk * P
-//   out = out_base[k] + b * batch_stride + blk * P
+//   in  = in_base[k]  + b * in_batch_stride + blk * P
+//   out = out_base[k] + b * batch_stride    + blk * P
+// With reduce_input set, a forward transform first reduces each loaded residue
+// modulo its row's prime (the digit broadcast of a key switch: the input row holds
+// residues of another prime, rns_polynomial.c:824-843).
 struct RowSet {
     uint64_t* out[kMaxLimbs];
     const uint64_t* in[kMaxLimbs];
@@ -36,11 +39,16 @@ struct RowSet {
     int split;
     int logP;
     int batch;
-    long long batch_stride;  // in elements
+    long long batch_stride;     // output stride between polynomials, in elements
+    long long in_batch_stride;  // input stride between polynomials, in elements
+    int reduce_input;
 };
 
 // Launch the forward (inverse=false) or inverse transform of every row in `rows`.
 // Work is enqueued on `stream`; returns a cudaError_t code (0 on success).
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
+
+// Count of kernels this engine has launched (vfhe_cuda_launch_count).
+void note_launch(int n = 1);
 
 }  // namespace vc

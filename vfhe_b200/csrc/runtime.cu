@@ -4,6 +4,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <map>
 #include <string>
 
@@ -414,8 +415,17 @@ void poly_destroy(Poly* p) {
 
 }  // namespace vc
 
+namespace vc {
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+}  // namespace vc
+
 // ---------------------------------------------------------------- status ABI
 extern "C" {
+
+uint64_t vfhe_cuda_launch_count(void) { return vc::g_launches.load(); }
 
 int vfhe_cuda_status(void) { return vc::g_status; }
 
