@@ -126,9 +126,30 @@ int run_pass(const RowSet& rows, const PrimeInfo* d_primes, int bit_lo, int k, i
 
 }  // namespace
 
+int launch_ntt_rb(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
+
+namespace {
+// The register-blocked kernels use 16-byte vector accesses on row segments.
+bool rows_aligned16(const RowSet& rows) {
+    if ((rows.batch_stride | rows.in_batch_stride) & 1) return false;
+    for (int k = 0; k < rows.nlimbs; ++k)
+        if ((((uintptr_t)rows.out[k]) | ((uintptr_t)rows.in[k])) & 15) return false;
+    return true;
+}
+int g_force_generic = -1;
+}  // namespace
+
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream) {
     const int logP = rows.logP;
     if (rows.batch <= 0 || rows.nlimbs <= 0) return 0;
+    if (g_force_generic < 0) {
+        const char* s = getenv("VFHE_CUDA_NTT_GENERIC");
+        g_force_generic = (s && atoi(s)) ? 1 : 0;
+    }
+    if (!g_force_generic && logP >= 8 && logP <= 17 && rows_aligned16(rows)) {
+        const int e = launch_ntt_rb(rows, d_primes, inverse, stream);
+        if (e != -1) return e;
+    }
     if (logP <= 14) {
         return inverse ? run_pass<true>(rows, d_primes, 0, logP, 0, true, stream)
                        : run_pass<false>(rows, d_primes, 0, logP, 0, true, stream);
