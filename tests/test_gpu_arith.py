@@ -56,6 +56,31 @@ def test_forward_inverse(rings):
     same(g, o)
 
 
+@pytest.mark.parametrize("bits", [30, 40, 45, 49, 50])
+@pytest.mark.parametrize("logn", [8, 10, 12, 13, 14, 15, 16, 17])
+def test_transform_prime_sizes_and_extremes(engines, bits, logn):
+    """Every transform schedule (one tile, column + tile) and both butterfly arithmetics
+    at the edges of their ranges: primes just below 2^bits and residues at 0 and q-1."""
+    rings = twin_rings(engines, 1 << logn, [bits], 1)
+    q = rings[0].primes[0]
+    rng = np.random.default_rng(logn * 100 + bits)
+    N = 1 << logn
+    cases = [
+        np.full((1, N), q - 1, dtype=np.uint64),
+        np.tile(np.array([0, q - 1], dtype=np.uint64), N // 2)[None, :],
+        rng.integers(0, q, (1, N), dtype=np.uint64),
+    ]
+    for rows in cases:
+        g, o = poly_from_rows(rings[0], rows), poly_from_rows(rings[1], rows)
+        g.to_NTT()
+        o.to_NTT()
+        same(g, o)
+        g2, o2 = poly_from_rows(rings[0], rows, repr.ntt), poly_from_rows(rings[1], rows, repr.ntt)
+        g2.to_coeff()
+        o2.to_coeff()
+        same(g2, o2)
+
+
 def test_round_trip_identity(rings):
     rng = np.random.default_rng(2)
     rows = uniform_rows(rings[0], rng)

@@ -14,6 +14,7 @@ from .test_gpu_arith import (  # noqa: F401  (re-collected here with other engin
     test_permute,
     test_round_trip_identity,
     test_scaled_lift_and_base_extension,
+    test_transform_prime_sizes_and_extremes,
 )
 
 CPU_RINGS = [

@@ -68,6 +68,7 @@ inline int poly_ntt(Poly* out, Poly* in, uint64_t mask, bool inverse) {
     rs.logP = t->logP;
     rs.batch = 1;
     rs.batch_stride = 0;
+    mark_fp64(rs, t);
     return launch_ntt(rs, t->d_info, inverse, stream());
 }
 

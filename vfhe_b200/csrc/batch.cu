@@ -73,6 +73,7 @@ int vfhe_cuda_ntt_batch(void* ntt, int inverse, uint64_t* d_out, const uint64_t*
     if (!vc::ensure_ready()) return 1;
     RowSet rs;
     if (!batch_rowset(as_ntt(ntt), d_out, d_in, batch, limbs, nlimbs, &rs, "vfhe_cuda_ntt_batch")) return 1;
+    mark_fp64(rs, as_ntt(ntt));
     const int e = launch_ntt(rs, as_ntt(ntt)->d_info, inverse != 0, (cudaStream_t)stream_);
     return check_cuda(e, "vfhe_cuda_ntt_batch") ? 0 : 1;
 }

@@ -208,6 +208,7 @@ int digits_forward(IncNtt* t, uint64_t* D, const uint64_t* src, long long src_st
         rs.batch_stride = (long long)nd * ne * N;
         rs.in_batch_stride = src_stride;
         rs.reduce_input = 1;
+        mark_fp64(rs, t);
         const int e = launch_ntt(rs, t->d_info, false, st);
         if (e) return e;
     }
@@ -231,6 +232,7 @@ int blocks_transform(IncNtt* t, uint64_t* data, uint64_t count, const uint32_t* 
     rs.batch = (int)count;
     rs.batch_stride = (long long)nl * N;
     rs.in_batch_stride = rs.batch_stride;
+    mark_fp64(rs, t);
     return launch_ntt(rs, t->d_info, inverse, st);
 }
 

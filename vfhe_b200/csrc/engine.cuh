@@ -96,6 +96,14 @@ inline IncNtt* as_ntt(void* p) { return reinterpret_cast<IncNtt*>(p); }
 inline Poly* as_poly(void* p) { return reinterpret_cast<Poly*>(p); }
 inline RNS_MLWE as_mlwe(void* p) { return reinterpret_cast<RNS_MLWE>(p); }
 
+// Allow the FP64 butterfly kernels for a row set when all its primes are below 2^50.
+inline void mark_fp64(RowSet& rs, const IncNtt* t) {
+    int ok = 1;
+    for (int k = 0; k < rs.nlimbs; ++k)
+        if (!t->info[rs.prime[k]].fp64) ok = 0;
+    rs.fp64 = ok;
+}
+
 IncNtt* ntt_create(const uint64_t* primes, uint64_t split, uint64_t N, uint64_t count);
 bool ntt_extend(IncNtt* t, const uint64_t* primes, uint64_t count);
 Poly* poly_create(uint64_t N, uint64_t mask, IncNtt* t);

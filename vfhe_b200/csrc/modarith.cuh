@@ -32,7 +32,14 @@ struct PrimeInfo {
     const uint64_t* fwd;     // P twiddles psi^brv(i), Shoup companions interleaved: [w, w']
     const uint64_t* inv;     // P twiddles psi^-brv(i), interleaved the same way
     const uint64_t* twist;   // P values psi^(2 brv(k) + 1), interleaved [w, w']
-    const double* fwd_f;     // reserved for the FP64 butterfly path (may be null)
+    // FP64 butterfly path (q < 2^50 only, fp64 != 0): twiddles centred to |w| <= q/2
+    // and interleaved with fl(w/q); constants as (centred value, fl(value/q)).
+    const double* fwd_d;
+    const double* inv_d;
+    double qd, qinv;
+    double pinv_d, pinv_q;
+    double ilast_d, ilast_q;
+    int fp64;
 };
 
 VC_HD uint64_t umulhi(uint64_t a, uint64_t b) {

@@ -127,6 +127,7 @@ int run_pass(const RowSet& rows, const PrimeInfo* d_primes, int bit_lo, int k, i
 }  // namespace
 
 int launch_ntt_rb(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
+int launch_ntt_f64(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
 
 namespace {
 // The register-blocked kernels use 16-byte vector accesses on row segments.
@@ -137,6 +138,7 @@ bool rows_aligned16(const RowSet& rows) {
     return true;
 }
 int g_force_generic = -1;
+int g_force_int = -1;
 }  // namespace
 
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream) {
@@ -146,7 +148,15 @@ int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cuda
         const char* s = getenv("VFHE_CUDA_NTT_GENERIC");
         g_force_generic = (s && atoi(s)) ? 1 : 0;
     }
+    if (g_force_int < 0) {
+        const char* s = getenv("VFHE_CUDA_NTT_INT");
+        g_force_int = (s && atoi(s)) ? 1 : 0;
+    }
     if (!g_force_generic && logP >= 8 && logP <= 17 && rows_aligned16(rows)) {
+        if (rows.fp64 && !g_force_int) {
+            const int e = launch_ntt_f64(rows, d_primes, inverse, stream);
+            if (e != -1) return e;
+        }
         const int e = launch_ntt_rb(rows, d_primes, inverse, stream);
         if (e != -1) return e;
     }

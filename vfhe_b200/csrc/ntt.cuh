@@ -42,6 +42,8 @@ struct RowSet {
     long long batch_stride;     // output stride between polynomials, in elements
     long long in_batch_stride;  // input stride between polynomials, in elements
     int reduce_input;
+    // set by launch_ntt when every prime of the set is below 2^50 (FP64 butterflies)
+    int fp64;
 };
 
 // Launch the forward (inverse=false) or inverse transform of every row in `rows`.

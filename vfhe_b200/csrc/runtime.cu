@@ -276,13 +276,27 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
         tw[2 * kk] = w;
         tw[2 * kk + 1] = host_shoup(w, q);
     }
+    // FP64 twiddles: centred w and fl(w / q) (see fp64mod.cuh for why this is exact)
+    const bool fp64 = q < (1ULL << 50);
+    std::vector<double> fwd_d(2 * P), inv_d(2 * P);
+    auto centred = [q](uint64_t v) -> double {
+        return v > q / 2 ? -(double)(q - v) : (double)v;
+    };
+    for (uint64_t i = 0; i < P && fp64; ++i) {
+        fwd_d[2 * i] = centred(fwd[2 * i]);
+        fwd_d[2 * i + 1] = fwd_d[2 * i] / (double)q;
+        inv_d[2 * i] = centred(inv[2 * i]);
+        inv_d[2 * i + 1] = inv_d[2 * i] / (double)q;
+    }
     void* blk = nullptr;
-    const size_t bytes = sizeof(uint64_t) * 6 * P;
+    const size_t bytes = sizeof(uint64_t) * 10 * P;
     if (!check_cuda(cudaMalloc(&blk, bytes), "table alloc")) return false;
     uint64_t* d = (uint64_t*)blk;
     if (!check_cuda(cudaMemcpy(d, fwd.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
         !check_cuda(cudaMemcpy(d + 2 * P, inv.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
-        !check_cuda(cudaMemcpy(d + 4 * P, tw.data(), 16 * P, cudaMemcpyHostToDevice), "table upload"))
+        !check_cuda(cudaMemcpy(d + 4 * P, tw.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
+        !check_cuda(cudaMemcpy(d + 6 * P, fwd_d.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
+        !check_cuda(cudaMemcpy(d + 8 * P, inv_d.data(), 16 * P, cudaMemcpyHostToDevice), "table upload"))
         return false;
     t->dev_blocks.push_back(blk);
 
@@ -302,7 +316,15 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
     o.fwd = d;
     o.inv = d + 2 * P;
     o.twist = d + 4 * P;
-    o.fwd_f = nullptr;
+    o.fwd_d = reinterpret_cast<const double*>(d + 6 * P);
+    o.inv_d = reinterpret_cast<const double*>(d + 8 * P);
+    o.fp64 = fp64 ? 1 : 0;
+    o.qd = (double)q;
+    o.qinv = 1.0 / (double)q;
+    o.pinv_d = centred(o.p_inv);
+    o.pinv_q = o.pinv_d / (double)q;
+    o.ilast_d = centred(o.inv_last);
+    o.ilast_q = o.ilast_d / (double)q;
     return true;
 }
 
