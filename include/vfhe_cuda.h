@@ -301,6 +301,22 @@ int vfhe_cuda_poly_mul_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a, co
 int vfhe_cuda_ntt_mul_intt_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
                                  uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
 
+/* Same result as vfhe_cuda_ntt_mul_intt_batch, for callers that cannot let a library
+ * allocate GPU memory: code building a CUDA graph by stream capture, host runtimes
+ * (a JVM or Go service, say) that own the device memory through their own allocator,
+ * and serving loops that cannot afford an allocation's device synchronisation.  It
+ * calls no cudaMalloc, cudaFree or other allocating routine: its scratch is a static
+ * device array of 2^20 residues (8 MiB) inside the library, which every GPU that loads
+ * the library holds until the process exits.  batch * nlimbs * N must not exceed 2^20;
+ * larger requests are rejected (nonzero return, vfhe_cuda_last_error says why).  The
+ * first call on a device resolves the array's device address on that device, so make
+ * it before any stream capture.  All calls share the one array: calls whose work
+ * overlaps on the GPU (different streams, or a second call before the first has
+ * finished on another stream) race on it.  Call with the engine's device current.
+ * No counterpart in the reference. */
+int vfhe_cuda_ntt_mul_intt_batch_noalloc(void *ntt, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
+                                         uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
+
 /* CKKS evaluation over device-resident ciphertexts.
  *
  * A ciphertext at level with L active limbs is [2][L][N] uint64: component 0 is a,

@@ -21,15 +21,15 @@ Context& ctx() {
 namespace {
 std::mutex g_err_mu;
 int g_status = 0;
-std::string g_error;
+char g_error[512];  // fixed buffer: recording an error never allocates
 }  // namespace
 
 void set_error(const char* where, const char* what) {
     std::lock_guard<std::mutex> lk(g_err_mu);
     if (g_status == 0) {
         g_status = 1;
-        g_error = std::string(where) + ": " + what;
-        if (getenv("VFHE_CUDA_QUIET") == nullptr) fprintf(stderr, "vfhe cuda engine: %s\n", g_error.c_str());
+        snprintf(g_error, sizeof g_error, "%s: %s", where, what);
+        if (getenv("VFHE_CUDA_QUIET") == nullptr) fprintf(stderr, "vfhe cuda engine: %s\n", g_error);
     }
 }
 
@@ -451,12 +451,12 @@ uint64_t vfhe_cuda_launch_count(void) { return vc::g_launches.load(); }
 
 int vfhe_cuda_status(void) { return vc::g_status; }
 
-const char* vfhe_cuda_last_error(void) { return vc::g_error.c_str(); }
+const char* vfhe_cuda_last_error(void) { return vc::g_error; }
 
 void vfhe_cuda_clear_error(void) {
     std::lock_guard<std::mutex> lk(vc::g_err_mu);
     vc::g_status = 0;
-    vc::g_error.clear();
+    vc::g_error[0] = '\0';
 }
 
 int vfhe_cuda_device(void) {
