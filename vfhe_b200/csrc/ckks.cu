@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "abi_common.cuh"
+#include "fp64mod.cuh"
 
 namespace vc {
 
@@ -67,6 +68,32 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
     const uint64_t* kb = ka + dstride;
     uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
     uint64_t* ob = oa + dstride;
+    if (pi.fp64) {
+        // Exact FP64 multiply-accumulate (fp64mod.cuh): each term is y k - n q with
+        // |term| <= 3q/4 for canonical y, k < q (k/q formed as fl(k) fl(1/q), whose
+        // 2^-52 relative error only moves the quotient estimate); partial sums are
+        // brought back below q every four digits so they stay exact (< 2^52).
+        const double q = pi.qd, qinv = pi.qinv;
+        for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+             x += (long long)gridDim.x * blockDim.x) {
+            double sa = 0.0, sb = 0.0;
+            for (int j = 0; j < nd; ++j) {
+                const double v = f_from_u64(d[j * dstride + x]);
+                const double wa = f_from_u64(ka[j * kstride + x]);
+                const double wb = f_from_u64(kb[j * kstride + x]);
+                sa = __dadd_rn(sa, f_mulmod(v, wa, __dmul_rn(wa, qinv), q));
+                sb = __dadd_rn(sb, f_mulmod(v, wb, __dmul_rn(wb, qinv), q));
+                if ((j & 3) == 3) {
+                    sa = f_reduce(sa, q, qinv);
+                    sb = f_reduce(sb, q, qinv);
+                }
+            }
+            // -sum, canonical
+            oa[x] = f_to_canonical(-sa, q, qinv, pi.q);
+            ob[x] = f_to_canonical(-sb, q, qinv, pi.q);
+        }
+        return;
+    }
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
          x += (long long)gridDim.x * blockDim.x) {
         uint64_t sa = 0, sb = 0;

@@ -32,16 +32,50 @@ struct FCtx {
     const double2* tw;
 };
 
+// Twiddles of one pass.  In the field at LO, the butterfly of residue m at tile bit
+// b = LO + bb uses index (... + (i >> (b+1))), which depends on m only through
+// h = m >> (bb+1): stage bb needs 2^(3-bb) twiddles, a 4-stage pass 15.  Descending
+// (forward) stages are stored first-stage-first; ascending (inverse) the same way.
+template <int LO, int BFROM, int BTO>
+struct PassTw {
+    __host__ __device__ static constexpr int count() {
+        int n = 0;
+        for (int b = BFROM;; b += (BTO >= BFROM ? 1 : -1)) {
+            n += 1 << (3 - (b - LO));
+            if (b == BTO) break;
+        }
+        return n;
+    }
+    // offset of stage b's twiddles
+    __host__ __device__ static constexpr int offset(int bq) {
+        int n = 0;
+        for (int b = BFROM; b != bq; b += (BTO >= BFROM ? 1 : -1)) n += 1 << (3 - (b - LO));
+        return n;
+    }
+    double2 w[count()];
+};
+
 template <int K, int LO, int BHI, int BLO>
-__device__ __forceinline__ void f_fwd_bits(double (&x)[16], int t, int hi, int logP, const FCtx& c) {
+__device__ __forceinline__ void f_fwd_tw(PassTw<LO, BHI, BLO>& T, int t, int hi, int logP, const double2* tw) {
 #pragma unroll
     for (int b = BHI; b >= BLO; --b) {
         const int bb = b - LO;
         const int base = (1 << (logP - 1 - b)) + (hi << (K - b - 1));
 #pragma unroll
+        for (int h = 0; h < (1 << (3 - bb)); ++h)
+            T.w[PassTw<LO, BHI, BLO>::offset(b) + h] = __ldg(&tw[base + (own<LO>(t, h << (bb + 1)) >> (b + 1))]);
+    }
+}
+
+template <int K, int LO, int BHI, int BLO>
+__device__ __forceinline__ void f_fwd_bits(double (&x)[16], const PassTw<LO, BHI, BLO>& T, const FCtx& c) {
+#pragma unroll
+    for (int b = BHI; b >= BLO; --b) {
+        const int bb = b - LO;
+#pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & (1 << bb)) continue;
-            const double2 w = __ldg(&c.tw[base + (own<LO>(t, m) >> (b + 1))]);
+            const double2 w = T.w[PassTw<LO, BHI, BLO>::offset(b) + (m >> (bb + 1))];
             const double v = f_mulmod(x[m | (1 << bb)], w.x, w.y, c.q);
             const double u = x[m];
             x[m] = __dadd_rn(u, v);
@@ -55,13 +89,25 @@ __device__ __forceinline__ void f_fwd_bits(double (&x)[16], int t, int hi, int l
 // Inverse stages at bits BLO..BHI of the field at LO.  FINAL: the global last bit folds
 // P^-1 (constants pinv and ilast, centred with their fl(./q) companions).
 template <int K, int LO, int BLO, int BHI, bool FINAL>
-__device__ __forceinline__ void f_inv_bits(double (&x)[16], int t, int hi, int logP, const FCtx& c,
+__device__ __forceinline__ void f_inv_tw(PassTw<LO, BLO, BHI>& T, int t, int hi, int logP, const double2* tw) {
+#pragma unroll
+    for (int b = BLO; b <= BHI; ++b) {
+        if (FINAL && b == BHI) break;  // the last stage uses the P^-1 constants
+        const int bb = b - LO;
+        const int base = ((1 << logP) >> (b + 1)) + (hi << (K - b - 1));
+#pragma unroll
+        for (int h = 0; h < (1 << (3 - bb)); ++h)
+            T.w[PassTw<LO, BLO, BHI>::offset(b) + h] = __ldg(&tw[base + (own<LO>(t, h << (bb + 1)) >> (b + 1))]);
+    }
+}
+
+template <int K, int LO, int BLO, int BHI, bool FINAL>
+__device__ __forceinline__ void f_inv_bits(double (&x)[16], const PassTw<LO, BLO, BHI>& T, const FCtx& c,
                                            const PrimeInfo& pi) {
 #pragma unroll
     for (int b = BLO; b <= BHI; ++b) {
         const int bb = b - LO;
         const int j = b - BLO;  // stage index within this pass
-        const int base = ((1 << logP) >> (b + 1)) + (hi << (K - b - 1));
         const bool last = FINAL && b == BHI;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
@@ -71,7 +117,7 @@ __device__ __forceinline__ void f_inv_bits(double (&x)[16], int t, int hi, int l
                 x[m] = f_mulmod(__dadd_rn(u, v), pi.pinv_d, pi.pinv_q, c.q);
                 x[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), pi.ilast_d, pi.ilast_q, c.q);
             } else {
-                const double2 w = __ldg(&c.tw[base + (own<LO>(t, m) >> (b + 1))]);
+                const double2 w = T.w[PassTw<LO, BLO, BHI>::offset(b) + (m >> (bb + 1))];
                 x[m] = __dadd_rn(u, v);
                 x[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), w.x, w.y, c.q);
             }
@@ -161,25 +207,35 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
     constexpr int L2 = (K - 8) > 0 ? (K - 8) : 0;
     constexpr int L3 = (K - 12) > 0 ? (K - 12) : 0;
     const bool red = rows.reduce_input != 0;
+    // each pass's twiddles are requested before the exchange that precedes the pass,
+    // so their latency overlaps the barrier
+    PassTw<L1, K - 1, L1> tw1;
+    f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c.tw);
 #pragma unroll
     for (int m = 0; m < 16; ++m) x[m] = load_in(r.src + own<L1>(t, m), IN_D, red, c);
-    f_fwd_bits<K, L1, K - 1, L1>(x, t, hi, logP, c);
+    f_fwd_bits<K, L1, K - 1, L1>(x, tw1, c);
+    PassTw<L2, L1 - 1, L2> tw2;
+    f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c.tw);
     fput<L1>(sm, x, t);
     __syncthreads();
     fget<L2>(x, sm, t);
-    f_fwd_bits<K, L2, L1 - 1, L2>(x, t, hi, logP, c);
+    f_fwd_bits<K, L2, L1 - 1, L2>(x, tw2, c);
     if constexpr (L2 > 0) {
+        PassTw<L3, L2 - 1, L3> tw3;
+        f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c.tw);
         __syncthreads();
         fput<L2>(sm, x, t);
         __syncthreads();
         fget<L3>(x, sm, t);
-        f_fwd_bits<K, L3, L2 - 1, L3>(x, t, hi, logP, c);
+        f_fwd_bits<K, L3, L2 - 1, L3>(x, tw3, c);
         if constexpr (L3 > 0) {
+            PassTw<0, L3 - 1, 0> tw4;
+            f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c.tw);
             __syncthreads();
             fput<L3>(sm, x, t);
             __syncthreads();
             fget<0>(x, sm, t);
-            f_fwd_bits<K, 0, L3 - 1, 0>(x, t, hi, logP, c);
+            f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
         }
     }
     ulonglong2* out = reinterpret_cast<ulonglong2*>(r.dst + 16 * t);
@@ -223,27 +279,46 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __gr
         x[m] = f_from_u64(v.x);
         x[m + 1] = f_from_u64(v.y);
     }
-    f_inv_bits<K, 0, 0, 3, false>(x, t, hi, logP, c, pi);
-    fput<0>(sm, x, t);
-    __syncthreads();
-    fget<F1>(x, sm, t);
+    PassTw<0, 0, 3> tw1;
+    f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c.tw);
+    f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
     if constexpr (K <= 8) {
-        f_inv_bits<K, F1, 4, K - 1, FINAL>(x, t, hi, logP, c, pi);
+        PassTw<F1, 4, K - 1> tw2;
+        f_inv_tw<K, F1, 4, K - 1, FINAL>(tw2, t, hi, logP, c.tw);
+        fput<0>(sm, x, t);
+        __syncthreads();
+        fget<F1>(x, sm, t);
+        f_inv_bits<K, F1, 4, K - 1, FINAL>(x, tw2, c, pi);
     } else {
-        f_inv_bits<K, F1, 4, 7, false>(x, t, hi, logP, c, pi);
+        PassTw<F1, 4, 7> tw2;
+        f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c.tw);
+        fput<0>(sm, x, t);
         __syncthreads();
-        fput<F1>(sm, x, t);
-        __syncthreads();
-        fget<F2>(x, sm, t);
+        fget<F1>(x, sm, t);
+        f_inv_bits<K, F1, 4, 7, false>(x, tw2, c, pi);
         if constexpr (K <= 12) {
-            f_inv_bits<K, F2, 8, K - 1, FINAL>(x, t, hi, logP, c, pi);
+            PassTw<F2, 8, K - 1> tw3;
+            f_inv_tw<K, F2, 8, K - 1, FINAL>(tw3, t, hi, logP, c.tw);
+            __syncthreads();
+            fput<F1>(sm, x, t);
+            __syncthreads();
+            fget<F2>(x, sm, t);
+            f_inv_bits<K, F2, 8, K - 1, FINAL>(x, tw3, c, pi);
         } else {
-            f_inv_bits<K, F2, 8, 11, false>(x, t, hi, logP, c, pi);
+            PassTw<F2, 8, 11> tw3;
+            f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c.tw);
+            __syncthreads();
+            fput<F1>(sm, x, t);
+            __syncthreads();
+            fget<F2>(x, sm, t);
+            f_inv_bits<K, F2, 8, 11, false>(x, tw3, c, pi);
+            PassTw<F3, 12, K - 1> tw4;
+            f_inv_tw<K, F3, 12, K - 1, FINAL>(tw4, t, hi, logP, c.tw);
             __syncthreads();
             fput<F2>(sm, x, t);
             __syncthreads();
             fget<F3>(x, sm, t);
-            f_inv_bits<K, F3, 12, K - 1, FINAL>(x, t, hi, logP, c, pi);
+            f_inv_bits<K, F3, 12, K - 1, FINAL>(x, tw4, c, pi);
         }
     }
     constexpr int LAST = K - 4;
