@@ -349,6 +349,24 @@ int vfhe_cuda_ckks_rotate_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct
                                 const uint64_t *gens, const uint64_t *const *d_gks, void *workspace,
                                 void *stream);
 
+/* Batched CGGI16 functional bootstrap with the RNS gadget (CGGI16.functional_bootstrap,
+ * modules/fhe/python/src/vfhe/fhe/cggi16.py:46-128, over mgsw_CMUX, mgsw.c:52-72).
+ * `batch` LWE ciphertexts of dimension n over the L0 (1 or 2) primes limbs[] are
+ * blind-rotated through one bootstrapping key and sample-extracted at coefficient 0.
+ *   d_in_a  [batch][L0][n]   LWE masks      d_in_b  [batch][L0]  LWE bodies
+ *   d_bk    [n][2*L0][2][L0+1][N]  MGSW of each secret coefficient, NTT domain, in the
+ *           order of MGSW_Scheme.encrypt (mgsw.py:18-55): L0 digits of the a row, then L0
+ *           of the b row; extended limbs = limbs[] then `special`
+ *   d_tv    [2][L0][N]       LUT test vector (rank-1 MLWE), coefficient domain
+ *   d_out_a [batch][L0][N]   extracted masks; d_out_b [batch][L0] extracted bodies.
+ * torus_base is the LUT size t (rot_b uses floor(Q / 4t), cggi16.py:65).  The n
+ * rotation steps run as one CUDA graph, captured at the first call per shape. */
+uint64_t vfhe_cuda_cggi_workspace_bytes(void *ntt, uint64_t batch, uint32_t n, uint32_t nlimbs);
+int vfhe_cuda_cggi_bootstrap_batch(void *ntt, uint64_t *d_out_a, uint64_t *d_out_b, const uint64_t *d_in_a,
+                                   const uint64_t *d_in_b, uint64_t batch, uint32_t n, const uint32_t *limbs,
+                                   uint32_t nlimbs, uint32_t special, const uint64_t *d_bk, const uint64_t *d_tv,
+                                   uint64_t torus_base, void *workspace, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,43 @@ class CkksBatch:
         return out
 
 
+class CggiBatch:
+    """Batched CGGI16 functional bootstrap (vfhe_cuda_cggi_bootstrap_batch)."""
+
+    def __init__(self, scheme, engine: Engine | None = None):
+        self.engine = engine or cuda_engine()
+        self.ffi, self.lib = self.engine.ffi, self.engine.lib
+        self.ring = scheme.rings[0]
+        self.special = scheme.special_rings[0].prime_indices[-1]
+        self._limbs = self.ffi.new("uint32_t[]", list(self.ring.prime_indices))
+        self._ws: torch.Tensor | None = None
+
+    def bootstrap(self, lwe_a: torch.Tensor, lwe_b: torch.Tensor, bk: torch.Tensor, tv: torch.Tensor,
+                  torus_base: int, stream=None) -> tuple[torch.Tensor, torch.Tensor]:
+        B, L0, n = lwe_a.shape
+        N = self.ring.N
+        out_a = torch.empty((B, L0, N), dtype=torch.int64, device="cuda")
+        out_b = torch.empty((B, L0), dtype=torch.int64, device="cuda")
+        nbytes = self.lib.vfhe_cuda_cggi_workspace_bytes(self.ring.NTT, B, n, L0)
+        if self._ws is None or self._ws.numel() * 8 < nbytes:
+            self._ws = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device="cuda")
+        st = stream or torch.cuda.current_stream()
+        rc = self.lib.vfhe_cuda_cggi_bootstrap_batch(
+            self.ring.NTT, _ptr(self.ffi, out_a), _ptr(self.ffi, out_b), _ptr(self.ffi, lwe_a), _ptr(self.ffi, lwe_b),
+            B, n, self._limbs, L0, self.special, _ptr(self.ffi, bk), _ptr(self.ffi, tv), torus_base,
+            self.ffi.cast("void*", self._ws.data_ptr()), self.ffi.cast("void*", st.cuda_stream))
+        if rc != 0:
+            self.engine.check("cggi_bootstrap_batch")
+            raise EngineError("cggi_bootstrap_batch")
+        return out_a, out_b
+
+
+def bootstrap_key_tensor(bk) -> torch.Tensor:
+    """Device copy of a CGGI16_Key: [n][2 L0][2][L0+1][N] (MGSW rows in encryption order)."""
+    arr = np.stack([np.stack([np.stack([c.component_rows(0), c.component_rows(1)]) for c in m.obj]) for m in bk.bk])
+    return to_device(arr)
+
+
 def ciphertext_rows(ct: MLWE) -> np.ndarray:
     """[2][L][N] raw rows of a rank-1 ciphertext."""
     return np.stack([ct.component_rows(0), ct.component_rows(1)])

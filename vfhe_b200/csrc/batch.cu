@@ -15,6 +15,10 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
                            cudaStream_t st);
 int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const uint32_t* limbs, uint32_t L,
                 uint32_t special, const uint64_t* gens, const uint64_t* const* gks, uint64_t* ws, cudaStream_t st);
+uint64_t cggi_ws_elems(uint64_t N, uint64_t B, uint64_t n, uint32_t L0);
+int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* in_a, const uint64_t* in_b,
+                   uint64_t B, uint32_t n, const uint32_t* limbs, uint32_t L0, uint32_t special, const uint64_t* bk,
+                   const uint64_t* tv, uint64_t torus_base, uint64_t* ws, cudaStream_t st);
 }  // namespace vc
 
 namespace {
@@ -153,6 +157,25 @@ int vfhe_cuda_ckks_rotate_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct
     if (!ws) ws = engine_workspace(vfhe_cuda_ckks_rotate_workspace_bytes(ntt, batch, nlimbs), st);
     if (!ws) return 1;
     return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, gens, d_gks, ws, st);
+}
+
+uint64_t vfhe_cuda_cggi_workspace_bytes(void* ntt, uint64_t batch, uint32_t n, uint32_t nlimbs) {
+    IncNtt* t = as_ntt(ntt);
+    return t ? 8 * cggi_ws_elems(t->pub.N, batch, n, nlimbs) : 0;
+}
+
+int vfhe_cuda_cggi_bootstrap_batch(void* ntt, uint64_t* d_out_a, uint64_t* d_out_b, const uint64_t* d_in_a,
+                                   const uint64_t* d_in_b, uint64_t batch, uint32_t n, const uint32_t* limbs,
+                                   uint32_t nlimbs, uint32_t special, const uint64_t* d_bk, const uint64_t* d_tv,
+                                   uint64_t torus_base, void* workspace, void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    IncNtt* t = as_ntt(ntt);
+    cudaStream_t st = (cudaStream_t)stream_;
+    uint64_t* ws = (uint64_t*)workspace;
+    if (!ws) ws = engine_workspace(vfhe_cuda_cggi_workspace_bytes(ntt, batch, n, nlimbs), st);
+    if (!ws) return 1;
+    return cggi_bootstrap(t, d_out_a, d_out_b, d_in_a, d_in_b, batch, n, limbs, nlimbs, special, d_bk, d_tv,
+                          torus_base, ws, st);
 }
 
 }  // extern "C"

@@ -1,0 +1,367 @@
+// Batched CGGI16 functional bootstrap with the RNS gadget (the reference's CGGI16:
+// modules/fhe/python/src/vfhe/fhe/cggi16.py:46-128 over mgsw_CMUX / mgsw_external_product,
+// modules/mlwe/c/src/mgsw.c:6-72).
+//
+// For every LWE of the batch (all sharing one bootstrapping key):
+//   rotations  rot_b = round((b + floor(Q / 4t)) 2N / Q) mod 2N,  a_i' = round(a_i 2N / Q) mod 2N
+//              (cggi16.py:56-79; Q = product of the LWE's primes, values by exact CRT)
+//   acc        = tv * X^(2N - rot_b)
+//   step i     acc = CMUX(acc, acc X^(a_i'), bk_i) = acc + ExtProd(bk_i, acc X^(a_i') - acc)
+//   output     sample extraction at coefficient 0 (mlwe.c:40-68)
+// ExtProd: digit d = limb l of component c of the difference, lifted to the key's
+// extended limbs and transformed; accumulated against bk_i[d]; inverse transform;
+// rounded division by the special prime.
+//
+// The accumulator stays in the coefficient domain: the reference transforms the CMUX
+// output forward (mgsw.c:48,67) and the next step back (cggi16.py:84); both maps are
+// exact inverses on canonical residues, so skipping them leaves every bit unchanged.
+// A step with a_i' = 0 (skipped by the reference) adds ExtProd(bk_i, 0) = 0 here.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <vector>
+
+#include "abi_common.cuh"
+#include "fp64mod.cuh"
+
+namespace vc {
+
+namespace {
+
+struct CggiShape {
+    uint32_t lwe_prime[4];   // pool indices of the LWE / accumulator limbs (L0 of them)
+    uint32_t ext_prime[5];   // extended limbs: lwe_prime then the special prime
+    int L0;                  // accumulator limbs
+    int n;                   // LWE dimension
+    long long N;
+};
+
+__device__ __forceinline__ unsigned __int128 crt2(uint64_t r0, uint64_t r1, uint64_t q0, uint64_t q1,
+                                                   uint64_t q0inv_mod_q1, const PrimeInfo& p1) {
+    // v = r0 + q0 * ((r1 - r0) * q0^-1 mod q1)
+    const uint64_t d = sub_mod(r1, r0 % q1, q1);
+    const uint64_t k = mul_mod(d, q0inv_mod_q1, p1);
+    return (unsigned __int128)r0 + (unsigned __int128)q0 * k;
+}
+
+// round(v * 2N / Q) mod 2N for 0 <= v < 2Q; v 2N has no exact half-integer quotient
+// because Q is odd, so round-half-up equals the reference's rounding.
+__device__ __forceinline__ uint32_t rotation(unsigned __int128 v, unsigned __int128 Q, long long N) {
+    const unsigned __int128 num = v * (unsigned __int128)(2 * N);
+    const unsigned __int128 k = (2 * num + Q) / (2 * Q);
+    return (uint32_t)(k % (unsigned __int128)(2 * N));
+}
+
+// rots[i][b] = a_i' and rot0[b] = 2N - rot_b, for L0 = 1 or 2 LWE limbs.
+// a: [B][L0][n], bb: [B][L0].
+__global__ void k_rotations(uint32_t* __restrict__ rots, uint32_t* __restrict__ rot0, const uint64_t* __restrict__ a,
+                            const uint64_t* __restrict__ bb, const __grid_constant__ CggiShape sh,
+                            const PrimeInfo* __restrict__ primes, long long B, uint64_t q0inv, uint64_t offset_lo,
+                            uint64_t offset_hi) {
+    const PrimeInfo p0 = primes[sh.lwe_prime[0]];
+    const PrimeInfo p1 = primes[sh.lwe_prime[sh.L0 > 1 ? 1 : 0]];
+    const unsigned __int128 Q = sh.L0 > 1 ? (unsigned __int128)p0.q * p1.q : (unsigned __int128)p0.q;
+    const long long total = B * (sh.n + 1);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long b = e / (sh.n + 1);
+        const int i = (int)(e - b * (sh.n + 1));
+        unsigned __int128 v;
+        if (i < sh.n) {
+            const uint64_t* ab = a + (b * sh.L0) * sh.n;
+            v = sh.L0 > 1 ? crt2(ab[i], ab[sh.n + i], p0.q, p1.q, q0inv, p1) : (unsigned __int128)ab[i];
+            rots[(long long)i * B + b] = rotation(v, Q, sh.N);
+        } else {
+            const uint64_t* bv = bb + b * sh.L0;
+            v = sh.L0 > 1 ? crt2(bv[0], bv[1], p0.q, p1.q, q0inv, p1) : (unsigned __int128)bv[0];
+            v += ((unsigned __int128)offset_hi << 64) | offset_lo;
+            const uint32_t r = rotation(v, Q, sh.N);
+            rot0[b] = (uint32_t)((2 * sh.N - r) % (2 * sh.N));
+        }
+    }
+}
+
+// acc[b][c][l] = tv[c][l] * X^rot0[b]   (mlwe_RNSc_mul_by_xai, rns_polynomial.c:1048-1106)
+__global__ void k_init_acc(uint64_t* __restrict__ acc, const uint64_t* __restrict__ tv, const uint32_t* __restrict__ rot0,
+                           const __grid_constant__ CggiShape sh, const PrimeInfo* __restrict__ primes) {
+    const long long N = sh.N;
+    const int rows = 2 * sh.L0;
+    const long long b = blockIdx.y / rows;
+    const int cl = blockIdx.y - (int)(b * rows);
+    const uint64_t q = primes[sh.lwe_prime[cl % sh.L0]].q;
+    const uint64_t a = rot0[b];
+    const uint64_t* src = tv + (long long)cl * N;
+    uint64_t* dst = acc + (b * rows + cl) * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x) {
+        const uint64_t s = ((uint64_t)x + 2 * N - a) & (2 * N - 1);
+        dst[x] = s < (uint64_t)N ? src[s] : neg_mod(src[s - N], q);
+    }
+}
+
+// diff[b][c][l] = acc X^r - acc, r = rots[step][b]  (mgsw_CMUX's in2 - in1, mgsw.c:60-61)
+__global__ void k_rot_diff(uint64_t* __restrict__ diff, const uint64_t* __restrict__ acc,
+                           const uint32_t* __restrict__ rots_step, const __grid_constant__ CggiShape sh,
+                           const PrimeInfo* __restrict__ primes) {
+    const long long N = sh.N;
+    const int rows = 2 * sh.L0;
+    const long long b = blockIdx.y / rows;
+    const int cl = blockIdx.y - (int)(b * rows);
+    const uint64_t q = primes[sh.lwe_prime[cl % sh.L0]].q;
+    const uint64_t a = rots_step[b];
+    const uint64_t* src = acc + (b * rows + cl) * N;
+    uint64_t* dst = diff + (b * rows + cl) * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x) {
+        const uint64_t s = ((uint64_t)x + 2 * N - a) & (2 * N - 1);
+        const uint64_t v = s < (uint64_t)N ? src[s] : neg_mod(src[s - N], q);
+        dst[x] = sub_mod(v, src[x], q);
+    }
+}
+
+// ext[b][c'][e] = sum_d D[b][d][e] * G[d][c'][e]   (gadget_mul_addto_polynomial, gadget.c:5-20)
+// D: [B][nd][ne][N]; G: [nd][2][ne][N] (one MGSW of the key); ext: [B][2][ne][N].
+__global__ void k_mac_shared(uint64_t* __restrict__ ext, const uint64_t* __restrict__ D, const uint64_t* __restrict__ G,
+                             const __grid_constant__ CggiShape sh, const PrimeInfo* __restrict__ primes, int nd) {
+    const long long N = sh.N;
+    const int ne = sh.L0 + 1;
+    const long long b = blockIdx.y / ne;
+    const int e = blockIdx.y - (int)(b * ne);
+    const PrimeInfo pi = primes[sh.ext_prime[e]];
+    const double q = pi.qd, qinv = pi.qinv;
+    const long long dstr = (long long)ne * N, gstr = 2LL * ne * N;
+    const uint64_t* d = D + b * nd * dstr + (long long)e * N;
+    const uint64_t* ga = G + (long long)e * N;
+    const uint64_t* gb = ga + dstr;
+    uint64_t* oa = ext + b * 2 * dstr + (long long)e * N;
+    uint64_t* ob = oa + dstr;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x) {
+        double sa = 0.0, sb = 0.0;
+        for (int j = 0; j < nd; ++j) {
+            const double v = f_from_u64(d[j * dstr + x]);
+            const double wa = f_from_u64(ga[j * gstr + x]);
+            const double wb = f_from_u64(gb[j * gstr + x]);
+            sa = __dadd_rn(sa, f_mulmod(v, wa, __dmul_rn(wa, qinv), q));
+            sb = __dadd_rn(sb, f_mulmod(v, wb, __dmul_rn(wb, qinv), q));
+            if ((j & 3) == 3) {
+                sa = f_reduce(sa, q, qinv);
+                sb = f_reduce(sb, q, qinv);
+            }
+        }
+        oa[x] = f_to_canonical(sa, q, qinv, pi.q);
+        ob[x] = f_to_canonical(sb, q, qinv, pi.q);
+    }
+}
+
+struct DivConsts {
+    uint64_t half_sp[4], inv_sp[4], inv_sp_sh[4];
+    uint64_t p, half_p;
+};
+
+// acc[b][c][l] += round(ext[b][c] / p) limb l   (round division by the special prime,
+// rns_polynomial.c:939-976, then the CMUX's + in1, mgsw.c:65-68)
+__global__ void k_moddown_acc(uint64_t* __restrict__ acc, const uint64_t* __restrict__ ext,
+                              const __grid_constant__ CggiShape sh, const __grid_constant__ DivConsts dc,
+                              const PrimeInfo* __restrict__ primes) {
+    const long long N = sh.N;
+    const int L0 = sh.L0, ne = L0 + 1;
+    const long long b = blockIdx.y >> 1;
+    const int c = blockIdx.y & 1;
+    const uint64_t* ex = ext + (b * 2 + c) * ne * N;
+    uint64_t* ac = acc + (b * 2 + c) * L0 * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x) {
+        const uint64_t t = add_mod(ex[(long long)L0 * N + x], dc.half_p, dc.p);
+        for (int l = 0; l < L0; ++l) {
+            const PrimeInfo& pi = primes[sh.lwe_prime[l]];
+            uint64_t v = add_mod(ex[(long long)l * N + x], dc.half_sp[l], pi.q);
+            v = sub_mod(v, reduce64(t, pi), pi.q);
+            v = shoup(v, dc.inv_sp[l], dc.inv_sp_sh[l], pi.q);
+            ac[(long long)l * N + x] = add_mod(ac[(long long)l * N + x], v, pi.q);
+        }
+    }
+}
+
+// Sample extraction at coefficient 0 (mlwe.c:40-68): out_a[b][l][i] = a[0] for i = 0,
+// -a[N - i] otherwise; out_b[b][l] = b[0].
+__global__ void k_extract0(uint64_t* __restrict__ out_a, uint64_t* __restrict__ out_b, const uint64_t* __restrict__ acc,
+                           const __grid_constant__ CggiShape sh, const PrimeInfo* __restrict__ primes) {
+    const long long N = sh.N;
+    const int L0 = sh.L0;
+    const long long b = blockIdx.y / L0;
+    const int l = blockIdx.y - (int)(b * L0);
+    const uint64_t q = primes[sh.lwe_prime[l]].q;
+    const uint64_t* a = acc + (b * 2 * L0 + l) * N;
+    const uint64_t* bv = acc + (b * 2 * L0 + L0 + l) * N;
+    uint64_t* o = out_a + (b * L0 + l) * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        o[i] = i == 0 ? a[0] : neg_mod(a[N - i], q);
+    if (blockIdx.x == 0 && threadIdx.x == 0) out_b[b * L0 + l] = bv[0];
+}
+
+dim3 cg_grid(long long n, long long y) {
+    note_launch();
+    long long blocks = (n + 255) / 256;
+    if (blocks > 64) blocks = 64;
+    if (blocks < 1) blocks = 1;
+    return dim3((unsigned)blocks, (unsigned)y, 1);
+}
+
+struct GraphKey {
+    const void* ptrs[8];
+    uint64_t batch;
+    uint32_t n;
+    uint32_t primes[5];  // LWE limbs then the special prime (kernel arguments baked into the graph)
+    bool operator==(const GraphKey& o) const {
+        return batch == o.batch && n == o.n && memcmp(ptrs, o.ptrs, sizeof ptrs) == 0 &&
+               memcmp(primes, o.primes, sizeof primes) == 0;
+    }
+};
+
+}  // namespace
+
+uint64_t cggi_ws_elems(uint64_t N, uint64_t B, uint64_t n, uint32_t L0) {
+    const uint64_t ne = L0 + 1, nd = 2 * (uint64_t)L0;
+    // acc + diff + digits + ext, plus rotation tables (uint32, rounded up to words)
+    return B * N * (2 * L0 + 2 * L0 + nd * ne + 2 * ne) + (B * (n + 1) + 1) / 2 + 64;
+}
+
+int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* in_a, const uint64_t* in_b,
+                   uint64_t B, uint32_t n, const uint32_t* limbs, uint32_t L0, uint32_t special, const uint64_t* bk,
+                   const uint64_t* tv, uint64_t torus_base, uint64_t* ws, cudaStream_t st) {
+    const char* where = "vfhe_cuda_cggi_bootstrap_batch";
+    if (!t || L0 < 1 || L0 > 2 || !limbs || special >= t->pub.l || t->pub.split_degree != 1 || n == 0 ||
+        torus_base == 0) {
+        set_error(where, "needs split_degree 1, one or two LWE limbs, a special prime and n > 0");
+        return 1;
+    }
+    if (B == 0 || B > 16383) {  // grid.y carries batch x 4 rows
+        set_error(where, "batch must be in [1, 16383]");
+        return 1;
+    }
+    for (uint32_t k = 0; k < L0; ++k)
+        if (limbs[k] >= t->pub.l || !t->info[limbs[k]].fp64) {
+            set_error(where, "limb outside the pool or prime above 2^50");
+            return 1;
+        }
+    if (!t->info[special].fp64) {
+        set_error(where, "special prime above 2^50");
+        return 1;
+    }
+    const long long N = (long long)t->pub.N;
+    CggiShape sh;
+    memset(&sh, 0, sizeof sh);
+    for (uint32_t k = 0; k < L0; ++k) sh.lwe_prime[k] = sh.ext_prime[k] = limbs[k];
+    sh.ext_prime[L0] = special;
+    sh.L0 = (int)L0;
+    sh.n = (int)n;
+    sh.N = N;
+    const int ne = (int)L0 + 1, nd = 2 * (int)L0;
+
+    uint64_t* acc = ws;                                  // [B][2][L0][N]  coefficient domain
+    uint64_t* diff = acc + B * 2 * L0 * N;               // [B][2][L0][N]
+    uint64_t* D = diff + B * 2 * L0 * N;                 // [B][nd][ne][N] NTT domain
+    uint64_t* ext = D + B * (uint64_t)nd * ne * N;       // [B][2][ne][N]
+    uint32_t* rot0 = (uint32_t*)(ext + B * 2 * ne * N);  // [B]
+    uint32_t* rots = rot0 + B;                           // [n][B]
+
+    // constants
+    const uint64_t q0 = t->info[limbs[0]].q, q1 = L0 > 1 ? t->info[limbs[1]].q : 1;
+    const uint64_t q0inv = L0 > 1 ? host_inv_mod(q0 % q1, q1) : 0;
+    const unsigned __int128 Q = (unsigned __int128)q0 * q1;
+    const unsigned __int128 off = Q / (4 * (unsigned __int128)torus_base);
+    DivConsts dc;
+    memset(&dc, 0, sizeof dc);
+    const uint64_t p = t->info[special].q;
+    dc.p = p;
+    dc.half_p = p / 2;
+    for (uint32_t l = 0; l < L0; ++l) {
+        const uint64_t q = t->info[limbs[l]].q;
+        dc.half_sp[l] = (p / 2) % q;
+        dc.inv_sp[l] = host_inv_mod(p % q, q);
+        dc.inv_sp_sh[l] = host_shoup(dc.inv_sp[l], q);
+    }
+    const PrimeInfo* dp = t->d_info;
+
+    // digit transforms: slot k = d * ne + e, d = c * L0 + l: diff row (b, c, l) lifted to ext limb e
+    RowSet dig;
+    memset(&dig, 0, sizeof dig);
+    for (int d = 0; d < nd; ++d)
+        for (int e = 0; e < ne; ++e) {
+            const int k = d * ne + e;
+            dig.in[k] = diff + (long long)d * N;
+            dig.out[k] = D + (long long)k * N;
+            dig.prime[k] = sh.ext_prime[e];
+        }
+    dig.nlimbs = nd * ne;
+    dig.split = 1;
+    dig.logP = t->logP;
+    dig.batch = (int)B;
+    dig.batch_stride = (long long)nd * ne * N;
+    dig.in_batch_stride = 2LL * L0 * N;
+    dig.reduce_input = 1;
+    mark_fp64(dig, t);
+    RowSet inv;
+    memset(&inv, 0, sizeof inv);
+    for (int e = 0; e < ne; ++e) {
+        inv.in[e] = ext + (long long)e * N;
+        inv.out[e] = ext + (long long)e * N;
+        inv.prime[e] = sh.ext_prime[e];
+    }
+    inv.nlimbs = ne;
+    inv.split = 1;
+    inv.logP = t->logP;
+    inv.batch = (int)(2 * B);
+    inv.batch_stride = (long long)ne * N;
+    inv.in_batch_stride = inv.batch_stride;
+    mark_fp64(inv, t);
+
+    k_rotations<<<cg_grid(B * (n + 1), 1), 256, 0, st>>>(rots, rot0, in_a, in_b, sh, dp, (long long)B, q0inv,
+                                                         (uint64_t)off, (uint64_t)(off >> 64));
+    k_init_acc<<<cg_grid(N, B * 2 * L0), 256, 0, st>>>(acc, tv, rot0, sh, dp);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+
+    // the n blind-rotation steps: one CUDA graph per (shape, buffers), replayed
+    static std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
+    GraphKey key;
+    memset(&key, 0, sizeof key);
+    const void* ptrs[8] = {t, acc, diff, D, ext, rots, bk, dp};
+    memcpy(key.ptrs, ptrs, sizeof ptrs);
+    key.batch = B;
+    key.n = n;
+    memcpy(key.primes, sh.ext_prime, sizeof key.primes);
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : graphs)
+        if (g.first == key) exec = g.second;
+    if (!exec) {
+        cudaStream_t cs = nullptr;
+        if (!check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), where)) return 1;
+        if (!check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), where)) return 1;
+        const uint64_t bk_stride = (uint64_t)nd * 2 * ne * N;
+        int err = 0;
+        for (uint32_t i = 0; i < n && !err; ++i) {
+            k_rot_diff<<<cg_grid(N, B * 2 * L0), 256, 0, cs>>>(diff, acc, rots + (uint64_t)i * B, sh, dp);
+            err = launch_ntt(dig, dp, false, cs);
+            if (err) break;
+            k_mac_shared<<<cg_grid(N, B * ne), 256, 0, cs>>>(ext, D, bk + i * bk_stride, sh, dp, nd);
+            err = launch_ntt(inv, dp, true, cs);
+            if (err) break;
+            k_moddown_acc<<<cg_grid(N, B * 2), 256, 0, cs>>>(acc, ext, sh, dc, dp);
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e1 = cudaStreamEndCapture(cs, &graph);
+        cudaStreamDestroy(cs);
+        if (err || !check_cuda(e1, where)) {
+            if (graph) cudaGraphDestroy(graph);
+            if (err) check_cuda(err, where);
+            return 1;
+        }
+        const cudaError_t e2 = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (!check_cuda(e2, where)) return 1;
+        graphs.emplace_back(key, exec);
+    }
+    if (!check_cuda(cudaGraphLaunch(exec, st), where)) return 1;
+    note_launch((int)(5 * n));
+    k_extract0<<<cg_grid(N, B * L0), 256, 0, st>>>(out_a, out_b, acc, sh, dp);
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+}  // namespace vc
