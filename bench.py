@@ -210,6 +210,53 @@ def run_reference_arm(args) -> None:
 
 
 # ----------------------------------------------------------------------------- gpu arm
+def worklist_leg(eng, count: int, reps: int) -> dict:
+    """Uneven batch: `count` jobs, N in 2^12..2^16, L in 2..24, half NTT->product->INTT
+    chains and half key switches, as one work-list graph launch vs one call per job."""
+    import torch
+
+    from vfhe_b200.worklist import WorkList, per_call_workspace, run_per_call, uneven_jobs
+
+    jobs = uneven_jobs(eng, count=count, seed=SEED + 3)
+    wl = WorkList(eng)
+    for j in jobs:
+        wl.add(j)
+    stream = torch.cuda.current_stream()
+    wl.run(stream)  # compile + capture + first replay
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        wl.run(stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_wl = ev0.elapsed_time(ev1) / reps
+    outs = [torch.empty_like(j.out) for j in jobs]
+    ws = per_call_workspace(eng, jobs)
+    calls = run_per_call(eng, jobs, outs, ws, stream)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(reps):
+        run_per_call(eng, jobs, outs, ws, stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_pc = ev0.elapsed_time(ev1) / reps
+    exact = all(torch.equal(j.out, o) for j, o in zip(jobs, outs))
+    moved = sum(j.bytes_moved() for j in jobs)
+    res = {
+        "jobs": count, "jobs_per_s": count / (ms_wl * 1e-3), "ms_per_run": ms_wl,
+        "per_call_jobs_per_s": count / (ms_pc * 1e-3), "per_call_ms": ms_pc, "per_call_calls": calls,
+        "speedup_vs_per_call": ms_pc / ms_wl, "bit_exact_vs_per_call": bool(exact),
+        "graph_kernels_per_run": wl.launches, "device_bytes": wl.device_bytes,
+        "algorithmic_gb_per_s": moved / (ms_wl * 1e-3) / 1e9,
+        "mix": {"chain": sum(j.kind == "chain" for j in jobs), "keyswitch": sum(j.kind == "keyswitch" for j in jobs)},
+    }
+    wl.close()
+    del jobs, outs, ws
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_cuda_arm(args) -> None:
     import torch
 
@@ -358,6 +405,8 @@ def run_cuda_arm(args) -> None:
     del b16
     eng.check("bench")
 
+    uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
+
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -395,7 +444,7 @@ def run_cuda_arm(args) -> None:
         "config": dict(CONFIG, pairs_per_step=PAIRS),
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
                 "d2h_bytes_per_step": int(hout.numel() * 8), "ms_per_step": e2e_ms},
-        "roofline": {"bound": "hbm", "kernel": "k_ntt_pass (digit transforms, 2560 rows x 2^14)",
+        "roofline": {"bound": "hbm", "kernel": "forward FP64 NTT, k_col_f<2,0> + k_tile_fwd_f<12,1> (digit transforms, 2560 rows x 2^14)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "launch_ms": ntt_ms,
                      "algorithmic_bytes": alg_bytes},
@@ -405,6 +454,8 @@ def run_cuda_arm(args) -> None:
         "ntt_2p16_L24": {"limbs_per_s": limbs16, "ms_per_8_polys": ms16,
                          "frac_hbm": 16 * 2**16 * limbs16 / 1e9 / peak},
     }
+    if uneven is not None:
+        line["uneven_worklist"] = uneven
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
@@ -422,6 +473,8 @@ def main() -> None:
     ap.add_argument("--pairs", type=int, default=PAIRS,
                     help="ciphertext pairs per step (the workload is 256; smaller only for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU leg")
+    ap.add_argument("--no-worklist", action="store_true", help="skip the uneven work-list leg")
+    ap.add_argument("--worklist-jobs", type=int, default=512, help="jobs in the uneven work-list leg")
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT))
     if args.impl == "reference":

@@ -367,6 +367,49 @@ int vfhe_cuda_cggi_bootstrap_batch(void *ntt, uint64_t *d_out_a, uint64_t *d_out
                                    uint32_t nlimbs, uint32_t special, const uint64_t *d_bk, const uint64_t *d_tv,
                                    uint64_t torus_base, void *workspace, void *stream);
 
+/* Batched GHS key switch of rank-1 samples with one key (mlwe_RNSc_GHS_hybrid_keyswitch,
+ * mlwe.c:557-598, with a single key component): for each [2][L][N] coefficient-domain
+ * sample (a, b), d_out = (moddown(-sum_j d_j K_j.a), b + moddown(-sum_j d_j K_j.b)),
+ * d_j = limb j of a lifted to limbs[] + special.  Key layout as for the CKKS calls. */
+uint64_t vfhe_cuda_keyswitch_workspace_bytes(void *ntt, uint64_t batch, uint32_t nlimbs);
+int vfhe_cuda_keyswitch_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct, uint64_t batch,
+                              const uint32_t *limbs, uint32_t nlimbs, uint32_t special, const uint64_t *d_ksk,
+                              void *workspace, void *stream);
+
+/* Transform launch schedule for one (log2 P, floor(log2 rows-per-launch)) class, as
+ * picked by the autotuner: tile_bits (P-point rows are split into a radix-2^(logP -
+ * tile_bits) column pass and tiles of 2^tile_bits; == logP for one pass; 8..13),
+ * tiles_per_cta (rows or row segments one CTA holds), ctas_per_sm (0: one CTA per tile
+ * group; k: persistent grid of k CTAs per SM).  Zero = built-in default.  Schedules
+ * never change results.  get_schedule writes the three fields for a launch of `rows`
+ * rows.  No counterpart in the reference (its transforms are single-threaded loops). */
+int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_bits, int32_t tiles_per_cta,
+                               int32_t ctas_per_sm);
+int vfhe_cuda_ntt_get_schedule(uint32_t logP, uint64_t rows, int32_t *out3);
+
+/* Work list: independent jobs of any mix of ring degree and limb count, run as ONE
+ * CUDA-graph launch (grouped per transform pool; each stage of a group is one launch
+ * over a device-resident row table).  Jobs:
+ *   chain      d_out = INTT(NTT(d_a) * NTT(d_b)), [nlimbs][N] each (as
+ *              vfhe_cuda_ntt_mul_intt_batch with batch 1);
+ *   keyswitch  as vfhe_cuda_keyswitch_batch with batch 1 (d_ct [2][nlimbs][N],
+ *              d_out [2][nlimbs][N], d_ksk [nlimbs][2][nlimbs+1][N]).
+ * All primes below 2^50, rows 16-byte aligned, 2^8 <= N/split <= 2^17.  compile (or
+ * the first run) allocates the work list's scratch and tables and captures the graph;
+ * run replays it on `stream`.  The job buffers must stay allocated at the same
+ * addresses while the work list is used; adding a job drops the compiled graph.
+ * No counterpart in the reference. */
+void *vfhe_cuda_worklist_new(void);
+void vfhe_cuda_worklist_free(void *wl);
+int vfhe_cuda_worklist_add_chain(void *wl, void *ntt, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
+                                 const uint32_t *limbs, uint32_t nlimbs);
+int vfhe_cuda_worklist_add_keyswitch(void *wl, void *ntt, uint64_t *d_out, const uint64_t *d_ct,
+                                     const uint32_t *limbs, uint32_t nlimbs, uint32_t special, const uint64_t *d_ksk);
+int vfhe_cuda_worklist_compile(void *wl);
+int vfhe_cuda_worklist_run(void *wl, void *stream);
+uint64_t vfhe_cuda_worklist_device_bytes(void *wl);
+int vfhe_cuda_worklist_launches(void *wl);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,14 +13,14 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _setup(cuda, N, n_mid, pairs, steps, seed):
+def _setup(cuda, N, n_mid, pairs, steps, seed, split=1):
     from vfhe_b200.arith import Ring
     from vfhe_b200.fhe import CKKS_Scheme
     from vfhe_b200.native import use_engine
 
     with use_engine(cuda):
         rng = np.random.default_rng(seed)
-        R = Ring(N, prime_size=[50] + [40] * n_mid + [50], split_degree=1)
+        R = Ring(N, prime_size=[50] + [40] * n_mid + [50], split_degree=split)
         s = CKKS_Scheme(R, scaling_factor=2**40, special_primes=1)
         key = s.key_gen_uniform_ternary(3.2, rng)
         rlk = s.gen_rlk(key, key, lvl=0, rng=rng)
@@ -32,14 +32,14 @@ def _setup(cuda, N, n_mid, pairs, steps, seed):
         return s, key, rlk, gks, cts
 
 
-@pytest.mark.parametrize("N,n_mid", [(2**12, 3), (2**14, 8)])
-def test_batched_ckks_matches_single_calls(cuda, N, n_mid):
+@pytest.mark.parametrize("N,n_mid,split", [(2**12, 3, 1), (2**14, 8, 1), (2**12, 3, None), (2**13, 2, 2)])
+def test_batched_ckks_matches_single_calls(cuda, N, n_mid, split):
     import torch
 
     from vfhe_b200.batch import CkksBatch, ciphertext_rows, key_tensor, to_device, to_host
 
     steps = [1, 4]
-    s, key, rlk, gks, cts = _setup(cuda, N, n_mid, 6, steps, seed=31)
+    s, key, rlk, gks, cts = _setup(cuda, N, n_mid, 6, steps, seed=31, split=split)
     c1, c2 = cts[0::2], cts[1::2]
     rot_steps = [steps[i % len(steps)] for i in range(len(c1))]
 

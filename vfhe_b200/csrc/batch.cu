@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <vector>
+
 #include "abi_common.cuh"
 
 using namespace vc;
@@ -176,6 +178,42 @@ int vfhe_cuda_cggi_bootstrap_batch(void* ntt, uint64_t* d_out_a, uint64_t* d_out
     if (!ws) return 1;
     return cggi_bootstrap(t, d_out_a, d_out_b, d_in_a, d_in_b, batch, n, limbs, nlimbs, special, d_bk, d_tv,
                           torus_base, ws, st);
+}
+
+uint64_t vfhe_cuda_keyswitch_workspace_bytes(void* ntt, uint64_t batch, uint32_t nlimbs) {
+    return vfhe_cuda_ckks_rotate_workspace_bytes(ntt, batch, nlimbs);
+}
+
+int vfhe_cuda_keyswitch_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct, uint64_t batch,
+                              const uint32_t* limbs, uint32_t nlimbs, uint32_t special, const uint64_t* d_ksk,
+                              void* workspace, void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    IncNtt* t = as_ntt(ntt);
+    cudaStream_t st = (cudaStream_t)stream_;
+    uint64_t* ws = (uint64_t*)workspace;
+    if (!ws) ws = engine_workspace(vfhe_cuda_keyswitch_workspace_bytes(ntt, batch, nlimbs), st);
+    if (!ws) return 1;
+    std::vector<const uint64_t*> keys(batch, d_ksk);
+    return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, nullptr, keys.data(), ws, st);
+}
+
+int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_bits, int32_t tiles_per_cta,
+                               int32_t ctas_per_sm) {
+    const NttSchedule s = {tile_bits, tiles_per_cta, ctas_per_sm};
+    if (!set_ntt_schedule((int)logP, (int)rows_log2, s)) {
+        set_error("vfhe_cuda_ntt_set_schedule", "schedule outside the supported shapes");
+        return 1;
+    }
+    return 0;
+}
+
+int vfhe_cuda_ntt_get_schedule(uint32_t logP, uint64_t rows, int32_t* out3) {
+    if (!out3) return 1;
+    const NttSchedule s = get_ntt_schedule((int)logP, (long long)rows);
+    out3[0] = s.tile_bits;
+    out3[1] = s.tiles_per_cta;
+    out3[2] = s.ctas_per_sm;
+    return 0;
 }
 
 }  // extern "C"

@@ -20,6 +20,7 @@
 
 #include "abi_common.cuh"
 #include "fp64mod.cuh"
+#include "keyswitch.cuh"
 
 namespace vc {
 
@@ -29,10 +30,25 @@ struct LimbPrimes {
     uint32_t p[kMaxLimbs];
 };
 
-// d0 = a1 a2, d1 = a1 b2 + b1 a2, d2 = b1 b2 per NTT slot (mlwe.c:665-709 at rank 1).
+// Block o, slot x of the incomplete product u (*) v over S blocks of P slots
+// (polynomial_mul_RNS_polynomial, rns_polynomial.c:311-356).
+__device__ __forceinline__ uint64_t inc_prod_slot(const uint64_t* u, const uint64_t* v, int S, long long P,
+                                                  long long x, int o, const PrimeInfo& pi) {
+    if (S == 1) return mul_mod(u[x], v[x], pi);
+    uint64_t acc = 0, wrap = 0;
+    for (int i = 0; i < S; ++i) {
+        const int k = o - i;
+        if (k >= 0) acc = add_mod(acc, mul_mod(u[(long long)i * P + x], v[(long long)k * P + x], pi), pi.q);
+        else wrap = add_mod(wrap, mul_mod(u[(long long)i * P + x], v[(long long)(k + S) * P + x], pi), pi.q);
+    }
+    const ulonglong2 w = reinterpret_cast<const ulonglong2*>(pi.twist)[x];
+    return add_mod(acc, shoup(wrap, w.x, w.y, pi.q), pi.q);
+}
+
+// d0 = a1 a2, d1 = a1 b2 + b1 a2, d2 = b1 b2 in the NTT domain (mlwe.c:665-709 at rank 1).
 __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ c1,
                          const uint64_t* __restrict__ c2, const __grid_constant__ LimbPrimes lp,
-                         const PrimeInfo* __restrict__ primes, int L, long long N) {
+                         const PrimeInfo* __restrict__ primes, int L, long long N, int S) {
     const int by = blockIdx.y;
     const int b = by / L, k = by - b * L;
     const PrimeInfo pi = primes[lp.p[k]];
@@ -42,21 +58,34 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
     const uint64_t* a2 = c2 + b * cs + k * N;
     const uint64_t* b2 = a2 + LN;
     uint64_t* t0 = T + b * ts + k * N;
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
-         x += (long long)gridDim.x * blockDim.x) {
-        const uint64_t va1 = a1[x], vb1 = b1[x], va2 = a2[x], vb2 = b2[x];
-        t0[x] = mul_mod(va1, va2, pi);
-        t0[x + LN] = add_mod(mul_mod(va1, vb2, pi), mul_mod(vb1, va2, pi), pi.q);
-        t0[x + 2 * LN] = mul_mod(vb1, vb2, pi);
+    if (S == 1) {
+        for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+             x += (long long)gridDim.x * blockDim.x) {
+            const uint64_t va1 = a1[x], vb1 = b1[x], va2 = a2[x], vb2 = b2[x];
+            t0[x] = mul_mod(va1, va2, pi);
+            t0[x + LN] = add_mod(mul_mod(va1, vb2, pi), mul_mod(vb1, va2, pi), pi.q);
+            t0[x + 2 * LN] = mul_mod(vb1, vb2, pi);
+        }
+        return;
+    }
+    const long long P = N / S;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int o = (int)(idx / P);
+        const long long x = idx - o * P;
+        t0[idx] = inc_prod_slot(a1, a2, S, P, x, o, pi);
+        t0[idx + LN] = add_mod(inc_prod_slot(a1, b2, S, P, x, o, pi), inc_prod_slot(b1, a2, S, P, x, o, pi), pi.q);
+        t0[idx + 2 * LN] = inc_prod_slot(b1, b2, S, P, x, o, pi);
     }
 }
 
-// acc[b][c][i] = -sum_j D[b][j][i] * K_b[j][c][i]   (gadget_mul_subto_polynomial, gadget.c:22-36)
+// acc[b][c][i] = -sum_j D[b][j][i] (*) K_b[j][c][i]   (gadget_mul_subto_polynomial, gadget.c:22-36;
+// (*) the ring's incomplete product, pointwise at split 1)
 // D: [B][nd][ne][N]; K_b: [digits][2][ne][N] (only the first nd digits are used);
-// acc: [B][2][ne][N].
+// acc: [B][2][ne][N].  Thread index over N = (block o, slot x).
 __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
                       const uint64_t* const* __restrict__ keys, const __grid_constant__ LimbPrimes lp,
-                      const PrimeInfo* __restrict__ primes, int nd, int ne, long long N) {
+                      const PrimeInfo* __restrict__ primes, int nd, int ne, long long N, int S) {
     const int by = blockIdx.y;
     const int b = by / ne, i = by - b * ne;
     const PrimeInfo pi = primes[lp.p[i]];
@@ -68,11 +97,8 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
     const uint64_t* kb = ka + dstride;
     uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
     uint64_t* ob = oa + dstride;
-    if (pi.fp64) {
-        // Exact FP64 multiply-accumulate (fp64mod.cuh): each term is y k - n q with
-        // |term| <= 3q/4 for canonical y, k < q (k/q formed as fl(k) fl(1/q), whose
-        // 2^-52 relative error only moves the quotient estimate); partial sums are
-        // brought back below q every four digits so they stay exact (< 2^52).
+    if (S == 1 && pi.fp64) {
+        // pointwise products: the streaming loop, partial sums reduced every four digits
         const double q = pi.qd, qinv = pi.qinv;
         for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
              x += (long long)gridDim.x * blockDim.x) {
@@ -88,37 +114,20 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
                     sb = f_reduce(sb, q, qinv);
                 }
             }
-            // -sum, canonical
             oa[x] = f_to_canonical(-sa, q, qinv, pi.q);
             ob[x] = f_to_canonical(-sb, q, qinv, pi.q);
         }
         return;
     }
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
-         x += (long long)gridDim.x * blockDim.x) {
-        uint64_t sa = 0, sb = 0;
-        for (int j = 0; j < nd; ++j) {
-            const uint64_t v = d[j * dstride + x];
-            sa = add_mod(sa, mul_mod(v, ka[j * kstride + x], pi), pi.q);
-            sb = add_mod(sb, mul_mod(v, kb[j * kstride + x], pi), pi.q);
-        }
-        oa[x] = neg_mod(sa, pi.q);
-        ob[x] = neg_mod(sb, pi.q);
+    const long long P = N / S;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int o = (int)(idx / P);
+        const long long x = idx - o * P;
+        if (pi.fp64) mac_slot(oa, ob, d, dstride, ka, kb, kstride, nd, S, P, x, o, pi);
+        else mac_slot_int(oa, ob, d, dstride, ka, kb, kstride, nd, S, P, x, o, pi);
     }
 }
-
-struct ModDownConsts {
-    uint32_t prime[kMaxLimbs];      // pool index of output limb i (i < nl)
-    uint64_t half_sp[kMaxLimbs];    // floor(p/2) mod q_i, p the special prime
-    uint64_t inv_sp[kMaxLimbs];     // p^-1 mod q_i
-    uint64_t inv_sp_sh[kMaxLimbs];
-    uint64_t half_r[kMaxLimbs];     // floor(q_top/2) mod q_i
-    uint64_t inv_r[kMaxLimbs];      // q_top^-1 mod q_i
-    uint64_t inv_r_sh[kMaxLimbs];
-    uint32_t special;               // pool index of the special prime
-    uint64_t p, half_p;             // special prime and floor(p/2)
-    uint64_t q_top, half_top;       // top prime dropped by the rescale
-};
 
 // Per coefficient: divide the key-switch accumulator by the special prime with
 // rounding, add the pass-through component, and optionally rescale by the top prime.
@@ -263,6 +272,9 @@ int blocks_transform(IncNtt* t, uint64_t* data, uint64_t count, const uint32_t* 
     return launch_ntt(rs, t->d_info, inverse, st);
 }
 
+
+}  // namespace
+
 ModDownConsts moddown_consts(IncNtt* t, const uint32_t* limbs, int nl, uint32_t special) {
     ModDownConsts mc;
     memset(&mc, 0, sizeof mc);
@@ -285,8 +297,6 @@ ModDownConsts moddown_consts(IncNtt* t, const uint32_t* limbs, int nl, uint32_t 
     }
     return mc;
 }
-
-}  // namespace
 
 uint64_t ckks_mul_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
     const uint64_t ne = L + 1;
@@ -326,12 +336,13 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     std::vector<const uint64_t*> kp(B, rlk);
     if (!check_cuda(cudaMemcpyAsync(keyptrs, kp.data(), B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where))
         return 1;
-    k_tensor<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N);
+    k_tensor<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N,
+                                                            (int)t->pub.split_degree);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
     if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
     k_mac<<<grid_xy(N, (long long)B * ne), 256, 0, st>>>(acc, D, (const uint64_t* const*)keyptrs, lpe, t->d_info,
-                                                          nl, ne, N);
+                                                          nl, ne, N, (int)t->pub.split_degree);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
@@ -340,16 +351,19 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
 
+// gens == nullptr: a plain key switch of every ciphertext (no automorphism); the
+// digits and the pass-through b are read from ct itself.
 int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const uint32_t* limbs, uint32_t L,
                 uint32_t special, const uint64_t* gens, const uint64_t* const* gks, uint64_t* ws, cudaStream_t st) {
-    const char* where = "vfhe_cuda_ckks_rotate_batch";
+    const char* where = gens ? "vfhe_cuda_ckks_rotate_batch" : "vfhe_cuda_keyswitch_batch";
     if (!check_shape(t, limbs, L, special, where)) return 1;
     const long long N = (long long)t->pub.N;
-    for (uint64_t b = 0; b < B; ++b)
-        if ((gens[b] & 1) == 0 || gens[b] >= 2 * (uint64_t)N) {
-            set_error(where, "Galois elements must be odd and below 2N");
-            return 1;
-        }
+    if (gens)
+        for (uint64_t b = 0; b < B; ++b)
+            if ((gens[b] & 1) == 0 || gens[b] >= 2 * (uint64_t)N) {
+                set_error(where, "Galois elements must be odd and below 2N");
+                return 1;
+            }
     const int nl = (int)L, ne = nl + 1;
     uint32_t ext[kMaxLimbs];
     for (int i = 0; i < nl; ++i) ext[i] = limbs[i];
@@ -367,18 +381,23 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     uint64_t* acc = D + B * (uint64_t)nl * ne * N;      // [B][2][ne][N]
     uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
     uint64_t* d_gens = keyptrs + B;                     // [B]
-    if (!check_cuda(cudaMemcpyAsync(keyptrs, gks, B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where) ||
-        !check_cuda(cudaMemcpyAsync(d_gens, gens, B * sizeof(uint64_t), cudaMemcpyHostToDevice, st), where))
+    if (!check_cuda(cudaMemcpyAsync(keyptrs, gks, B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where))
         return 1;
-    k_permute_batch<<<grid_xy(N, (long long)B * 2 * nl), 256, 0, st>>>(Pm, ct, d_gens, lp, t->d_info, nl, N, ls);
-    if (!check_cuda(cudaGetLastError(), where)) return 1;
-    if (!check_cuda(digits_forward(t, D, Pm, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
+    const uint64_t* src = ct;
+    if (gens) {
+        if (!check_cuda(cudaMemcpyAsync(d_gens, gens, B * sizeof(uint64_t), cudaMemcpyHostToDevice, st), where))
+            return 1;
+        k_permute_batch<<<grid_xy(N, (long long)B * 2 * nl), 256, 0, st>>>(Pm, ct, d_gens, lp, t->d_info, nl, N, ls);
+        if (!check_cuda(cudaGetLastError(), where)) return 1;
+        src = Pm;
+    }
+    if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
     k_mac<<<grid_xy(N, (long long)B * ne), 256, 0, st>>>(acc, D, (const uint64_t* const*)keyptrs, lpe, t->d_info,
-                                                          nl, ne, N);
+                                                          nl, ne, N, (int)t->pub.split_degree);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
-    k_moddown<<<grid_xy(N, (long long)B * 2), 256, 0, st>>>(out, acc, Pm, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
+    k_moddown<<<grid_xy(N, (long long)B * 2), 256, 0, st>>>(out, acc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
                                                             mc, t->d_info, nl, 0, N);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }

@@ -26,6 +26,7 @@ namespace vc {
 // ---------------------------------------------------------------- context
 struct Context {
     int device = -1;
+    int sms = 0;  // streaming multiprocessors of the device
     cudaStream_t stream = nullptr;
     bool ready = false;
     std::recursive_mutex mu;

@@ -143,6 +143,12 @@ int g_force_int = -1;
 
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream) {
     const int logP = rows.logP;
+    if (rows.table) {
+        // work lists are built only from FP64-eligible, 16-byte aligned rows
+        if (rows.table_rows <= 0) return 0;
+        const int e = launch_ntt_f64(rows, d_primes, inverse, stream);
+        return e == -1 ? (int)cudaErrorInvalidValue : e;
+    }
     if (rows.batch <= 0 || rows.nlimbs <= 0) return 0;
     if (g_force_generic < 0) {
         const char* s = getenv("VFHE_CUDA_NTT_GENERIC");

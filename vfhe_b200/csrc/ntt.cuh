@@ -23,6 +23,15 @@ namespace vc {
 
 constexpr int kMaxLimbs = 64;
 
+// One P-point row of a work list: where it is read, where it is written (may be the
+// same row) and the constants of its prime.  32 bytes.
+struct RowDesc {
+    const uint64_t* in;
+    uint64_t* out;
+    const PrimeInfo* pi;
+    uint64_t reserved;
+};
+
 // A set of rows (one row = one P-point transform) described compactly.
 // Row r of the launch maps to (poly b, limb slot k, block blk):
 //   r = (b * nlimbs + k) * split + blk
@@ -44,13 +53,51 @@ struct RowSet {
     int reduce_input;
     // set by launch_ntt when every prime of the set is below 2^50 (FP64 butterflies)
     int fp64;
+    // Work-list mode (FP64 path only): when `table` is set (device memory), row r of
+    // the launch is table[r], one P-point row with its own prime, so rows of any
+    // polynomials, pools and limb sets with the same P share one launch; the slot
+    // arrays, nlimbs, split and batch are then unused.
+    const RowDesc* table;
+    long long table_rows;
+    int table_src_is_dst;  // read table[r].out instead of .in (second pass of a split transform)
 };
+
+// Rows one launch of `rows` transforms.
+inline long long rowset_rows(const RowSet& rows) {
+    return rows.table ? rows.table_rows : (long long)rows.batch * rows.nlimbs * rows.split;
+}
+
+// Launch shape of the FP64 transform for one (log2 P, log2 rows) class:
+//   tile_bits      low index bits done by one CTA tile (== logP: one pass; else a
+//                  radix-2^(logP - tile_bits) column pass first), 8..13;
+//   tiles_per_cta  tiles (rows or row segments) one CTA holds at once;
+//   ctas_per_sm    0 = one CTA per tile group; k = persistent grid of k x SMs CTAs
+//                  walking the tile groups.
+// Zero fields mean the built-in choice.  Set by the autotuner through the C ABI.
+struct NttSchedule {
+    int tile_bits;
+    int tiles_per_cta;
+    int ctas_per_sm;
+};
+constexpr int kSchedMaxLogP = 17;
+constexpr int kSchedRowBuckets = 32;
+bool set_ntt_schedule(int logP, int rows_log2, const NttSchedule& s);
+NttSchedule get_ntt_schedule(int logP, long long nrows);
+int sm_count();
 
 // Launch the forward (inverse=false) or inverse transform of every row in `rows`.
 // Work is enqueued on `stream`; returns a cudaError_t code (0 on success).
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
 
-// Count of kernels this engine has launched (vfhe_cuda_launch_count).
+// Count of kernels this engine has launched (vfhe_cuda_launch_count).  Kernels
+// recorded into a CUDA graph are counted at capture; the capturing code takes that
+// count back (forget_launches) and notes it again at every replay.
 void note_launch(int n = 1);
+uint64_t launch_counter();
+void forget_launches(uint64_t n);
+
+// Raise the dynamic shared-memory limit of every transform kernel once, outside any
+// stream capture, so that launches recorded into graphs make no attribute calls.
+int prepare_ntt_kernels();
 
 }  // namespace vc

@@ -13,6 +13,9 @@
 //     every second stage and at pass end; products are always <= 3q/4.
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <vector>
+
 #include "fp64mod.cuh"
 #include "ntt.cuh"
 
@@ -151,21 +154,30 @@ struct Tile {
     int hi;
 };
 
+template <bool TABLE>
 __device__ __forceinline__ Tile locate(const RowSet& rows, const PrimeInfo* primes, int K, long long tile,
                                        int tiles_per_row) {
     const long long row = tile / tiles_per_row;
     const int hi = (int)(tile - row * tiles_per_row);
+    Tile r;
+    r.hi = hi;
+    if constexpr (TABLE) {
+        const RowDesc d = rows.table[row];
+        const long long off = (long long)hi << K;
+        r.src = (rows.table_src_is_dst ? d.out : d.in) + off;
+        r.dst = d.out + off;
+        r.pi = d.pi;
+        return r;
+    }
     const int per_poly = rows.nlimbs * rows.split;
     const long long b = row / per_poly;
     const int rem = (int)(row - b * per_poly);
     const int slot = rem / rows.split;
     const int blk = rem - slot * rows.split;
     const long long off = ((long long)blk << rows.logP) + ((long long)hi << K);
-    Tile r;
     r.src = rows.in[slot] + b * rows.in_batch_stride + off;
     r.dst = rows.out[slot] + b * rows.batch_stride + off;
     r.pi = primes + rows.prime[slot];
-    r.hi = hi;
     return r;
 }
 
@@ -184,17 +196,23 @@ __device__ __forceinline__ double load_in(const uint64_t* p, bool in_double, boo
 // Forward transform of the low K bits of each row.  IN_D: the row holds centred
 // doubles from the column pass; otherwise canonical (or foreign, with reduce_input)
 // uint64 residues.  Output: canonical uint64.
-template <int K, bool IN_D>
+// PERSIST: CTAs walk the ngroups groups of tiles_per_cta tiles (every thread of a CTA
+// makes the same number of trips); otherwise CTA b takes group b and the grid covers
+// all groups (the loop body runs once, and the compiler keeps the lean straight-line
+// register allocation).
+template <int K, bool IN_D, bool PERSIST, bool TABLE>
 __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __grid_constant__ RowSet rows,
                                                                      const PrimeInfo* __restrict__ primes,
-                                                                     int tiles_per_cta, int tiles_per_row) {
+                                                                     int tiles_per_cta, int tiles_per_row,
+                                                                     long long ngroups) {
     constexpr int TPT = 1 << (K - 4);
     extern __shared__ double fsm[];
     const int lt = threadIdx.x / TPT;
     const int t = threadIdx.x - lt * TPT;
-    const long long tile = (long long)blockIdx.x * tiles_per_cta + lt;  // always exists
     double* sm = fsm + lt * ((1 << K) + (1 << (K - 4)));
-    const Tile r = locate(rows, primes, K, tile, tiles_per_row);
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const long long tile = grp * tiles_per_cta + lt;
+    const Tile r = locate<TABLE>(rows, primes, K, tile, tiles_per_row);
     const PrimeInfo& pi = *r.pi;
     FCtx c;
     c.q = pi.qd;
@@ -246,21 +264,26 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
         v.y = f_to_canonical(x[m + 1], c.q, c.qinv, pi.q);
         out[m / 2] = v;
     }
+    if (!PERSIST) break;
+    __syncthreads();  // the next trip rewrites shared memory
+    }
 }
 
 // Inverse transform of the low K bits.  FINAL (K == logP): P^-1 folded in, canonical
 // output; otherwise centred doubles are written for the column pass.
-template <int K, bool FINAL>
+template <int K, bool FINAL, bool PERSIST, bool TABLE>
 __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __grid_constant__ RowSet rows,
                                                                      const PrimeInfo* __restrict__ primes,
-                                                                     int tiles_per_cta, int tiles_per_row) {
+                                                                     int tiles_per_cta, int tiles_per_row,
+                                                                     long long ngroups) {
     constexpr int TPT = 1 << (K - 4);
     extern __shared__ double fsm[];
     const int lt = threadIdx.x / TPT;
     const int t = threadIdx.x - lt * TPT;
-    const long long tile = (long long)blockIdx.x * tiles_per_cta + lt;
     double* sm = fsm + lt * ((1 << K) + (1 << (K - 4)));
-    const Tile r = locate(rows, primes, K, tile, tiles_per_row);
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const long long tile = grp * tiles_per_cta + lt;
+    const Tile r = locate<TABLE>(rows, primes, K, tile, tiles_per_row);
     const PrimeInfo& pi = *r.pi;
     FCtx c;
     c.q = pi.qd;
@@ -328,28 +351,43 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __gr
         if (FINAL) *p = f_to_canonical(x[m], c.q, c.qinv, pi.q);
         else *p = (uint64_t)__double_as_longlong(x[m]);
     }
+    if (!PERSIST) break;
+    __syncthreads();  // the next trip rewrites shared memory
+    }
 }
 
-// Column pass over bits [12, logP): thread c owns j = m * 4096 + c, m < 2^K1.
+// Column pass over bits [KT, logP), KT the tile bits of the second pass: thread c
+// owns j = m * 2^KT + c, m < 2^K1.
 // Forward (first pass): canonical/foreign uint64 in, centred doubles out.
 // Inverse (last pass): centred doubles in, canonical uint64 out.
 template <int K1, bool INV>
 __global__ void __launch_bounds__(256) k_col_f(const __grid_constant__ RowSet rows,
-                                               const PrimeInfo* __restrict__ primes, long long ncols) {
+                                               const PrimeInfo* __restrict__ primes, long long ncols, int KT) {
     constexpr int R = 1 << K1;
     const long long gc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gc >= ncols) return;  // no barriers in this kernel
-    const long long row = gc >> 12;
-    const int cc = (int)(gc & 4095);
-    const int per_poly = rows.nlimbs * rows.split;
-    const long long b = row / per_poly;
-    const int rem = (int)(row - b * per_poly);
-    const int slot = rem / rows.split;
-    const int blk = rem - slot * rows.split;
-    const long long off = ((long long)blk << rows.logP) + cc;
-    const uint64_t* src = rows.in[slot] + b * rows.in_batch_stride + off;
-    uint64_t* dst = rows.out[slot] + b * rows.batch_stride + off;
-    const PrimeInfo& pi = primes[rows.prime[slot]];
+    const long long row = gc >> KT;
+    const int cc = (int)(gc & ((1 << KT) - 1));
+    const uint64_t* src;
+    uint64_t* dst;
+    const PrimeInfo* pp;
+    if (rows.table) {
+        const RowDesc d = rows.table[row];
+        src = (rows.table_src_is_dst ? d.out : d.in) + cc;
+        dst = d.out + cc;
+        pp = d.pi;
+    } else {
+        const int per_poly = rows.nlimbs * rows.split;
+        const long long b = row / per_poly;
+        const int rem = (int)(row - b * per_poly);
+        const int slot = rem / rows.split;
+        const int blk = rem - slot * rows.split;
+        const long long off = ((long long)blk << rows.logP) + cc;
+        src = rows.in[slot] + b * rows.in_batch_stride + off;
+        dst = rows.out[slot] + b * rows.batch_stride + off;
+        pp = primes + rows.prime[slot];
+    }
+    const PrimeInfo& pi = *pp;
     const double q = pi.qd, qinv = pi.qinv;
     const int logP = rows.logP;
     double x[R];
@@ -357,12 +395,12 @@ __global__ void __launch_bounds__(256) k_col_f(const __grid_constant__ RowSet ro
         const double2* tw = reinterpret_cast<const double2*>(pi.fwd_d);
 #pragma unroll
         for (int m = 0; m < R; ++m) {
-            double v = f_from_u64(src[(long long)m << 12]);
+            double v = f_from_u64(src[(long long)m << KT]);
             x[m] = rows.reduce_input ? f_reduce(v, q, qinv) : v;
         }
 #pragma unroll
         for (int bb = K1 - 1; bb >= 0; --bb) {
-            const int base = 1 << (logP - 13 - bb);
+            const int base = 1 << (logP - KT - 1 - bb);
 #pragma unroll
             for (int m = 0; m < R; ++m) {
                 if (m & (1 << bb)) continue;
@@ -380,14 +418,14 @@ __global__ void __launch_bounds__(256) k_col_f(const __grid_constant__ RowSet ro
         }
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            dst[(long long)m << 12] = (uint64_t)__double_as_longlong(f_reduce(x[m], q, qinv));
+            dst[(long long)m << KT] = (uint64_t)__double_as_longlong(f_reduce(x[m], q, qinv));
     } else {
         const double2* tw = reinterpret_cast<const double2*>(pi.inv_d);
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = __longlong_as_double((long long)src[(long long)m << 12]);
+        for (int m = 0; m < R; ++m) x[m] = __longlong_as_double((long long)src[(long long)m << KT]);
 #pragma unroll
         for (int bb = 0; bb < K1; ++bb) {
-            const int base = (1 << logP) >> (bb + 13);
+            const int base = (1 << logP) >> (bb + KT + 1);
             const bool last = bb == K1 - 1;
 #pragma unroll
             for (int m = 0; m < R; ++m) {
@@ -409,104 +447,188 @@ __global__ void __launch_bounds__(256) k_col_f(const __grid_constant__ RowSet ro
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) dst[(long long)m << 12] = f_to_canonical(x[m], q, qinv, pi.q);
+        for (int m = 0; m < R; ++m) dst[(long long)m << KT] = f_to_canonical(x[m], q, qinv, pi.q);
     }
 }
+
+// Largest dynamic shared memory the tile kernels may be given (200 KiB of the 227).
+constexpr size_t kTileSmemMax = 200 * 1024;
 
 template <typename KernelT>
 int set_smem(KernelT kern, size_t bytes) {
     if (bytes <= 48 * 1024) return 0;
-    return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // one attribute call per kernel: raised straight to the maximum, then remembered
+    static std::mutex mu;
+    static std::vector<const void*> done;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const void* k : done)
+        if (k == (const void*)kern) return 0;
+    const int e = (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemMax);
+    if (!e) done.push_back((const void*)kern);
+    return e;
 }
 
 // mode: 0 forward (canonical in), 1 forward (doubles in), 2 inverse final, 3 inverse to doubles
 template <int K>
-int tile_launch(const RowSet& rows, const PrimeInfo* d_primes, int mode, int tiles_per_row, cudaStream_t st) {
+int tile_launch(const RowSet& rows, const PrimeInfo* d_primes, int mode, int tiles_per_row, const NttSchedule& sc,
+                cudaStream_t st) {
     constexpr int TPT = 1 << (K - 4);
-    const long long nrows = (long long)rows.batch * rows.nlimbs * rows.split;
-    const long long ntiles = nrows * tiles_per_row;
+    const long long ntiles = rowset_rows(rows) * tiles_per_row;
     int tiles_per_cta = TPT >= 256 ? 1 : 256 / TPT;
+    // a tuned tiles-per-CTA is taken when it fits the kernel's launch bound and shared memory
+    if (sc.tiles_per_cta > 0 && TPT * sc.tiles_per_cta <= TileThreads<K>::value &&
+        (sc.tiles_per_cta & (sc.tiles_per_cta - 1)) == 0 &&
+        sizeof(double) * (size_t)sc.tiles_per_cta * ((1 << K) + (1 << (K - 4))) <= kTileSmemMax)
+        tiles_per_cta = sc.tiles_per_cta;
+    // the tile groups must cover the tiles exactly: no thread may leave before a barrier
     while (tiles_per_cta > 1 && (ntiles % tiles_per_cta) != 0) tiles_per_cta >>= 1;
-    const long long grid = ntiles / tiles_per_cta;
+    const long long ngroups = ntiles / tiles_per_cta;
+    long long grid = ngroups;
+    if (sc.ctas_per_sm > 0) {
+        const long long cap = (long long)sc.ctas_per_sm * sm_count();
+        if (cap < grid) grid = cap;
+    }
+    if (grid > 0x7fffffffLL) grid = 0x7fffffffLL;
     const size_t smem = sizeof(double) * (size_t)tiles_per_cta * ((1 << K) + (1 << (K - 4)));
     const int threads = TPT * tiles_per_cta;
+    const bool persist = grid < ngroups;
     int e = 0;
-    switch (mode) {
-        case 0:
-            e = set_smem(k_tile_fwd_f<K, false>, smem);
-            if (!e) k_tile_fwd_f<K, false><<<(unsigned)grid, threads, smem, st>>>(rows, d_primes, tiles_per_cta, tiles_per_row);
-            break;
-        case 1:
-            e = set_smem(k_tile_fwd_f<K, true>, smem);
-            if (!e) k_tile_fwd_f<K, true><<<(unsigned)grid, threads, smem, st>>>(rows, d_primes, tiles_per_cta, tiles_per_row);
-            break;
-        case 2:
-            e = set_smem(k_tile_inv_f<K, true>, smem);
-            if (!e) k_tile_inv_f<K, true><<<(unsigned)grid, threads, smem, st>>>(rows, d_primes, tiles_per_cta, tiles_per_row);
-            break;
-        default:
-            e = set_smem(k_tile_inv_f<K, false>, smem);
-            if (!e) k_tile_inv_f<K, false><<<(unsigned)grid, threads, smem, st>>>(rows, d_primes, tiles_per_cta, tiles_per_row);
-            break;
+#define VC_TILE_LAUNCH(KERN)                                                                              \
+    do {                                                                                                  \
+        e = set_smem(KERN, smem);                                                                         \
+        if (!e) KERN<<<(unsigned)grid, threads, smem, st>>>(rows, d_primes, tiles_per_cta, tiles_per_row, ngroups); \
+    } while (0)
+    const bool table = rows.table != nullptr;
+    switch (mode * 4 + (persist ? 2 : 0) + (table ? 1 : 0)) {
+        case 0: VC_TILE_LAUNCH((k_tile_fwd_f<K, false, false, false>)); break;
+        case 1: VC_TILE_LAUNCH((k_tile_fwd_f<K, false, false, true>)); break;
+        case 2: VC_TILE_LAUNCH((k_tile_fwd_f<K, false, true, false>)); break;
+        case 3: VC_TILE_LAUNCH((k_tile_fwd_f<K, false, true, true>)); break;
+        case 4: VC_TILE_LAUNCH((k_tile_fwd_f<K, true, false, false>)); break;
+        case 5: VC_TILE_LAUNCH((k_tile_fwd_f<K, true, false, true>)); break;
+        case 6: VC_TILE_LAUNCH((k_tile_fwd_f<K, true, true, false>)); break;
+        case 7: VC_TILE_LAUNCH((k_tile_fwd_f<K, true, true, true>)); break;
+        case 8: VC_TILE_LAUNCH((k_tile_inv_f<K, true, false, false>)); break;
+        case 9: VC_TILE_LAUNCH((k_tile_inv_f<K, true, false, true>)); break;
+        case 10: VC_TILE_LAUNCH((k_tile_inv_f<K, true, true, false>)); break;
+        case 11: VC_TILE_LAUNCH((k_tile_inv_f<K, true, true, true>)); break;
+        case 12: VC_TILE_LAUNCH((k_tile_inv_f<K, false, false, false>)); break;
+        case 13: VC_TILE_LAUNCH((k_tile_inv_f<K, false, false, true>)); break;
+        case 14: VC_TILE_LAUNCH((k_tile_inv_f<K, false, true, false>)); break;
+        default: VC_TILE_LAUNCH((k_tile_inv_f<K, false, true, true>)); break;
     }
+#undef VC_TILE_LAUNCH
     if (e) return e;
     note_launch();
     return (int)cudaGetLastError();
 }
 
 template <int K1>
-int col_launch(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t st) {
-    const long long ncols = (long long)rows.batch * rows.nlimbs * rows.split * 4096;
+int col_launch(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, int KT, cudaStream_t st) {
+    const long long ncols = rowset_rows(rows) << KT;
     const long long grid = (ncols + 255) / 256;
-    if (inverse) k_col_f<K1, true><<<(unsigned)grid, 256, 0, st>>>(rows, d_primes, ncols);
-    else k_col_f<K1, false><<<(unsigned)grid, 256, 0, st>>>(rows, d_primes, ncols);
+    if (inverse) k_col_f<K1, true><<<(unsigned)grid, 256, 0, st>>>(rows, d_primes, ncols, KT);
+    else k_col_f<K1, false><<<(unsigned)grid, 256, 0, st>>>(rows, d_primes, ncols, KT);
     note_launch();
     return (int)cudaGetLastError();
 }
 
-int tile_dispatch(int K, const RowSet& rows, const PrimeInfo* d, int mode, int tpr, cudaStream_t st) {
+int tile_dispatch(int K, const RowSet& rows, const PrimeInfo* d, int mode, int tpr, const NttSchedule& sc,
+                  cudaStream_t st) {
     switch (K) {
-        case 8: return tile_launch<8>(rows, d, mode, tpr, st);
-        case 9: return tile_launch<9>(rows, d, mode, tpr, st);
-        case 10: return tile_launch<10>(rows, d, mode, tpr, st);
-        case 11: return tile_launch<11>(rows, d, mode, tpr, st);
-        case 12: return tile_launch<12>(rows, d, mode, tpr, st);
-        case 13: return tile_launch<13>(rows, d, mode, tpr, st);
+        case 8: return tile_launch<8>(rows, d, mode, tpr, sc, st);
+        case 9: return tile_launch<9>(rows, d, mode, tpr, sc, st);
+        case 10: return tile_launch<10>(rows, d, mode, tpr, sc, st);
+        case 11: return tile_launch<11>(rows, d, mode, tpr, sc, st);
+        case 12: return tile_launch<12>(rows, d, mode, tpr, sc, st);
+        case 13: return tile_launch<13>(rows, d, mode, tpr, sc, st);
         default: return (int)cudaErrorInvalidValue;
     }
 }
 
-int col_dispatch(int K1, const RowSet& rows, const PrimeInfo* d, bool inverse, cudaStream_t st) {
+int col_dispatch(int K1, const RowSet& rows, const PrimeInfo* d, bool inverse, int KT, cudaStream_t st) {
     switch (K1) {
-        case 2: return col_launch<2>(rows, d, inverse, st);
-        case 3: return col_launch<3>(rows, d, inverse, st);
-        case 4: return col_launch<4>(rows, d, inverse, st);
-        case 5: return col_launch<5>(rows, d, inverse, st);
+        case 1: return col_launch<1>(rows, d, inverse, KT, st);
+        case 2: return col_launch<2>(rows, d, inverse, KT, st);
+        case 3: return col_launch<3>(rows, d, inverse, KT, st);
+        case 4: return col_launch<4>(rows, d, inverse, KT, st);
+        case 5: return col_launch<5>(rows, d, inverse, KT, st);
         default: return (int)cudaErrorInvalidValue;
     }
+}
+
+NttSchedule g_sched[kSchedMaxLogP + 1][kSchedRowBuckets];
+
+template <int K, bool P, bool T>
+int prepare_kp() {
+    int e = set_smem(k_tile_fwd_f<K, false, P, T>, kTileSmemMax);
+    if (!e) e = set_smem(k_tile_fwd_f<K, true, P, T>, kTileSmemMax);
+    if (!e) e = set_smem(k_tile_inv_f<K, true, P, T>, kTileSmemMax);
+    if (!e) e = set_smem(k_tile_inv_f<K, false, P, T>, kTileSmemMax);
+    return e;
+}
+
+template <int K>
+int prepare_k() {
+    int e = prepare_kp<K, false, false>();
+    if (!e) e = prepare_kp<K, false, true>();
+    if (!e) e = prepare_kp<K, true, false>();
+    if (!e) e = prepare_kp<K, true, true>();
+    return e;
 }
 
 }  // namespace
+
+int prepare_ntt_kernels() {
+    int e = prepare_k<8>();
+    if (!e) e = prepare_k<9>();
+    if (!e) e = prepare_k<10>();
+    if (!e) e = prepare_k<11>();
+    if (!e) e = prepare_k<12>();
+    if (!e) e = prepare_k<13>();
+    return e;
+}
+
+bool set_ntt_schedule(int logP, int rows_log2, const NttSchedule& s) {
+    if (logP < 8 || logP > kSchedMaxLogP || rows_log2 < 0 || rows_log2 >= kSchedRowBuckets) return false;
+    if (s.tile_bits != 0 && (s.tile_bits < 8 || s.tile_bits > 13 || s.tile_bits > logP || logP - s.tile_bits > 5))
+        return false;
+    if (s.tiles_per_cta < 0 || s.tiles_per_cta > 64 || s.ctas_per_sm < 0 || s.ctas_per_sm > 64) return false;
+    g_sched[logP][rows_log2] = s;
+    return true;
+}
+
+NttSchedule get_ntt_schedule(int logP, long long nrows) {
+    NttSchedule s = {0, 0, 0};
+    if (logP < 8 || logP > kSchedMaxLogP || nrows <= 0) return s;
+    int b = 0;
+    while (b + 1 < kSchedRowBuckets && (2LL << b) <= nrows) ++b;  // floor(log2 nrows)
+    return g_sched[logP][b];
+}
 
 // FP64-butterfly transform of every row (8 <= logP <= 17, all primes below 2^50).
 int launch_ntt_f64(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream) {
     const int logP = rows.logP;
     if (logP < 8 || logP > 17) return -1;
-    if (logP <= 13) return tile_dispatch(logP, rows, d_primes, inverse ? 2 : 0, 1, stream);
-    const int K1 = logP - 12;
+    const NttSchedule sc = get_ntt_schedule(logP, rowset_rows(rows));
+    int K = sc.tile_bits ? sc.tile_bits : (logP <= 13 ? logP : 12);
+    if (K > logP || logP - K > 5) K = logP <= 13 ? logP : 12;
+    if (K == logP) return tile_dispatch(logP, rows, d_primes, inverse ? 2 : 0, 1, sc, stream);
+    const int K1 = logP - K;
     RowSet second = rows;
     for (int i = 0; i < rows.nlimbs; ++i) second.in[i] = rows.out[i];
     second.in_batch_stride = rows.batch_stride;
     second.reduce_input = 0;
+    second.table_src_is_dst = 1;
     int e;
     if (!inverse) {
-        e = col_dispatch(K1, rows, d_primes, false, stream);
+        e = col_dispatch(K1, rows, d_primes, false, K, stream);
         if (e) return e;
-        return tile_dispatch(12, second, d_primes, 1, 1 << K1, stream);
+        return tile_dispatch(K, second, d_primes, 1, 1 << K1, sc, stream);
     }
-    e = tile_dispatch(12, rows, d_primes, 3, 1 << K1, stream);
+    e = tile_dispatch(K, rows, d_primes, 3, 1 << K1, sc, stream);
     if (e) return e;
-    return col_dispatch(K1, second, d_primes, true, stream);
+    return col_dispatch(K1, second, d_primes, true, K, stream);
 }
 
 }  // namespace vc

@@ -39,6 +39,11 @@ bool check_cuda(int code, const char* where) {
     return false;
 }
 
+int sm_count() {
+    const int n = ctx().sms;
+    return n > 0 ? n : 148;
+}
+
 bool ensure_ready() {
     Context& c = ctx();
     if (c.ready) return true;
@@ -56,6 +61,7 @@ bool ensure_ready() {
     if (!check_cuda(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "init: stream"))
         return false;
     c.device = dev;
+    if (cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c.sms <= 0) c.sms = 148;
     c.ready = true;
     return true;
 }
@@ -442,6 +448,8 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 }
 void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+uint64_t launch_counter() { return g_launches.load(); }
+void forget_launches(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 }  // namespace vc
 
 // ---------------------------------------------------------------- status ABI

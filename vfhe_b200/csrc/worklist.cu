@@ -1,0 +1,523 @@
+// Work list: many independent jobs of uneven ring degree N and limb count L run as
+// one CUDA-graph launch.
+//
+// Job kinds (each is bit-exact with the one-job-per-call entry points, which follow
+// the reference's own calls):
+//   chain      out = INTT(NTT(a) (x) NTT(b)), (x) the incomplete product of the
+//              ring's split degree (rns_polynomial.c:311-356, polynomial_RNSc_to_RNS
+//              and back, rns_polynomial.c:582-614);
+//   keyswitch  GHS key switch of a rank-1 sample (a, b) in the coefficient domain
+//              with one key-switching key (mlwe.c:557-598): digits = limbs of a
+//              lifted to limbs + special prime, NTT, -sum digit x key, INTT, round
+//              division by the special prime, + b.
+//
+// Compilation groups the jobs by transform pool (same N, split and prime tables) and
+// writes, per group, device-resident row tables: one descriptor per P-point row to
+// transform, per limb row to multiply, per (job, limb) to multiply-accumulate and per
+// (job, component) to divide.  Each stage of a group is ONE launch over its table,
+// whatever the mix of L and job kinds (the transform kernels read their row, prime
+// and twiddles from the descriptor); groups are independent branches of the graph,
+// so small-N groups run beside large ones.  Transform launch shapes come from the
+// tuned schedule of (log2 P, rows) (vfhe_cuda_ntt_set_schedule).
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "abi_common.cuh"
+#include "fp64mod.cuh"
+#include "keyswitch.cuh"
+
+namespace vc {
+
+namespace {
+
+// product of one limb row: S blocks of P slots
+struct ProdDesc {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* out;
+    const PrimeInfo* pi;
+};
+
+// one (job, extended limb) of a key switch: digits d + j*ne*N, key k + j*2*ne*N,
+// outputs oa and oa + ne*N
+struct MacDesc {
+    const uint64_t* d;
+    const uint64_t* k;
+    uint64_t* oa;
+    const PrimeInfo* pi;
+    int nd;
+    int ne;
+};
+
+// one (job, component) of the special-prime division: acc [nl+1][N] -> out [nl][N] (+ pass)
+struct DownDesc {
+    const uint64_t* acc;
+    uint64_t* out;
+    const uint64_t* pass;
+    const ModDownConsts* mc;
+    int nl;
+    int pad;
+};
+
+constexpr int kWlThreads = 256;
+
+template <int S>
+__global__ void __launch_bounds__(kWlThreads) k_wl_product(const ProdDesc* __restrict__ tab, long long chunks,
+                                                           int logP) {
+    const long long e = blockIdx.x / chunks;
+    const long long chunk = blockIdx.x - e * chunks;
+    const ProdDesc d = tab[e];
+    const PrimeInfo& pi = *d.pi;
+    const uint64_t q = pi.q;
+    const long long P = 1LL << logP;
+    const long long x = chunk * kWlThreads + threadIdx.x;
+    if (x >= P) return;
+    uint64_t av[S], bv[S], res[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        av[j] = d.a[j * P + x];
+        bv[j] = d.b[j * P + x];
+    }
+    const ulonglong2 w = S > 1 ? reinterpret_cast<const ulonglong2*>(pi.twist)[x] : make_ulonglong2(0, 0);
+#pragma unroll
+    for (int o = 0; o < S; ++o) {
+        uint64_t acc = 0, wrap = 0;
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            if (j <= o) acc = add_mod(acc, mul_mod(av[j], bv[o - j], pi), q);
+            else wrap = add_mod(wrap, mul_mod(av[j], bv[o - j + S], pi), q);
+        }
+        if (S > 1) acc = add_mod(acc, shoup(wrap, w.x, w.y, q), q);
+        res[o] = acc;
+    }
+#pragma unroll
+    for (int o = 0; o < S; ++o) d.out[o * P + x] = res[o];
+}
+
+// -sum_j D_j (*) K_j for one (job, extended limb): mac_slot over N = S blocks x P slots
+__global__ void __launch_bounds__(kWlThreads) k_wl_mac(const MacDesc* __restrict__ tab, long long chunks,
+                                                       long long N, int S) {
+    const long long e = blockIdx.x / chunks;
+    const long long chunk = blockIdx.x - e * chunks;
+    const MacDesc d = tab[e];
+    const long long idx = chunk * kWlThreads + threadIdx.x;
+    if (idx >= N) return;
+    const long long P = N / S;
+    const int o = (int)(idx / P);
+    const long long x = idx - o * P;
+    const long long dstr = (long long)d.ne * N;
+    mac_slot(d.oa, d.oa + dstr, d.d, dstr, d.k, d.k + dstr, 2 * dstr, d.nd, S, P, x, o, *d.pi);
+}
+
+__global__ void __launch_bounds__(kWlThreads) k_wl_moddown(const DownDesc* __restrict__ tab, long long chunks,
+                                                           long long N, const PrimeInfo* __restrict__ primes) {
+    const long long e = blockIdx.x / chunks;
+    const long long chunk = blockIdx.x - e * chunks;
+    const DownDesc d = tab[e];
+    const long long x = chunk * kWlThreads + threadIdx.x;
+    if (x >= N) return;
+    const ModDownConsts& mc = *d.mc;
+    const uint64_t t = add_mod(d.acc[(long long)d.nl * N + x], mc.half_p, mc.p);
+    for (int i = 0; i < d.nl; ++i) {
+        const PrimeInfo& pi = primes[mc.prime[i]];
+        uint64_t v = add_mod(d.acc[(long long)i * N + x], mc.half_sp[i], pi.q);
+        v = sub_mod(v, reduce64(t, pi), pi.q);
+        v = shoup(v, mc.inv_sp[i], mc.inv_sp_sh[i], pi.q);
+        if (d.pass) v = add_mod(v, d.pass[(long long)i * N + x], pi.q);
+        d.out[(long long)i * N + x] = v;
+    }
+}
+
+struct Job {
+    int kind;  // 0 chain, 1 keyswitch
+    IncNtt* t;
+    uint64_t* out;
+    const uint64_t* a;
+    const uint64_t* b;    // chain: second operand; keyswitch: unused (b is a + L N)
+    const uint64_t* ksk;  // keyswitch: [L][2][L+1][N]
+    uint32_t limbs[kMaxLimbs];
+    int L;
+    uint32_t special;
+};
+
+struct Group {
+    IncNtt* t = nullptr;
+    std::vector<RowDesc> fwd, inv;
+    std::vector<ProdDesc> prod;
+    std::vector<MacDesc> mac;
+    std::vector<DownDesc> down;
+    // device copies
+    RowDesc* d_fwd = nullptr;
+    RowDesc* d_inv = nullptr;
+    ProdDesc* d_prod = nullptr;
+    MacDesc* d_mac = nullptr;
+    DownDesc* d_down = nullptr;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct WorkList {
+    std::vector<Job> jobs;
+    std::vector<Group> groups;
+    void* dev = nullptr;  // workspace and tables, one allocation
+    size_t dev_bytes = 0;
+    cudaGraphExec_t exec = nullptr;
+    int launches_per_run = 0;
+
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        if (dev) cudaFree(dev);
+        dev = nullptr;
+        dev_bytes = 0;
+        groups.clear();
+    }
+};
+
+namespace {
+
+const char* kWhere = "vfhe_cuda_worklist";
+
+bool job_rows_ok(const Job& j) {
+    const IncNtt* t = j.t;
+    if (!t || j.L <= 0 || j.L + 1 > kMaxLimbs) return false;
+    for (int i = 0; i < j.L; ++i)
+        if (j.limbs[i] >= t->pub.l || !t->info[j.limbs[i]].fp64) return false;
+    if (j.kind == 1 && (j.special >= t->pub.l || !t->info[j.special].fp64)) return false;
+    // transforms read 16-byte vectors
+    const uintptr_t m = (uintptr_t)j.out | (uintptr_t)j.a | (uintptr_t)j.b | (uintptr_t)j.ksk;
+    return (m & 15) == 0 && t->logP >= 8 && t->logP <= 17;
+}
+
+int compile(WorkList& w) {
+    w.release();
+    std::map<IncNtt*, size_t> gidx;
+    std::vector<std::vector<const Job*>> members;
+    for (const Job& j : w.jobs) {
+        auto it = gidx.find(j.t);
+        if (it == gidx.end()) {
+            it = gidx.emplace(j.t, w.groups.size()).first;
+            w.groups.emplace_back();
+            w.groups.back().t = j.t;
+            members.emplace_back();
+        }
+        members[it->second].push_back(&j);
+    }
+    // workspace layout (elements): chain tmp [L][N]; keyswitch D [L][L+1][N] + acc [2][L+1][N]
+    std::vector<size_t> ws_off(w.jobs.size());
+    size_t ws = 0;
+    for (size_t i = 0; i < w.jobs.size(); ++i) {
+        const Job& j = w.jobs[i];
+        const size_t N = j.t->pub.N;
+        ws_off[i] = ws;
+        ws += j.kind == 0 ? (size_t)j.L * N : (size_t)j.L * (j.L + 1) * N + 2 * (size_t)(j.L + 1) * N;
+    }
+    size_t nks = 0;
+    for (const Job& j : w.jobs) nks += j.kind == 1;
+    // device buffer: workspace | moddown constants | tables (sized after the host pass)
+    const size_t ws_bytes = align256(ws * 8);
+    const size_t mc_bytes = align256(nks * sizeof(ModDownConsts));
+    std::vector<ModDownConsts> consts;
+    consts.reserve(nks);
+    // the table pass needs the buffer's base address, so first count, then allocate, then fill
+    size_t tab_bytes = 0;
+    for (size_t g = 0; g < w.groups.size(); ++g) {
+        size_t nf = 0, np = 0, nm = 0, nd = 0;
+        for (const Job* j : members[g]) {
+            const size_t s = j->t->pub.split_degree;
+            if (j->kind == 0) {
+                nf += 2 * j->L * s;
+                np += j->L;
+            } else {
+                nf += (size_t)j->L * (j->L + 1) * s;
+                nm += j->L + 1;
+                nd += 2;
+            }
+        }
+        size_t ni = 0;
+        for (const Job* j : members[g]) ni += (j->kind == 0 ? j->L : 2 * (j->L + 1)) * j->t->pub.split_degree;
+        tab_bytes += align256(nf * sizeof(RowDesc)) + align256(ni * sizeof(RowDesc)) +
+                     align256(np * sizeof(ProdDesc)) + align256(nm * sizeof(MacDesc)) + align256(nd * sizeof(DownDesc));
+    }
+    w.dev_bytes = ws_bytes + mc_bytes + tab_bytes;
+    if (!check_cuda(cudaMalloc(&w.dev, w.dev_bytes), kWhere)) {
+        w.dev = nullptr;
+        return 1;
+    }
+    uint64_t* wsp = (uint64_t*)w.dev;
+    ModDownConsts* d_consts = (ModDownConsts*)((char*)w.dev + ws_bytes);
+    char* tab = (char*)w.dev + ws_bytes + mc_bytes;
+
+    std::map<const Job*, size_t> job_index;
+    for (size_t i = 0; i < w.jobs.size(); ++i) job_index[&w.jobs[i]] = i;
+    for (size_t g = 0; g < w.groups.size(); ++g) {
+        Group& G = w.groups[g];
+        IncNtt* t = G.t;
+        const long long N = (long long)t->pub.N;
+        const int s = (int)t->pub.split_degree;
+        const long long P = N / s;
+        const PrimeInfo* dinfo = t->d_info;
+        auto rows = [&](std::vector<RowDesc>& v, const uint64_t* in, uint64_t* out, uint32_t prime) {
+            for (int blk = 0; blk < s; ++blk) v.push_back(RowDesc{in + blk * P, out + blk * P, dinfo + prime, 0});
+        };
+        for (const Job* j : members[g]) {
+            uint64_t* tmp = wsp + ws_off[job_index[j]];
+            if (j->kind == 0) {
+                for (int l = 0; l < j->L; ++l) {
+                    rows(G.fwd, j->a + l * N, j->out + l * N, j->limbs[l]);
+                    rows(G.fwd, j->b + l * N, tmp + l * N, j->limbs[l]);
+                    G.prod.push_back(ProdDesc{j->out + l * N, tmp + l * N, j->out + l * N, dinfo + j->limbs[l]});
+                    rows(G.inv, j->out + l * N, j->out + l * N, j->limbs[l]);
+                }
+            } else {
+                const int nl = j->L, ne = nl + 1;
+                uint32_t ext[kMaxLimbs];
+                for (int i = 0; i < nl; ++i) ext[i] = j->limbs[i];
+                ext[nl] = j->special;
+                uint64_t* D = tmp;
+                uint64_t* acc = D + (long long)nl * ne * N;
+                for (int d = 0; d < nl; ++d)
+                    for (int e = 0; e < ne; ++e) rows(G.fwd, j->a + d * N, D + ((long long)d * ne + e) * N, ext[e]);
+                for (int e = 0; e < ne; ++e)
+                    G.mac.push_back(MacDesc{D + e * N, j->ksk + e * N, acc + e * N, dinfo + ext[e], nl, ne});
+                for (int c = 0; c < 2; ++c)
+                    for (int e = 0; e < ne; ++e)
+                        rows(G.inv, acc + ((long long)c * ne + e) * N, acc + ((long long)c * ne + e) * N, ext[e]);
+                const size_t ci = consts.size();
+                consts.push_back(moddown_consts(t, j->limbs, nl, j->special));
+                G.down.push_back(DownDesc{acc, j->out, nullptr, d_consts + ci, nl, 0});
+                G.down.push_back(DownDesc{acc + (long long)ne * N, j->out + (long long)nl * N, j->a + (long long)nl * N,
+                                          d_consts + ci, nl, 0});
+            }
+        }
+        auto place = [&](auto& v, auto*& dptr) {
+            using T = typename std::decay<decltype(v)>::type::value_type;
+            dptr = (T*)tab;
+            tab += align256(v.size() * sizeof(T));
+        };
+        place(G.fwd, G.d_fwd);
+        place(G.inv, G.d_inv);
+        place(G.prod, G.d_prod);
+        place(G.mac, G.d_mac);
+        place(G.down, G.d_down);
+    }
+    // upload constants and tables (once per compile)
+    if (nks && !check_cuda(cudaMemcpy(d_consts, consts.data(), nks * sizeof(ModDownConsts), cudaMemcpyHostToDevice),
+                           kWhere))
+        return 1;
+    for (Group& G : w.groups) {
+        if ((!G.fwd.empty() && !check_cuda(cudaMemcpy(G.d_fwd, G.fwd.data(), G.fwd.size() * sizeof(RowDesc),
+                                                      cudaMemcpyHostToDevice), kWhere)) ||
+            (!G.inv.empty() && !check_cuda(cudaMemcpy(G.d_inv, G.inv.data(), G.inv.size() * sizeof(RowDesc),
+                                                      cudaMemcpyHostToDevice), kWhere)) ||
+            (!G.prod.empty() && !check_cuda(cudaMemcpy(G.d_prod, G.prod.data(), G.prod.size() * sizeof(ProdDesc),
+                                                       cudaMemcpyHostToDevice), kWhere)) ||
+            (!G.mac.empty() && !check_cuda(cudaMemcpy(G.d_mac, G.mac.data(), G.mac.size() * sizeof(MacDesc),
+                                                      cudaMemcpyHostToDevice), kWhere)) ||
+            (!G.down.empty() && !check_cuda(cudaMemcpy(G.d_down, G.down.data(), G.down.size() * sizeof(DownDesc),
+                                                       cudaMemcpyHostToDevice), kWhere)))
+            return 1;
+    }
+
+    // capture: one branch per group, forked from and joined into one capture stream
+    const int G = (int)w.groups.size();
+    std::vector<cudaStream_t> gs(G, nullptr);
+    std::vector<cudaEvent_t> joins(G, nullptr);
+    cudaStream_t cs = nullptr;
+    cudaEvent_t fork = nullptr;
+    int err = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (!err) err = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    for (int g = 0; g < G && !err; ++g) {
+        err = cudaStreamCreateWithFlags(&gs[g], cudaStreamNonBlocking);
+        if (!err) err = cudaEventCreateWithFlags(&joins[g], cudaEventDisableTiming);
+    }
+    if (!err) err = prepare_ntt_kernels();
+    const uint64_t counted0 = launch_counter();
+    cudaGraph_t graph = nullptr;
+    if (!err) err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (!err) {
+        int cerr = cudaEventRecord(fork, cs);
+        for (int g = 0; g < G && !cerr; ++g) {
+            Group& Gr = w.groups[g];
+            IncNtt* t = Gr.t;
+            cudaStream_t q = gs[g];
+            const long long N = (long long)t->pub.N;
+            const int s = (int)t->pub.split_degree;
+            cerr = cudaStreamWaitEvent(q, fork, 0);
+            RowSet rs;
+            memset(&rs, 0, sizeof rs);
+            rs.logP = t->logP;
+            rs.split = s;
+            rs.fp64 = 1;
+            rs.reduce_input = 1;
+            rs.table = Gr.d_fwd;
+            rs.table_rows = (long long)Gr.fwd.size();
+            if (!cerr && rs.table_rows) cerr = launch_ntt(rs, t->d_info, false, q);
+            if (!cerr && !Gr.prod.empty()) {
+                const long long P = N / s;
+                const long long chunks = (P + kWlThreads - 1) / kWlThreads;
+                const unsigned grid = (unsigned)(chunks * (long long)Gr.prod.size());
+                switch (s) {
+                    case 1: k_wl_product<1><<<grid, kWlThreads, 0, q>>>(Gr.d_prod, chunks, t->logP); break;
+                    case 2: k_wl_product<2><<<grid, kWlThreads, 0, q>>>(Gr.d_prod, chunks, t->logP); break;
+                    case 4: k_wl_product<4><<<grid, kWlThreads, 0, q>>>(Gr.d_prod, chunks, t->logP); break;
+                    case 8: k_wl_product<8><<<grid, kWlThreads, 0, q>>>(Gr.d_prod, chunks, t->logP); break;
+                    case 16: k_wl_product<16><<<grid, kWlThreads, 0, q>>>(Gr.d_prod, chunks, t->logP); break;
+                    default: cerr = (int)cudaErrorInvalidValue;
+                }
+                if (!cerr) cerr = (int)cudaGetLastError();
+                note_launch();
+            }
+            if (!cerr && !Gr.mac.empty()) {
+                const long long chunks = (N + kWlThreads - 1) / kWlThreads;
+                k_wl_mac<<<(unsigned)(chunks * (long long)Gr.mac.size()), kWlThreads, 0, q>>>(Gr.d_mac, chunks, N, s);
+                cerr = (int)cudaGetLastError();
+                note_launch();
+            }
+            RowSet ri = rs;
+            ri.reduce_input = 0;
+            ri.table = Gr.d_inv;
+            ri.table_rows = (long long)Gr.inv.size();
+            if (!cerr && ri.table_rows) cerr = launch_ntt(ri, t->d_info, true, q);
+            if (!cerr && !Gr.down.empty()) {
+                const long long chunks = (N + kWlThreads - 1) / kWlThreads;
+                k_wl_moddown<<<(unsigned)(chunks * (long long)Gr.down.size()), kWlThreads, 0, q>>>(Gr.d_down, chunks,
+                                                                                                  N, t->d_info);
+                cerr = (int)cudaGetLastError();
+                note_launch();
+            }
+            if (!cerr) cerr = cudaEventRecord(joins[g], q);
+            if (!cerr) cerr = cudaStreamWaitEvent(cs, joins[g], 0);
+        }
+        const int e2 = cudaStreamEndCapture(cs, &graph);
+        err = cerr ? cerr : e2;
+    }
+    const uint64_t captured = launch_counter() - counted0;
+    forget_launches(captured);
+    if (!err) err = cudaGraphInstantiate(&w.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    for (int g = 0; g < G; ++g) {
+        if (gs[g]) cudaStreamDestroy(gs[g]);
+        if (joins[g]) cudaEventDestroy(joins[g]);
+    }
+    if (fork) cudaEventDestroy(fork);
+    if (cs) cudaStreamDestroy(cs);
+    if (err) {
+        check_cuda(err, kWhere);
+        w.exec = nullptr;
+        return 1;
+    }
+    w.launches_per_run = (int)captured;
+    return 0;
+}
+
+}  // namespace
+
+}  // namespace vc
+
+using vc::WorkList;
+
+extern "C" {
+
+void* vfhe_cuda_worklist_new(void) { return new WorkList(); }
+
+void vfhe_cuda_worklist_free(void* wl) {
+    WorkList* w = (WorkList*)wl;
+    if (!w) return;
+    w->release();
+    delete w;
+}
+
+int vfhe_cuda_worklist_add_chain(void* wl, void* ntt, uint64_t* d_out, const uint64_t* d_a, const uint64_t* d_b,
+                                 const uint32_t* limbs, uint32_t nlimbs) {
+    WorkList* w = (WorkList*)wl;
+    if (!w || !limbs || nlimbs == 0 || nlimbs > (uint32_t)vc::kMaxLimbs - 1) {
+        vc::set_error("vfhe_cuda_worklist_add_chain", "bad work list or limb list");
+        return 1;
+    }
+    vc::Job j;
+    memset(&j, 0, sizeof j);
+    j.kind = 0;
+    j.t = vc::as_ntt(ntt);
+    j.out = d_out;
+    j.a = d_a;
+    j.b = d_b;
+    j.L = (int)nlimbs;
+    memcpy(j.limbs, limbs, nlimbs * sizeof(uint32_t));
+    if (!vc::job_rows_ok(j)) {
+        vc::set_error("vfhe_cuda_worklist_add_chain",
+                      "limbs must be below 2^50 and inside the pool, rows 16-byte aligned, 2^8 <= P <= 2^17");
+        return 1;
+    }
+    w->release();
+    w->jobs.push_back(j);
+    return 0;
+}
+
+int vfhe_cuda_worklist_add_keyswitch(void* wl, void* ntt, uint64_t* d_out, const uint64_t* d_ct,
+                                     const uint32_t* limbs, uint32_t nlimbs, uint32_t special, const uint64_t* d_ksk) {
+    WorkList* w = (WorkList*)wl;
+    if (!w || !limbs || nlimbs == 0 || nlimbs > (uint32_t)vc::kMaxLimbs - 1) {
+        vc::set_error("vfhe_cuda_worklist_add_keyswitch", "bad work list or limb list");
+        return 1;
+    }
+    vc::Job j;
+    memset(&j, 0, sizeof j);
+    j.kind = 1;
+    j.t = vc::as_ntt(ntt);
+    j.out = d_out;
+    j.a = d_ct;
+    j.ksk = d_ksk;
+    j.L = (int)nlimbs;
+    j.special = special;
+    memcpy(j.limbs, limbs, nlimbs * sizeof(uint32_t));
+    if (!vc::job_rows_ok(j)) {
+        vc::set_error("vfhe_cuda_worklist_add_keyswitch",
+                      "limbs must be below 2^50 and inside the pool, rows 16-byte aligned, 2^8 <= P <= 2^17");
+        return 1;
+    }
+    w->release();
+    w->jobs.push_back(j);
+    return 0;
+}
+
+int vfhe_cuda_worklist_compile(void* wl) {
+    if (!vc::ensure_ready()) return 1;
+    WorkList* w = (WorkList*)wl;
+    if (!w || w->jobs.empty()) {
+        vc::set_error("vfhe_cuda_worklist_compile", "empty work list");
+        return 1;
+    }
+    return vc::compile(*w);
+}
+
+int vfhe_cuda_worklist_run(void* wl, void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    WorkList* w = (WorkList*)wl;
+    if (!w || w->jobs.empty()) {
+        vc::set_error("vfhe_cuda_worklist_run", "empty work list");
+        return 1;
+    }
+    if (!w->exec && vc::compile(*w)) return 1;
+    if (!vc::check_cuda(cudaGraphLaunch(w->exec, (cudaStream_t)stream_), "vfhe_cuda_worklist_run")) return 1;
+    vc::note_launch(w->launches_per_run);
+    return 0;
+}
+
+uint64_t vfhe_cuda_worklist_device_bytes(void* wl) {
+    WorkList* w = (WorkList*)wl;
+    return w ? (uint64_t)w->dev_bytes : 0;
+}
+
+int vfhe_cuda_worklist_launches(void* wl) {
+    WorkList* w = (WorkList*)wl;
+    return w ? w->launches_per_run : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,174 @@
+"""Uneven batched work list over the C ABI (vfhe_cuda_worklist_*).
+
+Jobs of any mix of ring degree N and limb count L -- NTT -> product -> INTT chains and
+GHS key switches -- are compiled once into device-resident row tables and one CUDA
+graph, then replayed with one launch per run.  ``run_per_call`` executes the same jobs
+one entry-point call each (vfhe_cuda_ntt_mul_intt_batch / vfhe_cuda_keyswitch_batch
+with batch 1): the plain path the work list is measured against, and its parity
+reference on the GPU.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .arith import Ring
+from .native import Engine, EngineError, cuda_engine
+
+
+def _ptr(ffi, t: torch.Tensor):
+    assert t.is_contiguous()
+    return ffi.cast("uint64_t*", t.data_ptr())
+
+
+@dataclass
+class Job:
+    """One work-list job.  chain: out = INTT(NTT(a) * NTT(b)), tensors [L][N];
+    keyswitch: out = GHS key switch of ct [2][L][N] with ksk [L][2][L+1][N]."""
+
+    kind: str
+    ring: Ring
+    L: int
+    limbs: list[int]
+    special: int | None
+    out: torch.Tensor
+    a: torch.Tensor
+    b: torch.Tensor | None = None
+    ksk: torch.Tensor | None = None
+    _limbs_c: object = field(default=None, repr=False)
+
+    @property
+    def N(self) -> int:
+        return self.ring.N
+
+    def bytes_moved(self) -> int:
+        """Algorithmic HBM bytes: inputs read once, outputs written once (keys read once)."""
+        n, L = self.ring.N, self.L
+        if self.kind == "chain":
+            return 8 * n * L * 3
+        return 8 * n * (2 * L + 2 * L + L * 2 * (L + 1))
+
+
+class WorkList:
+    """Compiled-once, replayed-many batch of independent jobs (one graph launch per run)."""
+
+    def __init__(self, engine: Engine | None = None):
+        self.engine = engine or cuda_engine()
+        self.ffi, self.lib = self.engine.ffi, self.engine.lib
+        self.handle = self.lib.vfhe_cuda_worklist_new()
+        self.jobs: list[Job] = []
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            self.engine.check(what)
+            raise EngineError(what)
+
+    def add(self, job: Job) -> None:
+        limbs = self.ffi.new("uint32_t[]", job.limbs)
+        job._limbs_c = limbs
+        if job.kind == "chain":
+            rc = self.lib.vfhe_cuda_worklist_add_chain(self.handle, job.ring.NTT, _ptr(self.ffi, job.out),
+                                                       _ptr(self.ffi, job.a), _ptr(self.ffi, job.b), limbs, job.L)
+        else:
+            rc = self.lib.vfhe_cuda_worklist_add_keyswitch(self.handle, job.ring.NTT, _ptr(self.ffi, job.out),
+                                                           _ptr(self.ffi, job.a), limbs, job.L, job.special,
+                                                           _ptr(self.ffi, job.ksk))
+        self._check(rc, "worklist_add")
+        self.jobs.append(job)
+
+    def compile(self) -> None:
+        self._check(self.lib.vfhe_cuda_worklist_compile(self.handle), "worklist_compile")
+
+    def run(self, stream: torch.cuda.Stream | None = None) -> None:
+        st = stream or torch.cuda.current_stream()
+        self._check(self.lib.vfhe_cuda_worklist_run(self.handle, self.ffi.cast("void*", st.cuda_stream)),
+                    "worklist_run")
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.vfhe_cuda_worklist_launches(self.handle))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.vfhe_cuda_worklist_device_bytes(self.handle))
+
+    def close(self) -> None:
+        if self.handle is not None:
+            self.lib.vfhe_cuda_worklist_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def per_call_workspace(engine: Engine, jobs: list[Job]) -> torch.Tensor:
+    need = max((engine.lib.vfhe_cuda_keyswitch_workspace_bytes(j.ring.NTT, 1, j.L) for j in jobs
+                if j.kind == "keyswitch"), default=8)
+    return torch.empty((need + 7) // 8, dtype=torch.int64, device="cuda")
+
+
+def run_per_call(engine: Engine, jobs: list[Job], outs: list[torch.Tensor], ws: torch.Tensor,
+                 stream: torch.cuda.Stream | None = None) -> int:
+    """The same jobs through the one-job-per-call entry points; returns the call count."""
+    ffi, lib = engine.ffi, engine.lib
+    st = ffi.cast("void*", (stream or torch.cuda.current_stream()).cuda_stream)
+    wsp = ffi.cast("void*", ws.data_ptr())
+    for j, o in zip(jobs, outs):
+        limbs = j._limbs_c if j._limbs_c is not None else ffi.new("uint32_t[]", j.limbs)
+        if j.kind == "chain":
+            rc = lib.vfhe_cuda_ntt_mul_intt_batch(j.ring.NTT, _ptr(ffi, o), _ptr(ffi, j.a), _ptr(ffi, j.b), 1,
+                                                  limbs, j.L, st)
+        else:
+            rc = lib.vfhe_cuda_keyswitch_batch(j.ring.NTT, _ptr(ffi, o), _ptr(ffi, j.a), 1, limbs, j.L, j.special,
+                                               _ptr(ffi, j.ksk), wsp, st)
+        if rc != 0:
+            engine.check("per-call job")
+            raise EngineError("per-call job")
+    return len(jobs)
+
+
+def uneven_jobs(engine: Engine, count: int = 512, seed: int = 3, logn: tuple[int, int] = (12, 16),
+                limbs: tuple[int, int] = (2, 24), device: str = "cuda") -> list[Job]:
+    """The uneven workload: N uniform over 2^logn[0]..2^logn[1], L uniform over
+    limbs[0]..limbs[1], half NTT->product->INTT chains and half key switches, every
+    residue uniform in [0, q) from a seeded generator.  Primes: the 50-bit primes of
+    Ring(N, prime_size=[50] * (L + 1)) at the ring's default split degree (the key
+    switch's special prime is the (L+1)-th)."""
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    rings: dict[int, Ring] = {}
+    jobs = []
+    for _ in range(count):
+        n = 1 << int(rng.integers(logn[0], logn[1] + 1))
+        L = int(rng.integers(limbs[0], limbs[1] + 1))
+        kind = "chain" if rng.random() < 0.5 else "keyswitch"
+        if n not in rings:
+            rings[n] = Ring(n, prime_size=[50] * (limbs[1] + 1), engine=engine)
+        R = rings[n]
+        idx = list(R.prime_indices[:L])
+        qs = R.primes[: L + 1]
+
+        def uniform(shape, prime_axis, nprimes):
+            t = torch.empty(shape, dtype=torch.int64, device=device)
+            for k in range(nprimes):
+                sl = [slice(None)] * len(shape)
+                sl[prime_axis] = k
+                t[tuple(sl)].random_(0, qs[k], generator=gen)
+            return t
+
+        if kind == "chain":
+            a = uniform((L, n), 0, L)
+            b = uniform((L, n), 0, L)
+            jobs.append(Job("chain", R, L, idx, None, torch.empty_like(a), a, b=b))
+        else:
+            ct = uniform((2, L, n), 1, L)
+            ksk = uniform((L, 2, L + 1, n), 2, L + 1)
+            jobs.append(Job("keyswitch", R, L, idx, R.prime_indices[L], torch.empty_like(ct), ct, ksk=ksk))
+    return jobs
