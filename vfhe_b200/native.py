@@ -93,8 +93,11 @@ _DEFAULT: Engine | None = None
 _CUDA: Engine | None = None
 
 
-def cuda_engine() -> Engine:
-    """The B200 engine.  Raises if the library was not built or no GPU is present."""
+def cuda_engine(apply_tuned: bool = True) -> Engine:
+    """The B200 engine.  Raises if the library was not built or no GPU is present.
+    On first load the tuned transform schedule (vfhe_b200/tuned/, written by
+    :mod:`vfhe_b200.autotune`) is applied when present and ``apply_tuned`` is set;
+    schedules change launch shapes only, never results."""
     global _CUDA
     if _CUDA is None:
         if not CUDA_LIB.exists():
@@ -106,6 +109,12 @@ def cuda_engine() -> Engine:
         if eng.lib.vfhe_cuda_device() < 0:
             msg = eng.ffi.string(eng.lib.vfhe_cuda_last_error()).decode()
             raise EngineError(f"cuda engine unavailable: {msg}")
+        if apply_tuned and not os.environ.get("VFHE_CUDA_NO_TUNED"):
+            from . import autotune
+
+            table = autotune.load()
+            if table:
+                autotune.apply(eng, table)
         _CUDA = eng
     return _CUDA
 
