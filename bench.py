@@ -257,6 +257,63 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
     return res
 
 
+def serving_leg(eng, requests: int, rates=(50.0, 200.0, 1000.0)) -> dict:
+    """Poisson request streams of mixed CKKS (N 2^13..2^16, L 4..24: multiply+relin+
+    rescale or rotate) and CGGI16 bootstrap batches (1..1024 LWEs, n = 630, N = 1024),
+    keys and ciphertexts resident in HBM, 160 GB budget: continuous batching (64 per
+    batch, 4 streams) vs the plain path (one request per call, one stream), p50/p99 and
+    throughput per arrival rate; plus CKKS multiply saturation at N = 2^14, L = 9."""
+    import torch
+
+    from vfhe_b200.serve import Server, ServingMix, poisson_arrivals, run_stream
+
+    mix = ServingMix(eng, seed=SEED + 5)
+    budget = 160 * 10**9
+    out = {"budget_bytes": budget, "resident_bytes": mix.resident, "requests_per_rate": requests,
+           "mix": "90% CKKS (half mul+relin+rescale, half rotate) over (2^13,4),(2^14,9),(2^15,16),(2^16,24); "
+                  "10% CGGI16 batches of 1..1024 LWEs (log-uniform), n=630, N=1024",
+           "rates": []}
+    reqs = mix.requests(requests, seed=SEED + 6, ckks_share=0.9)
+    p = mix.ckks[1]
+    sat = [("mul", 1, i % len(p.cts), (i + 1) % len(p.cts)) for i in range(256)]
+    modes = {"served": (4, 64), "plain": (1, 1)}
+    servers = {}
+    for name, (streams, mb) in modes.items():
+        srv = Server(budget, streams=streams, max_batch=mb, engine=eng)
+        mix.register(srv)
+        srv.reserve(16 * 10**9 if mb > 1 else 2 * 10**9)
+        # warm-up: every CGGI batch-size bucket once (captures its blind-rotation
+        # graph), a short mixed stream and a short multiply burst
+        for k in range(11):
+            run_stream(mix, srv, [("cggi", -1, 1 << k, 0)], np.zeros(1))
+        run_stream(mix, srv, reqs[:24], np.zeros(24))
+        run_stream(mix, srv, sat[:128], np.zeros(128))
+        servers[name] = srv
+    for rate in rates:
+        arr = poisson_arrivals(rate, len(reqs), np.random.default_rng(int(rate)))
+        row = {"rate_rps": rate}
+        for name, srv in servers.items():
+            b0 = srv.stats()["batches"]
+            r = run_stream(mix, srv, reqs, arr)
+            row[name] = {k: r[k] for k in ("p50_ms", "p99_ms", "mean_ms", "throughput_rps")}
+            row[name]["batches"] = int(srv.stats()["batches"] - b0)
+        out["rates"].append(row)
+    # saturation: 256 CKKS multiplies at the benchmark's parameters, all queued at t = 0
+    res = {}
+    for name, srv in servers.items():
+        b0 = srv.stats()["batches"]
+        r = run_stream(mix, srv, sat, np.zeros(len(sat)))
+        res[name] = {k: r[k] for k in ("p50_ms", "p99_ms", "throughput_rps")}
+        res[name]["batches"] = int(srv.stats()["batches"] - b0)
+    for srv in servers.values():
+        srv.close()
+    res["speedup"] = res["served"]["throughput_rps"] / res["plain"]["throughput_rps"]
+    out["ckks_mul_saturation_n2p14_L9"] = res
+    del mix
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_cuda_arm(args) -> None:
     import torch
 
@@ -406,6 +463,7 @@ def run_cuda_arm(args) -> None:
     eng.check("bench")
 
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
+    serving = None if args.no_serving else serving_leg(eng, args.serving_requests)
 
     if rank != 0:
         if dist is not None:
@@ -456,6 +514,8 @@ def run_cuda_arm(args) -> None:
     }
     if uneven is not None:
         line["uneven_worklist"] = uneven
+    if serving is not None:
+        line["serving"] = serving
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
@@ -475,6 +535,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU leg")
     ap.add_argument("--no-worklist", action="store_true", help="skip the uneven work-list leg")
     ap.add_argument("--worklist-jobs", type=int, default=512, help="jobs in the uneven work-list leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT))
     if args.impl == "reference":

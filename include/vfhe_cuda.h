@@ -410,6 +410,40 @@ int vfhe_cuda_worklist_run(void *wl, void *stream);
 uint64_t vfhe_cuda_worklist_device_bytes(void *wl);
 int vfhe_cuda_worklist_launches(void *wl);
 
+/* Serving loop (continuous batching on one GPU).  Requests name device-resident
+ * ciphertexts and keys; a native worker thread queues them per (operation, class),
+ * starts a batch whenever one of `nstreams` stream slots is free and the batch's
+ * scratch fits the HBM budget left (up to max_batch requests; CGGI requests merge up
+ * to the class's max_count ciphertexts), gathers inputs with device-to-device copies
+ * into stream-ordered scratch, runs one batched call, scatters the outputs and records
+ * a completion event.  Requests arriving meanwhile join the next batches.  CKKS
+ * ciphertext pointers must be 16-byte aligned.  reserve grows the server's memory
+ * pool ahead of time.  Latency =
+ * submission to observed completion (host steady clock).  max_batch = 1 with one
+ * stream is the plain one-call-per-request path.  Inputs must be complete on the
+ * device when submitted; outputs are complete when wait returns.  Results equal the
+ * batched entry points' (vfhe_cuda_ckks_mul_relin_rescale_batch, _rotate_batch,
+ * vfhe_cuda_cggi_bootstrap_batch) for every request, alone or mixed.  The worker
+ * is the only thread that may launch engine work while the server runs.
+ * No counterpart in the reference. */
+void *vfhe_cuda_server_new(uint64_t hbm_budget_bytes, uint32_t nstreams, uint32_t max_batch);
+void vfhe_cuda_server_free(void *server);
+int vfhe_cuda_server_note_resident(void *server, uint64_t bytes);
+int vfhe_cuda_server_reserve(void *server, uint64_t bytes);
+int vfhe_cuda_server_ckks_class(void *server, void *ntt, const uint32_t *limbs, uint32_t nlimbs, uint32_t special,
+                                const uint64_t *d_rlk);
+int vfhe_cuda_server_cggi_class(void *server, void *ntt, const uint32_t *limbs, uint32_t nlimbs, uint32_t special,
+                                uint32_t n, const uint64_t *d_bk, const uint64_t *d_tv, uint64_t torus_base,
+                                uint32_t max_count);
+int64_t vfhe_cuda_server_submit_ckks_mul(void *server, int cls, uint64_t *d_out, const uint64_t *d_ct1,
+                                         const uint64_t *d_ct2);
+int64_t vfhe_cuda_server_submit_ckks_rotate(void *server, int cls, uint64_t *d_out, const uint64_t *d_ct,
+                                            uint64_t gen, const uint64_t *d_gk);
+int64_t vfhe_cuda_server_submit_cggi(void *server, int cls, uint64_t *d_out_a, uint64_t *d_out_b,
+                                     const uint64_t *d_in_a, const uint64_t *d_in_b, uint64_t count);
+int vfhe_cuda_server_wait(void *server, int64_t id, double *latency_ms);
+int vfhe_cuda_server_stats(void *server, uint64_t *out5);
+
 #ifdef __cplusplus
 }
 #endif

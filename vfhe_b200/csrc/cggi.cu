@@ -319,7 +319,12 @@ int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* 
     if (!check_cuda(cudaGetLastError(), where)) return 1;
 
     // the n blind-rotation steps: one CUDA graph per (shape, buffers), replayed
-    static std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
+    struct Cached {
+        GraphKey key;
+        cudaGraphExec_t exec;
+        uint64_t launches;  // kernels per replay
+    };
+    static std::vector<Cached> graphs;
     GraphKey key;
     memset(&key, 0, sizeof key);
     const void* ptrs[8] = {t, acc, diff, D, ext, rots, bk, dp};
@@ -328,9 +333,15 @@ int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* 
     key.n = n;
     memcpy(key.primes, sh.ext_prime, sizeof key.primes);
     cudaGraphExec_t exec = nullptr;
+    uint64_t per_replay = 0;
     for (auto& g : graphs)
-        if (g.first == key) exec = g.second;
+        if (g.key == key) {
+            exec = g.exec;
+            per_replay = g.launches;
+        }
     if (!exec) {
+        if (!check_cuda(prepare_ntt_kernels(), where)) return 1;
+        const uint64_t counted0 = launch_counter();
         cudaStream_t cs = nullptr;
         if (!check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), where)) return 1;
         if (!check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), where)) return 1;
@@ -348,6 +359,8 @@ int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* 
         cudaGraph_t graph = nullptr;
         const cudaError_t e1 = cudaStreamEndCapture(cs, &graph);
         cudaStreamDestroy(cs);
+        per_replay = launch_counter() - counted0;  // counted at capture: taken back, noted per replay
+        forget_launches(per_replay);
         if (err || !check_cuda(e1, where)) {
             if (graph) cudaGraphDestroy(graph);
             if (err) check_cuda(err, where);
@@ -356,10 +369,10 @@ int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* 
         const cudaError_t e2 = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         if (!check_cuda(e2, where)) return 1;
-        graphs.emplace_back(key, exec);
+        graphs.push_back(Cached{key, exec, per_replay});
     }
     if (!check_cuda(cudaGraphLaunch(exec, st), where)) return 1;
-    note_launch((int)(5 * n));
+    note_launch((int)per_replay);
     k_extract0<<<cg_grid(N, B * L0), 256, 0, st>>>(out_a, out_b, acc, sh, dp);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }

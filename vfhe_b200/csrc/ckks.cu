@@ -334,8 +334,7 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
 
     std::vector<const uint64_t*> kp(B, rlk);
-    if (!check_cuda(cudaMemcpyAsync(keyptrs, kp.data(), B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where))
-        return 1;
+    if (!check_cuda(upload_small(keyptrs, (const uint64_t*)kp.data(), B, st), where)) return 1;
     k_tensor<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N,
                                                             (int)t->pub.split_degree);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
@@ -381,12 +380,10 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     uint64_t* acc = D + B * (uint64_t)nl * ne * N;      // [B][2][ne][N]
     uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
     uint64_t* d_gens = keyptrs + B;                     // [B]
-    if (!check_cuda(cudaMemcpyAsync(keyptrs, gks, B * sizeof(uint64_t*), cudaMemcpyHostToDevice, st), where))
-        return 1;
+    if (!check_cuda(upload_small(keyptrs, (const uint64_t*)gks, B, st), where)) return 1;
     const uint64_t* src = ct;
     if (gens) {
-        if (!check_cuda(cudaMemcpyAsync(d_gens, gens, B * sizeof(uint64_t), cudaMemcpyHostToDevice, st), where))
-            return 1;
+        if (!check_cuda(upload_small(d_gens, gens, B, st), where)) return 1;
         k_permute_batch<<<grid_xy(N, (long long)B * 2 * nl), 256, 0, st>>>(Pm, ct, d_gens, lp, t->d_info, nl, N, ls);
         if (!check_cuda(cudaGetLastError(), where)) return 1;
         src = Pm;

@@ -151,6 +151,12 @@ struct EwSet {
 
 int launch_ew(EwOp op, const EwSet& set, const PrimeInfo* d_primes, cudaStream_t st);
 
+// Copy a small host array (pointers, Galois elements) into device memory through
+// kernel parameters: stream-ordered and asynchronous for the host, unlike a
+// cudaMemcpyAsync from pageable memory, which first waits for the stream to drain.
+// Values go 256 per launch.
+int upload_small(uint64_t* d_dst, const uint64_t* h_src, uint64_t n, cudaStream_t st);
+
 // Incomplete (split-degree) product, rns_polynomial.c:311-435.  mode: 0 set, 1 add, 2 sub.
 int launch_inc_product(int mode, const EwSet& set, int split, int logP, const PrimeInfo* d_primes,
                        cudaStream_t st);

@@ -3,6 +3,7 @@
 // and the engine's sampling.  All are HBM-bound streaming kernels: one thread per
 // residue (grid-stride), limbs and polynomials of a batch on gridDim.y.
 #include <cuda_runtime.h>
+#include <string.h>
 #include <math.h>
 
 #include "engine.cuh"
@@ -302,6 +303,28 @@ int launch_sample_gaussian(const EwSet& set, double sigma, uint64_t seed, uint64
     if (set.nlimbs <= 0) return 0;
     k_gaussian<<<ew_grid(set), kThreads, 0, st>>>(set, d_primes, sigma, seed, counter);
     return (int)cudaGetLastError();
+}
+
+namespace {
+struct SmallBlock {
+    uint64_t v[256];
+};
+__global__ void k_upload_small(uint64_t* __restrict__ dst, const __grid_constant__ SmallBlock blk, int n) {
+    if ((int)threadIdx.x < n) dst[threadIdx.x] = blk.v[threadIdx.x];
+}
+}  // namespace
+
+int upload_small(uint64_t* d_dst, const uint64_t* h_src, uint64_t n, cudaStream_t st) {
+    for (uint64_t off = 0; off < n; off += 256) {
+        SmallBlock blk;
+        const int m = (int)(n - off < 256 ? n - off : 256);
+        memcpy(blk.v, h_src + off, (size_t)m * sizeof(uint64_t));
+        k_upload_small<<<1, 256, 0, st>>>(d_dst + off, blk, m);
+        note_launch();
+        const int e = (int)cudaGetLastError();
+        if (e) return e;
+    }
+    return 0;
 }
 
 }  // namespace vc
