@@ -410,6 +410,35 @@ int vfhe_cuda_worklist_run(void *wl, void *stream);
 uint64_t vfhe_cuda_worklist_device_bytes(void *wl);
 int vfhe_cuda_worklist_launches(void *wl);
 
+/* CGGI over the 32-bit torus with FP64 FFT external products (the TFHE bootstrap,
+ * Chillotti et al., J. Cryptology 33, 2020, with the reference's CGGI16 blind-rotation
+ * orchestration, cggi16.py:46-128).  Torus values are uint32; a rank-1 GLWE (a, b) of
+ * degree N (512, 1024 or 2048) has phase b - a S; gadget: base 2^base_log, `levels`
+ * levels (<= 4), signed digits.  No counterpart in the reference: its CGGI16 uses the
+ * RNS gadget (vfhe_cuda_cggi_bootstrap_batch above) and its LWE key switch is a stub.
+ *
+ * to_fourier: spectra d_out [count][N/2] complex doubles (re, im) of rows
+ *   d_rows [count][N] read as signed 32-bit coefficients (bootstrapping-key rows).
+ * bootstrap_batch: d_in [batch][n+1] LWEs (mask, body) -> d_out [batch][N+1]
+ *   extracted LWEs; d_bsk_f [n][2 levels][2][N/2] spectra of GGSW(s_i), row (c, l) at
+ *   c * levels + l; d_tv [N] test vector; rotation offset 2^32 / (4 torus_base).
+ *   One persistent launch: every CTA runs whole blind rotations with its accumulator
+ *   in shared memory.
+ * keyswitch_batch: d_in [batch][N+1] -> d_out [batch][n+1] with d_ksk [N][levels][n+1]
+ *   (base 2^base_log, signed digits); exact integer arithmetic.
+ * external_product: d_out[b] = ExtProd(GGSW spectra d_ggsw_f, GLWE d_c[b] [2][N]) rounded
+ *   to integers, and d_frac[b] = the largest distance of an unrounded coefficient to its
+ *   integer (NULL to skip), for measuring the FFT error against exact products. */
+int vfhe_cuda_cggi_fft_to_fourier(double *d_out, const uint32_t *d_rows, uint64_t count, uint32_t N, void *stream);
+int vfhe_cuda_cggi_fft_bootstrap_batch(uint32_t *d_out, const uint32_t *d_in, uint64_t batch, const double *d_bsk_f,
+                                       const uint32_t *d_tv, uint32_t n, uint32_t N, uint32_t base_log,
+                                       uint32_t levels, uint32_t torus_base, void *stream);
+int vfhe_cuda_cggi_fft_keyswitch_batch(uint32_t *d_out, const uint32_t *d_in, uint64_t batch, const uint32_t *d_ksk,
+                                       uint32_t N, uint32_t n, uint32_t base_log, uint32_t levels, void *stream);
+int vfhe_cuda_cggi_fft_external_product(uint32_t *d_out, const uint32_t *d_c, uint64_t batch, const double *d_ggsw_f,
+                                        uint32_t N, uint32_t base_log, uint32_t levels, double *d_frac,
+                                        void *stream);
+
 /* Serving loop (continuous batching on one GPU).  Requests name device-resident
  * ciphertexts and keys; a native worker thread queues them per (operation, class),
  * starts a batch whenever one of `nstreams` stream slots is free and the batch's

@@ -34,6 +34,35 @@ def build_oracle() -> Path:
     return ORACLE_LIB
 
 
+TORUS_SRC = ROOT / "oracle" / "cggi_torus_oracle.c"
+TORUS_LIB = ROOT / "oracle" / "_build" / "libcggi_torus_oracle.so"
+
+
+def build_torus_oracle() -> Path:
+    """Compile the exact-integer torus CGGI oracle if missing or stale."""
+    if not TORUS_LIB.exists() or TORUS_LIB.stat().st_mtime < TORUS_SRC.stat().st_mtime:
+        TORUS_LIB.parent.mkdir(exist_ok=True)
+        subprocess.run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-o", str(TORUS_LIB), str(TORUS_SRC)],
+                       check=True)
+    return TORUS_LIB
+
+
+@pytest.fixture(scope="session")
+def torus_oracle():
+    """ctypes handle on the exact torus CGGI oracle (checker only)."""
+    import ctypes
+
+    lib = ctypes.CDLL(str(build_torus_oracle()))
+    u32p, i32p = ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_int32)
+    lib.tor_external_product.argtypes = [u32p, u32p, u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.tor_bootstrap.argtypes = [u32p, u32p, ctypes.c_uint32, u32p, u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_uint32]
+    lib.tor_keyswitch.argtypes = [u32p, u32p, u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.tor_negacyclic_mac.argtypes = [u32p, i32p, u32p, ctypes.c_int]
+    lib.tor_decompose.argtypes = [i32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
+    return lib
+
+
 @pytest.fixture(scope="session")
 def oracle_engine():
     from vfhe_b200.native import Engine
