@@ -257,6 +257,70 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
     return res
 
 
+def cggi_fft_leg(eng, count: int, reps: int, million: bool = False) -> dict:
+    """Torus CGGI programmable bootstrap (n = 630, N = 1024, base 2^7 x 3, key switch
+    2^2 x 8): `count` LWEs of random 4-bit messages through one seeded 16-entry table
+    per batch; bootstraps/s, LUT mismatches and phase error (torus fractions)."""
+    import torch
+
+    from vfhe_b200.cggi_fft import CggiFft, TorusKeys, TorusParams, test_vector, to_device, to_host
+
+    p = TorusParams()
+    rng = np.random.default_rng(SEED + 9)
+    keys = TorusKeys.generate(p, rng)
+    dev = CggiFft(keys, eng)
+    lut = rng.integers(0, p.t, p.t)
+    tv = to_device(test_vector(lut, p))
+    m = rng.integers(0, p.t, count)
+    lwe = to_device(keys.encrypt(m, rng))
+    dev.bootstrap(lwe[:256], tv)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        ext = dev.blind_rotate(lwe, tv)
+    ev[1].record(stream)
+    for _ in range(reps):
+        out = dev.keyswitch(ext)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    br_ms = ev[0].elapsed_time(ev[1]) / reps
+    ks_ms = ev[1].elapsed_time(ev[2]) / reps
+    res_host, ext_host = to_host(out), to_host(ext)
+    err = np.abs(keys.phases(res_host) - lut[m] * p.delta) / 2.0**32
+    err_ext = np.abs(keys.phases(ext_host, keys.S) - lut[m] * p.delta) / 2.0**32
+    res = {
+        "workload": f"{count} LWEs, n=630 binary key sigma 2^-15; GLWE N=1024 k=1 binary key sigma 2^-25; "
+                    "gadget 2^7 x 3; key switch 2^2 x 8 (key noise sigma 2^-15); 4-bit messages + padding, "
+                    "16-entry LUT",
+        "bootstraps_per_s": count / ((br_ms + ks_ms) * 1e-3), "blind_rotation_ms": br_ms, "keyswitch_ms": ks_ms,
+        "checked": count, "box_half_width": 0.5 / (2 * p.t),
+        # after blind rotation + extraction (key S): the bootstrap's own noise
+        "mismatches_extracted": int((keys.decrypt(ext_host, keys.S) != lut[m]).sum()),
+        "phase_error_extracted_mean": float(err_ext.mean()), "phase_error_extracted_max": float(err_ext.max()),
+        # after the key switch back to s: adds the key-switching key's noise
+        "mismatches": int((keys.decrypt(res_host) != lut[m]).sum()),
+        "phase_error_mean": float(err.mean()), "phase_error_max": float(err.max()),
+    }
+    if million:
+        total, bad, bad_ext, worst, worst_ext = 0, 0, 0, 0.0, 0.0
+        while total < 1_000_000:
+            mm = rng.integers(0, p.t, count)
+            e = dev.blind_rotate(to_device(keys.encrypt(mm, rng)), tv)
+            o, eh = to_host(dev.keyswitch(e)), to_host(e)
+            bad += int((keys.decrypt(o) != lut[mm]).sum())
+            bad_ext += int((keys.decrypt(eh, keys.S) != lut[mm]).sum())
+            worst = max(worst, float((np.abs(keys.phases(o) - lut[mm] * p.delta) / 2.0**32).max()))
+            worst_ext = max(worst_ext, float((np.abs(keys.phases(eh, keys.S) - lut[mm] * p.delta) / 2.0**32).max()))
+            total += count
+        res["million"] = {"bootstraps": total, "mismatches_extracted": bad_ext, "phase_error_extracted_max": worst_ext,
+                          "mismatches": bad, "phase_error_max": worst}
+    del dev
+    torch.cuda.empty_cache()
+    return res
+
+
 def serving_leg(eng, requests: int, rates=(50.0, 200.0, 1000.0)) -> dict:
     """Poisson request streams of mixed CKKS (N 2^13..2^16, L 4..24: multiply+relin+
     rescale or rotate) and CGGI16 bootstrap batches (1..1024 LWEs, n = 630, N = 1024),
@@ -464,6 +528,7 @@ def run_cuda_arm(args) -> None:
 
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
     serving = None if args.no_serving else serving_leg(eng, args.serving_requests)
+    cggi_fft = None if args.no_cggi else cggi_fft_leg(eng, 4096, reps=3, million=args.cggi_million)
 
     if rank != 0:
         if dist is not None:
@@ -516,6 +581,8 @@ def run_cuda_arm(args) -> None:
         line["uneven_worklist"] = uneven
     if serving is not None:
         line["serving"] = serving
+    if cggi_fft is not None:
+        line["cggi_fft_bootstrap"] = cggi_fft
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
@@ -536,6 +603,9 @@ def main() -> None:
     ap.add_argument("--no-worklist", action="store_true", help="skip the uneven work-list leg")
     ap.add_argument("--worklist-jobs", type=int, default=512, help="jobs in the uneven work-list leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--no-cggi", action="store_true", help="skip the torus CGGI bootstrap leg")
+    ap.add_argument("--cggi-million", action="store_true",
+                    help="also bootstrap 10^6 LWEs and count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT))

@@ -42,7 +42,7 @@ def build_torus_oracle() -> Path:
     """Compile the exact-integer torus CGGI oracle if missing or stale."""
     if not TORUS_LIB.exists() or TORUS_LIB.stat().st_mtime < TORUS_SRC.stat().st_mtime:
         TORUS_LIB.parent.mkdir(exist_ok=True)
-        subprocess.run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-o", str(TORUS_LIB), str(TORUS_SRC)],
+        subprocess.run(["gcc", "-O3", "-std=gnu11", "-fPIC", "-shared", "-o", str(TORUS_LIB), str(TORUS_SRC)],
                        check=True)
     return TORUS_LIB
 

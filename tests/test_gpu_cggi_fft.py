@@ -94,3 +94,22 @@ def test_programmable_bootstrap_full_parameters(cuda):
     assert np.array_equal(keys.decrypt(out), lut[m])
     err = np.abs(keys.phases(out) - lut[m] * p.delta)
     assert err.max() < p.delta // 2  # every phase inside its box
+
+
+def test_full_parameter_blind_rotation_matches_exact(cuda, torus_oracle):
+    """n = 630: the GPU's FFT blind rotation and the exact-integer one decrypt alike and
+    differ by far less than the bootstrapping noise."""
+    from vfhe_b200.cggi_fft import CggiFft, test_vector, to_device, to_host
+
+    p, keys = _keys(630, 1024, 17)
+    dev = CggiFft(keys, cuda)
+    rng = np.random.default_rng(18)
+    lut = rng.integers(0, p.t, p.t)
+    tv = test_vector(lut, p)
+    m = rng.integers(0, p.t, 2)
+    lwe = keys.encrypt(m, rng)
+    got = to_host(dev.blind_rotate(to_device(lwe), to_device(tv)))
+    want = oracle_bootstrap(torus_oracle, lwe, tv, keys.bsk, p)
+    assert int(torus_distance(got, want).max()) < 1 << 14  # 2^-18 of the torus
+    assert np.array_equal(keys.decrypt(got, keys.S), keys.decrypt(want, keys.S))
+    assert np.array_equal(keys.decrypt(want, keys.S), lut[m])
