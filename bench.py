@@ -209,6 +209,23 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line))
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The slowest rank's time: every rank enters this reduction in the same order."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, world: int, ms: float) -> float:
+    """Units per second over all ranks (weak scaling: every rank does units_per_rank)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 # ----------------------------------------------------------------------------- gpu arm
 def worklist_leg(eng, count: int, reps: int) -> dict:
     """Uneven batch: `count` jobs, N in 2^12..2^16, L in 2..24, half NTT->product->INTT
@@ -444,12 +461,8 @@ def run_cuda_arm(args) -> None:
         barrier()
         torch.cuda.profiler.stop()
     launches = eng.lib.vfhe_cuda_launch_count() - launches0
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * PAIRS / (ms * 1e-3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, "cuda")
+    value = whole_job_rate(PAIRS, world, ms)
 
     # ---- end to end: pinned host inputs in, host results out, every step
     h1 = torch.from_numpy(host1.view(np.int64)).pin_memory()
@@ -465,19 +478,13 @@ def run_cuda_arm(args) -> None:
 
     e2e_step()
     barrier()
-    t0 = time.perf_counter()
     ev0.record(stream)
     for _ in range(e2e_steps):
         e2e_step()
     ev1.record(stream)
     barrier()
-    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * PAIRS / (e2e_ms * 1e-3)
-    _ = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, dist, "cuda")
+    e2e_value = whole_job_rate(PAIRS, world, e2e_ms)
 
     # ---- dominant kernel: the digit transforms (B x (L+1) rows of N = 2^14 per launch)
     ffi = eng.ffi
