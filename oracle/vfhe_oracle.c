@@ -962,3 +962,108 @@ void *lwe_new_trivial_sample(uint64_t *m, uint64_t n, uint64_t l, void *ntt)
     for (uint64_t i = 0; i < l; i++) c->b[i] = m ? m[i] : 0;
     return c;
 }
+
+/* ------------------------------------------------------------ complex FFT (CKKS encoding) */
+/* Scalar restatement of modules/arith/c/src/complex.c (the reference's portable build,
+ * complex.c:360-440): split real/imaginary layout, twiddles ws[0][m + i] / ws[1][m + i],
+ * every product and sum rounded separately (build with -ffp-contract=off). */
+#include <math.h>
+
+static uint32_t brv20(uint32_t x, uint32_t prec) /* complex.c:13-24 */
+{
+    uint32_t r = 0;
+    for (int b = 0; b < 20; ++b) r |= ((x >> b) & 1u) << (19 - b);
+    return r >> (20 - prec);
+}
+
+void bit_reverse_array(double *v, uint64_t N, uint32_t prec) /* complex.c:26-39 */
+{
+    double *tmp = (double *)malloc(N * sizeof(double));
+    for (int h = 0; h < 2; ++h) {
+        for (uint64_t i = 0; i < N; i++) tmp[brv20((uint32_t)i, prec)] = v[h * N + i];
+        memcpy(v + h * N, tmp, N * sizeof(double));
+    }
+    free(tmp);
+}
+
+void complex_poly_scale_double(double *v, double scale, uint64_t N) /* complex.c:366-370 */
+{
+    for (uint64_t i = 0; i < 2 * N; i++) v[i] *= scale;
+}
+
+static void *load_rous(double *re, double *im, uint64_t size) /* complex.c:371-387 */
+{
+    double **w = (double **)malloc(2 * sizeof(double *));
+    w[0] = (double *)malloc(size * sizeof(double));
+    w[1] = (double *)malloc(size * sizeof(double));
+    memcpy(w[0], re, size * sizeof(double));
+    memcpy(w[1], im, size * sizeof(double));
+    return w;
+}
+void *load_rous_CT(double *re, double *im, uint64_t size) { return load_rous(re, im, size); }
+void *load_rous_GS(double *re, double *im, uint64_t size) { return load_rous(re, im, size); }
+
+void CT_NR(double *x, void *pws, uint64_t n) /* complex.c:389-412 */
+{
+    double **ws = (double **)pws;
+    double *re = x, *im = x + n;
+    for (uint64_t t = n, m = 1; m < n; m <<= 1) {
+        t >>= 1;
+        for (uint64_t i = 0; i < m; i++) {
+            const double wr = ws[0][m + i], wi = ws[1][m + i];
+            for (uint64_t j = 2 * i * t; j < 2 * i * t + t; j++) {
+                const double vi = re[j + t] * wi + wr * im[j + t];
+                const double vr = re[j + t] * wr - im[j + t] * wi;
+                re[j + t] = re[j] - vr;
+                im[j + t] = im[j] - vi;
+                re[j] += vr;
+                im[j] += vi;
+            }
+        }
+    }
+}
+
+void GS_RN(double *x, void *pws, uint64_t n) /* complex.c:414-440 */
+{
+    double **ws = (double **)pws;
+    double *re = x, *im = x + n;
+    for (uint64_t t = 1, m = n; m > 1; t <<= 1, m >>= 1) {
+        const uint64_t h = m >> 1;
+        for (uint64_t i = 0; i < h; i++) {
+            const double wr = ws[0][h + i], wi = ws[1][h + i];
+            for (uint64_t j = 2 * i * t; j < 2 * i * t + t; j++) {
+                const double vr = re[j] - re[j + t], vi = im[j] - im[j + t];
+                re[j] += re[j + t];
+                im[j] += im[j + t];
+                im[j + t] = vr * wi + wr * vi;
+                re[j + t] = vr * wr - vi * wi;
+            }
+        }
+    }
+}
+
+void complex_poly_round_to_RNS(void *out, double *in, uint64_t N) /* complex.c:41-52 */
+{
+    (void)N;
+    RNS_Polynomial o = (RNS_Polynomial)out;
+    const uint64_t n = o->ntt->N;
+    uint64_t *tmp = (uint64_t *)malloc(n * sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; i++) tmp[i] = (uint64_t)(int64_t)llrint(in[i]);
+    int_array_to_RNS(o, tmp);
+    free(tmp);
+}
+
+/* complex.c:458-476 (one thread) */
+void complex_polys_ifft_scale_round_to_RNS_batch(void **rows_in, void **outs_rns, uint64_t count,
+                                                 uint64_t n_complex, uint32_t log_prec, void *gs_ws,
+                                                 double temp_delta)
+{
+    const double scale = temp_delta / (double)n_complex;
+    for (uint64_t i = 0; i < count; i++) {
+        double *row = (double *)rows_in[i];
+        bit_reverse_array(row, n_complex, log_prec);
+        GS_RN(row, gs_ws, n_complex);
+        complex_poly_scale_double(row, scale, n_complex);
+        complex_poly_round_to_RNS(outs_rns[i], row, n_complex);
+    }
+}

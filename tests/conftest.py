@@ -28,7 +28,7 @@ def build_oracle() -> Path:
     if not ORACLE_LIB.exists() or ORACLE_LIB.stat().st_mtime < ORACLE_SRC.stat().st_mtime:
         ORACLE_LIB.parent.mkdir(exist_ok=True)
         subprocess.run(
-            ["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-o", str(ORACLE_LIB), str(ORACLE_SRC)],
+            ["gcc", "-O2", "-std=gnu11", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(ORACLE_LIB), str(ORACLE_SRC), "-lm"],
             check=True,
         )
     return ORACLE_LIB

@@ -122,6 +122,31 @@ void ew_mask(EwOp op, Poly* out, Poly* a, Poly* b, uint64_t mask, const char* wh
 
 }  // namespace
 
+namespace vc {
+
+// Signed 64-bit integers (device array of N) into every active limb of `out`, in the
+// ring's coefficient layout, then the forward transform (int_array_to_RNS,
+// rns_polynomial.c:199-238).  Enqueued on `st` (the engine stream).
+int int_array_to_RNS_device(void* out, const int64_t* d_in, cudaStream_t st) {
+    Poly* o = as_poly(out);
+    IncNtt* t = pool_of(o);
+    const uint64_t N = t->pub.N;
+    prefetch_poly(o);
+    EwSet s = poly_set(o, nullptr, nullptr, o->pub.rns_mask);
+    for (int k = 0; k < s.nlimbs; ++k) s.a[k] = (const uint64_t*)d_in;
+    int ls = 0;
+    while ((1ULL << ls) < t->pub.split_degree) ++ls;
+    if (s.nlimbs) {
+        k_scatter<true><<<grid_for((long long)N, s.nlimbs), 256, 0, st>>>(s, t->d_info, (int)t->pub.split_degree, ls,
+                                                                        (long long)t->P);
+        const int e = (int)cudaGetLastError();
+        if (e) return e;
+    }
+    return poly_ntt(o, o, o->pub.rns_mask, false);
+}
+
+}  // namespace vc
+
 extern "C" {
 
 void* safe_aligned_malloc(uint64_t size) {
@@ -171,23 +196,11 @@ void polynomial_copy_RNS_polynomial(void* out, void* in) {
 void int_array_to_RNS(void* out, uint64_t* in) {
     VC_ENTER("int_array_to_RNS");
     if (!valid_poly(out, vc_where_) || !in) return;
-    Poly* o = as_poly(out);
-    IncNtt* t = pool_of(o);
-    const uint64_t N = t->pub.N;
+    const uint64_t N = pool_of(as_poly(out))->pub.N;
     uint64_t* d_in = (uint64_t*)device_alloc(N * 8);
     if (!d_in) return;
     VC_CHECK(cudaMemcpyAsync(d_in, in, N * 8, cudaMemcpyHostToDevice, stream()));
-    prefetch_poly(o);
-    EwSet s = poly_set(o, nullptr, nullptr, o->pub.rns_mask);
-    for (int k = 0; k < s.nlimbs; ++k) s.a[k] = d_in;
-    int ls = 0;
-    while ((1ULL << ls) < t->pub.split_degree) ++ls;
-    if (s.nlimbs) {
-        k_scatter<true><<<grid_for((long long)N, s.nlimbs), 256, 0, stream()>>>(
-            s, t->d_info, (int)t->pub.split_degree, ls, (long long)t->P);
-        VC_CHECK(cudaGetLastError());
-    }
-    VC_CHECK(poly_ntt(o, o, o->pub.rns_mask, false));
+    VC_CHECK(vc::int_array_to_RNS_device(out, (const int64_t*)d_in, stream()));
     VC_FINISH();
     device_free(d_in);
 }

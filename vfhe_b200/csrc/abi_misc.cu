@@ -1,6 +1,6 @@
 // misc.cdef / vfhe_cpu.cdef surface, RNS base conversion, and the parts of the
 // reference surface that lie outside this engine's hot path (multiprecision, field
-// extensions, GP25, CKKS complex FFT).  The latter exist so that a cffi module built
+// extensions, GP25).  The latter exist so that a cffi module built
 // from the reference cdefs links against this library; calling one records an error.
 #include <cuda_runtime.h>
 #include <stdlib.h>
@@ -172,28 +172,7 @@ void polynomial_base_conversion_RNSc(void* out, void* in, void* params) {
     VC_FINISH();
 }
 
-// ---- complex FFT (CKKS encode/decode): not yet provided by this engine
-void* load_rous_CT(double* rous_real, double* rous_imag, uint64_t size) {
-    (void)rous_real; (void)rous_imag; (void)size;
-    unsupported("load_rous_CT");
-    return nullptr;
-}
-void* load_rous_GS(double* rous_real, double* rous_imag, uint64_t size) {
-    (void)rous_real; (void)rous_imag; (void)size;
-    unsupported("load_rous_GS");
-    return nullptr;
-}
-void CT_NR(double* x, void* ws, uint64_t n) { (void)x; (void)ws; (void)n; unsupported("CT_NR"); }
-void GS_RN(double* x, void* ws, uint64_t n) { (void)x; (void)ws; (void)n; unsupported("GS_RN"); }
-void bit_reverse_array(double* v, uint64_t N, uint32_t prec) { (void)v; (void)N; (void)prec; unsupported("bit_reverse_array"); }
-void complex_poly_scale_double(double* v, double scale, uint64_t N) { (void)v; (void)scale; (void)N; unsupported("complex_poly_scale_double"); }
-void complex_poly_round_to_RNS(void* out, double* in, uint64_t N) { (void)out; (void)in; (void)N; unsupported("complex_poly_round_to_RNS"); }
-void complex_polys_ifft_scale_round_to_RNS_batch(void** rows_in, void** outs_rns, uint64_t count,
-                                                 uint64_t n_complex, uint32_t log_prec, void* gs_ws,
-                                                 double temp_delta) {
-    (void)rows_in; (void)outs_rns; (void)count; (void)n_complex; (void)log_prec; (void)gs_ws; (void)temp_delta;
-    unsupported("complex_polys_ifft_scale_round_to_RNS_batch");
-}
+// ---- complex FFT (CKKS encoding): complex_fft.cu
 
 // ---- multiprecision (portable layout: one uint64 per digit vector)
 int get_mp_vector_size(void) { return 1; }

@@ -2,103 +2,19 @@
 
 Host-side mirror of the reference's ``vfhe.fhe`` surface
 (modules/fhe/python/src/vfhe/fhe/ckks.py, cggi16.py).  Ciphertext arithmetic is
-engine calls.  CKKS encode/decode are the client-side special FFT of
-modules/arith/python/src/vfhe/arith/complex.py restated in numpy (the same roots,
-stage order and scaling); they are approximate FP64 maps whose last bits may differ
-from the reference's AVX-512 FMA kernels, which is why the parity tests inject the
-encoded plaintext rather than re-encoding it on each engine.
+engine calls; CKKS encode/decode drive the engine's complex special FFT through
+:mod:`vfhe_b200.complex` exactly as the reference does (on the cuda engine those
+transforms run on the GPU with the reference's scalar rounding).
 """
 
 from __future__ import annotations
 
-import functools
 import math
 
-import numpy as np
-
 from .arith import Polynomial, Ring, repr
+from .complex import ComplexPolynomial, ComplexRing
 from .mlwe import CMUX, LWE, MGSW_Scheme, MLWE, MLWE_Key, MLWE_Scheme, MLWE_Set
 from .numbers import crt
-
-
-@functools.lru_cache(maxsize=16)
-def special_roots(n2: int) -> tuple[np.ndarray, np.ndarray]:
-    """CKKS "special" roots for the n2/4-slot FFT and their inverses (complex.py:90-106).
-
-    Entry 2^(k-1)+i holds w^((5^brv(i)) n2 / 2^(k+1)) with w = exp(2 pi i / 2 n2);
-    computed with 100-bit mpmath and rounded to complex128, as the reference does.
-    """
-    import mpmath as mp
-
-    mp.mp.prec = 100
-    w = mp.exp(2 * mp.pi * 1j / (2 * mp.mpf(n2)))
-    res = [mp.mpc(1)] * n2
-    logn = int(math.log2(n2))
-    for k in range(logn - 1, 0, -1):
-        for i in range(2 ** (k - 1)):
-            b = int(bin(i)[2:].rjust(k - 1, "0")[::-1], 2) if k > 1 else 0
-            e = ((5**b) * n2 // (2 ** (k + 1))) % (2 * n2)
-            res[2 ** (k - 1) + i] = mp.power(w, e)
-    fwd = np.array([complex(x) for x in res], dtype=np.complex128)
-    inv = np.array([complex(x**-1) for x in res], dtype=np.complex128)
-    return fwd, inv
-
-
-def _brv_perm(n: int) -> np.ndarray:
-    logn = int(math.log2(n))
-    idx = np.arange(n)
-    r = np.zeros(n, dtype=np.int64)
-    for b in range(logn):
-        r |= ((idx >> b) & 1) << (logn - 1 - b)
-    return r
-
-
-def _ct_nr(x: np.ndarray, ws: np.ndarray) -> None:
-    n = x.size
-    t, m = n, 1
-    while m < n:
-        t >>= 1
-        for i in range(m):
-            j1 = 2 * i * t
-            v = x[j1 + t:j1 + 2 * t] * ws[m + i]
-            x[j1 + t:j1 + 2 * t] = x[j1:j1 + t] - v
-            x[j1:j1 + t] += v
-        m <<= 1
-
-
-def _gs_rn(x: np.ndarray, ws: np.ndarray) -> None:
-    n = x.size
-    t, m = 1, n
-    while m > 1:
-        h = m >> 1
-        blk = x.reshape(h, 2 * t)
-        u = blk[:, :t].copy()
-        v = blk[:, t:].copy()
-        blk[:, :t] = u + v
-        blk[:, t:] = (u - v) * ws[h:2 * h, None]
-        t <<= 1
-        m >>= 1
-
-
-def ckks_encode_coeffs(values, n_slots: int, delta: float) -> np.ndarray:
-    """Slots -> rounded integer coefficients (ckks.py:37-56 with complex.py IFFT)."""
-    z = np.zeros(n_slots, dtype=np.complex128)
-    z[: len(values)] = np.asarray(values, dtype=np.complex128)
-    _, inv = special_roots(2 * n_slots)
-    z = z[np.argsort(_brv_perm(n_slots))]
-    _gs_rn(z, inv)
-    z = z * (1.0 / n_slots) * delta
-    return np.concatenate([np.rint(z.real), np.rint(z.imag)]).astype(np.int64)
-
-
-def ckks_decode_coeffs(coeffs: np.ndarray, delta: float) -> np.ndarray:
-    """Signed coefficients -> slots (ckks.py:58-98 with complex.py FFT)."""
-    n = coeffs.size // 2
-    z = np.asarray(coeffs[:n], dtype=np.float64) + 1j * np.asarray(coeffs[n:], dtype=np.float64)
-    fwd, _ = special_roots(2 * n)
-    _ct_nr(z, fwd)
-    z = z[_brv_perm(n)]
-    return z / delta
 
 
 class CKKS_Scheme(MLWE_Scheme):
@@ -108,15 +24,34 @@ class CKKS_Scheme(MLWE_Scheme):
                  special_rings=None):
         super().__init__(rings, special_primes=special_primes, special_rings=special_rings, module_rank=module_rank)
         self.scaling_factor = scaling_factor
+        self.complex_ring = ComplexRing(self.ring.N // 2, True, engine=self.ring.engine)
 
     def encode(self, values) -> Polynomial:
-        assert len(values) == self.ring.N // 2
-        coeffs = ckks_encode_coeffs(values, self.ring.N // 2, self.scaling_factor)
-        poly = Polynomial(self.ring).from_array(coeffs.tolist())
+        """Slots -> plaintext (ckks.py:37-56): IFFT, scale, round, NTT."""
+        assert len(values) == self.ring.N // 2, f"Expected {self.ring.N // 2} values, got {len(values)}"
+        c_poly = ComplexPolynomial(self.complex_ring)
+        c_poly.from_array(values)
+        c_poly.IFFT()
+        c_poly *= self.scaling_factor
+        poly = c_poly.round_to_RNS_cpp(self.ring)
         poly.rns_mask = self.ring.mask
         return poly
 
+    def encode_batch(self, values_list) -> list[Polynomial]:
+        """Many encodings in one engine call (complex_polys_ifft_scale_round_to_RNS_batch)."""
+        polys = []
+        for values in values_list:
+            c = ComplexPolynomial(self.complex_ring)
+            c.from_array(values)
+            polys.append(c)
+        out = self.complex_ring.exp_complex_polys_ifft_scale_round_to_RNS_batch(polys, self.ring,
+                                                                                self.scaling_factor)
+        for p in out:
+            p.rns_mask = self.ring.mask
+        return out
+
     def decode(self, poly: Polynomial, scaling_factor: float | None = None) -> list[complex]:
+        """Plaintext -> slots (ckks.py:58-98): exact CRT, signed lift, FFT, 1/delta."""
         delta = self.scaling_factor if scaling_factor is None else scaling_factor
         mask = poly.rns_mask
         rns = poly.coeff_array()
@@ -124,11 +59,16 @@ class CKKS_Scheme(MLWE_Scheme):
                   if (mask >> idx) & 1]
         primes = [p for p, _ in active]
         q = math.prod(primes)
-        vals = np.empty(poly.ring.N, dtype=np.float64)
+        c_poly = ComplexPolynomial(self.complex_ring)
+        half = poly.ring.N // 2
+        coeffs = []
         for j in range(poly.ring.N):
             v = crt([int(r[j]) for _, r in active], primes)
-            vals[j] = float(v - q if v >= q // 2 else v)
-        return list(ckks_decode_coeffs(vals, delta))
+            coeffs.append(float(v - q if v >= q // 2 else v))
+        for i in range(half):
+            c_poly[i] = complex(coeffs[i], coeffs[i + half])
+        c_poly.FFT()
+        return [v / delta for v in c_poly]
 
     def encrypt(self, message: Polynomial, key: MLWE_Key, rng=None) -> CKKS_Ciphertext:
         out = CKKS_Ciphertext(self)

@@ -48,6 +48,9 @@ def _cdef_text() -> str:
         if s.startswith("#"):
             continue
         out.append(line)
+    # misc.cdef:17 binds libc free() to release safe_aligned_malloc buffers; it is not
+    # part of the engine library (the symbol resolves through its libc dependency)
+    out.append("void free(void *ptr);")
     return "\n".join(out)
 
 
