@@ -175,7 +175,7 @@ def cpu_baseline(time_budget: float = 15.0) -> dict:
     if not lib.exists():
         return {"value": None, "unit": "pairs/s", "cores": 1, "kind": "reference",
                 "sample": "unavailable: oracle/_ref not built"}
-    r = _ref_worker((1, 1, 50, SEED + 7, time_budget))
+    r = _ref_worker((1, 1, 100000, SEED + 7, time_budget))
     return {"value": r["pairs"] / r["elapsed"], "unit": "pairs/s", "cores": 1, "kind": "reference",
             "sample": f"{r['pairs']} pairs of the same workload on the reference's {name} engine, "
                       f"one thread, {r['elapsed']:.1f} s"}
@@ -207,6 +207,24 @@ def run_reference_arm(args) -> None:
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------- profiling
+PROFILE_LEG = "ckks"
+
+
+def profile_range(args, leg: str, start: bool) -> None:
+    """Open/close the profiler's capture range (ncu --profile-from-start off) around the
+    timed region of the leg chosen with --profile-leg."""
+    if PROFILE_LEG != leg:
+        return
+    import torch
+
+    torch.cuda.synchronize()
+    if start:
+        torch.cuda.profiler.start()
+    else:
+        torch.cuda.profiler.stop()
 
 
 # ----------------------------------------------------------------------------- ranks
@@ -242,11 +260,13 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
     wl.run(stream)  # compile + capture + first replay
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    profile_range(None, "worklist", True)
     ev0.record(stream)
     for _ in range(reps):
         wl.run(stream)
     ev1.record(stream)
     torch.cuda.synchronize()
+    profile_range(None, "worklist", False)
     ms_wl = ev0.elapsed_time(ev1) / reps
     outs = [torch.empty_like(j.out) for j in jobs]
     ws = per_call_workspace(eng, jobs)
@@ -294,6 +314,7 @@ def cggi_fft_leg(eng, count: int, reps: int, million: bool = False) -> dict:
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    profile_range(None, "cggi_fft", True)
     ev[0].record(stream)
     for _ in range(reps):
         ext = dev.blind_rotate(lwe, tv)
@@ -302,6 +323,7 @@ def cggi_fft_leg(eng, count: int, reps: int, million: bool = False) -> dict:
         out = dev.keyswitch(ext)
     ev[2].record(stream)
     torch.cuda.synchronize()
+    profile_range(None, "cggi_fft", False)
     br_ms = ev[0].elapsed_time(ev[1]) / reps
     ks_ms = ev[1].elapsed_time(ev[2]) / reps
     res_host, ext_host = to_host(out), to_host(ext)
@@ -335,6 +357,84 @@ def cggi_fft_leg(eng, count: int, reps: int, million: bool = False) -> dict:
                           "mismatches": bad, "phase_error_max": worst}
     del dev
     torch.cuda.empty_cache()
+    return res
+
+
+def _rns_cggi_setup(engine, n_lwe: int, count: int, seed: int):
+    """The reference's CGGI16 (RNS gadget) at N = 1024, [50, 50, 50] (one special), a
+    binary LWE key of dimension n_lwe, 5-bit LUT precision: keys and LWEs (seeded)."""
+    from vfhe_b200.arith import Ring
+    from vfhe_b200.fhe import CGGI16
+    from vfhe_b200.mlwe import LWE_Key, MLWE_Scheme, encrypt_lwe
+    from vfhe_b200.native import use_engine
+
+    with use_engine(engine):
+        rng = np.random.default_rng(seed)
+        Rq = Ring(1024, prime_size=[50, 50, 50], split_degree=1)
+        in_ring = Rq.quotient_ring(ell=2)
+        s = MLWE_Scheme(Rq, special_primes=1, module_rank=1, max_lvl=1)
+        key_s = [int(v) for v in rng.integers(0, 2, n_lwe)]
+        out_key = s.key_gen_sparse(64, 3.2, ternary=False, rng=rng)
+        cg = CGGI16(s)
+        bk = cg.generate_bootstrap_key(LWE_Key(ring=in_ring, key=key_s, n=n_lwe), out_key, rng=rng)
+        t = 16
+        lut = [int(v) for v in rng.integers(0, t, t)]
+        tv = cg.LUT_packing(lut, t, 5)
+        msgs = [int(v) for v in rng.integers(0, t, count)]
+        lwes = [encrypt_lwe(in_ring, key_s, [round(m * in_ring.q_l / 32) % q for q in in_ring.primes], 3.2, rng)
+                for m in msgs]
+        ok = out_key.extract_lwe_key()
+        key2 = LWE_Key(ring=in_ring, key=ok.get_s(), n=ok.n)
+        return s, cg, bk, tv, lwes, msgs, lut, in_ring, key2
+
+
+def rns_cggi_leg(eng, count: int = 1024, cpu_bootstraps: int = 2) -> dict:
+    """Batched RNS CGGI16 (the reference's scheme) at n = 630, N = 1024 on the GPU, and
+    the reference library's own functional_bootstrap on one host core."""
+    import torch
+
+    from vfhe_b200.batch import CggiBatch, bootstrap_key_tensor, to_device, to_host
+    from vfhe_b200.mlwe import LWE
+
+    s, cg, bk, tv, lwes, msgs, lut, in_ring, key2 = _rns_cggi_setup(eng, 630, count, SEED + 11)
+    a = to_device(np.stack([np.array(x.get_a(), dtype=np.uint64) for x in lwes]))
+    b = to_device(np.stack([np.array(x.get_b(), dtype=np.uint64) for x in lwes]))
+    tv.to_coeff()
+    tvt = to_device(np.stack([tv.component_rows(0), tv.component_rows(1)]))
+    bkt = bootstrap_key_tensor(bk)
+    runner = CggiBatch(s, eng)
+    oa, ob = runner.bootstrap(a, b, bkt, tvt, 16)  # captures the blind-rotation graph
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    profile_range(None, "cggi_rns", True)
+    e0.record(stream)
+    oa, ob = runner.bootstrap(a, b, bkt, tvt, 16)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    profile_range(None, "cggi_rns", False)
+    ms = e0.elapsed_time(e1)
+    ha, hb = to_host(oa), to_host(ob)
+    bad = 0
+    for i in range(min(count, 64)):
+        o = LWE(ring=in_ring, n=1024)
+        o.set_rows(ha[i], hb[i])
+        ph = o.phase(key2, recompose=True)
+        bad += int(round(ph * 32 / in_ring.q_l) % 32 != lut[msgs[i]])
+    res = {"workload": f"{count} LWEs, n=630, N=1024, RNS gadget over 2 x 50-bit primes + 1 special, 16-entry LUT",
+           "gpu_bootstraps_per_s": count / (ms * 1e-3), "gpu_ms": ms, "checked": min(count, 64),
+           "mismatches": bad}
+    lib, name = _ref_library()
+    if lib.exists() and cpu_bootstraps > 0:
+        from vfhe_b200.native import Engine
+
+        ref = Engine(lib)
+        rs, rcg, rbk, rtv, rlwes, _, _, rin, _ = _rns_cggi_setup(ref, 630, cpu_bootstraps, SEED + 12)
+        t0 = time.perf_counter()
+        for x in rlwes:
+            rcg.functional_bootstrap(LWE(ring=rin), rtv, x, rbk, torus_base=16)
+        res["cpu_reference_ms_per_bootstrap"] = 1e3 * (time.perf_counter() - t0) / cpu_bootstraps
+        res["cpu_reference"] = f"reference's {name} engine, one core, {cpu_bootstraps} bootstraps"
     return res
 
 
@@ -453,13 +553,13 @@ def run_cuda_arm(args) -> None:
     with ClockSampler(local) as clocks:
         barrier()
         # the timed region is also the profiler's capture range (ncu --profile-from-start off)
-        torch.cuda.profiler.start()
+        profile_range(args, "ckks", True)
         ev0.record(stream)
         for _ in range(args.steps):
             step()
         ev1.record(stream)
         barrier()
-        torch.cuda.profiler.stop()
+        profile_range(args, "ckks", False)
     launches = eng.lib.vfhe_cuda_launch_count() - launches0
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, "cuda")
     value = whole_job_rate(PAIRS, world, ms)
@@ -536,6 +636,7 @@ def run_cuda_arm(args) -> None:
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
     serving = None if args.no_serving else serving_leg(eng, args.serving_requests)
     cggi_fft = None if args.no_cggi else cggi_fft_leg(eng, 4096, reps=3, million=args.cggi_million)
+    rns_cggi = None if args.no_cggi else rns_cggi_leg(eng)
 
     if rank != 0:
         if dist is not None:
@@ -590,6 +691,8 @@ def run_cuda_arm(args) -> None:
         line["serving"] = serving
     if cggi_fft is not None:
         line["cggi_fft_bootstrap"] = cggi_fft
+    if rns_cggi is not None:
+        line["cggi16_rns_bootstrap"] = rns_cggi
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
@@ -614,7 +717,11 @@ def main() -> None:
     ap.add_argument("--cggi-million", action="store_true",
                     help="also bootstrap 10^6 LWEs and count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
+    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "cggi_fft", "cggi_rns", "worklist"],
+                    help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()
+    global PROFILE_LEG
+    PROFILE_LEG = args.profile_leg
     sys.path.insert(0, str(ROOT))
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:

@@ -120,6 +120,14 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
         return;
     }
     const long long P = N / S;
+    if (pi.fp64 && (S == 2 || S == 4)) {
+        for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < P;
+             x += (long long)gridDim.x * blockDim.x) {
+            if (S == 2) mac_slots<2>(oa, ob, d, dstride, ka, kb, kstride, nd, P, x, pi);
+            else mac_slots<4>(oa, ob, d, dstride, ka, kb, kstride, nd, P, x, pi);
+        }
+        return;
+    }
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
          idx += (long long)gridDim.x * blockDim.x) {
         const int o = (int)(idx / P);

@@ -72,6 +72,69 @@ __device__ __forceinline__ void mac_slot(uint64_t* oa, uint64_t* ob, const uint6
     ob[(long long)o * P + x] = f_to_canonical(-sb, q, qinv, pi.q);
 }
 
+// mac_slot for all S output blocks of slot x at once (S = 2 or 4): every digit's S
+// blocks of D and of both key components are loaded once (3 S loads per digit for S
+// outputs, the traffic of a pointwise product).  Same exact FP64 arithmetic and result.
+template <int S>
+__device__ __forceinline__ void mac_slots(uint64_t* oa, uint64_t* ob, const uint64_t* d, long long dstr,
+                                          const uint64_t* ka, const uint64_t* kb, long long kstr, int nd, long long P,
+                                          long long x, const PrimeInfo& pi) {
+    const double q = pi.qd, qinv = pi.qinv;
+    double sa[S], sb[S], wa[S], wb[S];
+#pragma unroll
+    for (int o = 0; o < S; ++o) sa[o] = sb[o] = wa[o] = wb[o] = 0.0;
+    int terms = 0;
+    for (int j = 0; j < nd; ++j) {
+        double v[S], ya[S], yqa[S], yb[S], yqb[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            v[i] = f_from_u64(d[j * dstr + (long long)i * P + x]);
+            ya[i] = f_from_u64(ka[j * kstr + (long long)i * P + x]);
+            yb[i] = f_from_u64(kb[j * kstr + (long long)i * P + x]);
+            yqa[i] = __dmul_rn(ya[i], qinv);
+            yqb[i] = __dmul_rn(yb[i], qinv);
+        }
+#pragma unroll
+        for (int o = 0; o < S; ++o)
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const int k = o - i;
+                const int kk = k < 0 ? k + S : k;
+                const double ta = f_mulmod(v[i], ya[kk], yqa[kk], q);
+                const double tb = f_mulmod(v[i], yb[kk], yqb[kk], q);
+                if (k < 0) {
+                    wa[o] = __dadd_rn(wa[o], ta);
+                    wb[o] = __dadd_rn(wb[o], tb);
+                } else {
+                    sa[o] = __dadd_rn(sa[o], ta);
+                    sb[o] = __dadd_rn(sb[o], tb);
+                }
+            }
+        // each accumulator gains at most S terms of <= 9q/16 per digit; with q < 2^50
+        // six terms on top of a reduced value stay below 2^52 (S <= 4 here)
+        terms += S;
+        if (terms + S > 6 || j == nd - 1) {
+#pragma unroll
+            for (int o = 0; o < S; ++o) {
+                sa[o] = f_reduce(sa[o], q, qinv);
+                sb[o] = f_reduce(sb[o], q, qinv);
+                wa[o] = f_reduce(wa[o], q, qinv);
+                wb[o] = f_reduce(wb[o], q, qinv);
+            }
+            terms = 0;
+        }
+    }
+    const double w = f_from_u64(reinterpret_cast<const ulonglong2*>(pi.twist)[x].x);
+    const double wq = __dmul_rn(w, qinv);
+#pragma unroll
+    for (int o = 0; o < S; ++o) {
+        const double ra = __dadd_rn(sa[o], f_mulmod(wa[o], w, wq, q));
+        const double rb = __dadd_rn(sb[o], f_mulmod(wb[o], w, wq, q));
+        oa[(long long)o * P + x] = f_to_canonical(-ra, q, qinv, pi.q);
+        ob[(long long)o * P + x] = f_to_canonical(-rb, q, qinv, pi.q);
+    }
+}
+
 // mac_slot for primes of any size (64-bit Barrett products, canonical sums).
 __device__ __forceinline__ void mac_slot_int(uint64_t* oa, uint64_t* ob, const uint64_t* d, long long dstr,
                                              const uint64_t* ka, const uint64_t* kb, long long kstr, int nd, int S,

@@ -98,18 +98,25 @@ __global__ void __launch_bounds__(kWlThreads) k_wl_product(const ProdDesc* __res
     for (int o = 0; o < S; ++o) d.out[o * P + x] = res[o];
 }
 
-// -sum_j D_j (*) K_j for one (job, extended limb): mac_slot over N = S blocks x P slots
+// -sum_j D_j (*) K_j for one (job, extended limb).  S <= 4: one thread per slot x
+// computes all S blocks (mac_slots); larger S: one thread per (block, slot).
+template <int S>
 __global__ void __launch_bounds__(kWlThreads) k_wl_mac(const MacDesc* __restrict__ tab, long long chunks,
-                                                       long long N, int S) {
+                                                       long long N) {
     const long long e = blockIdx.x / chunks;
     const long long chunk = blockIdx.x - e * chunks;
     const MacDesc d = tab[e];
     const long long idx = chunk * kWlThreads + threadIdx.x;
-    if (idx >= N) return;
     const long long P = N / S;
+    const long long dstr = (long long)d.ne * N;
+    if (S == 2 || S == 4) {
+        if (idx >= P) return;
+        mac_slots<(S == 2 ? 2 : 4)>(d.oa, d.oa + dstr, d.d, dstr, d.k, d.k + dstr, 2 * dstr, d.nd, P, idx, *d.pi);
+        return;
+    }
+    if (idx >= N) return;
     const int o = (int)(idx / P);
     const long long x = idx - o * P;
-    const long long dstr = (long long)d.ne * N;
     mac_slot(d.oa, d.oa + dstr, d.d, dstr, d.k, d.k + dstr, 2 * dstr, d.nd, S, P, x, o, *d.pi);
 }
 
@@ -375,8 +382,16 @@ int compile(WorkList& w) {
                 note_launch();
             }
             if (!cerr && !Gr.mac.empty()) {
-                const long long chunks = (N + kWlThreads - 1) / kWlThreads;
-                k_wl_mac<<<(unsigned)(chunks * (long long)Gr.mac.size()), kWlThreads, 0, q>>>(Gr.d_mac, chunks, N, s);
+                const long long work = (s == 2 || s == 4) ? N / s : N;  // threads per entry
+                const long long chunks = (work + kWlThreads - 1) / kWlThreads;
+                const unsigned grid = (unsigned)(chunks * (long long)Gr.mac.size());
+                switch (s) {
+                    case 1: k_wl_mac<1><<<grid, kWlThreads, 0, q>>>(Gr.d_mac, chunks, N); break;
+                    case 2: k_wl_mac<2><<<grid, kWlThreads, 0, q>>>(Gr.d_mac, chunks, N); break;
+                    case 4: k_wl_mac<4><<<grid, kWlThreads, 0, q>>>(Gr.d_mac, chunks, N); break;
+                    case 8: k_wl_mac<8><<<grid, kWlThreads, 0, q>>>(Gr.d_mac, chunks, N); break;
+                    default: k_wl_mac<16><<<grid, kWlThreads, 0, q>>>(Gr.d_mac, chunks, N); break;
+                }
                 cerr = (int)cudaGetLastError();
                 note_launch();
             }
