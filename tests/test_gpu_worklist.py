@@ -95,3 +95,49 @@ def test_schedules_do_not_change_results(cuda):
     # shapes outside the supported set are refused
     assert lib.vfhe_cuda_ntt_set_schedule(14, 3, 7, 0, 0) != 0
     lib.vfhe_cuda_clear_error()
+    assert lib.vfhe_cuda_device_faults() == 0  # no bounded tile-copy wait gave up
+
+
+def test_persistent_double_buffered_schedules(cuda):
+    """Grids smaller than the tile count take the persistent path (bulk asynchronous
+    tile loads into two shared buffers); results must equal the one-CTA-per-tile path."""
+    import torch
+
+    from vfhe_b200.arith import Ring
+    from vfhe_b200.batch import to_device, to_host
+
+    ffi, lib = cuda.ffi, cuda.lib
+    rng = np.random.default_rng(8)
+    st = ffi.cast("void*", torch.cuda.current_stream().cuda_stream)
+    for N, split, B, scheds in [(2**12, 1, 512, [(12, 0, 1), (12, 0, 2), (11, 2, 1)]),
+                                (2**10, 1, 1024, [(10, 4, 1), (10, 2, 2)]),
+                                (2**14, 1, 96, [(12, 0, 1), (11, 2, 2), (13, 0, 1)]),
+                                (2**16, 4, 24, [(12, 0, 2)])]:
+        R = Ring(N, prime_size=[50] * 3, split_degree=split, engine=cuda)
+        logP = (N // split).bit_length() - 1
+        rows = np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in R.primes]) for _ in range(B)])
+        limbs = ffi.new("uint32_t[]", R.prime_indices)
+        nrows = B * 3 * split
+        bucket = nrows.bit_length() - 1
+
+        def fwd_inv():
+            x = to_device(rows)
+            p = ffi.cast("uint64_t*", x.data_ptr())
+            assert lib.vfhe_cuda_ntt_batch(R.NTT, 0, p, p, B, limbs, 3, st) == 0
+            f = x.clone()
+            assert lib.vfhe_cuda_ntt_batch(R.NTT, 1, p, p, B, limbs, 3, st) == 0
+            torch.cuda.synchronize()
+            return f, x
+
+        saved = ffi.new("int32_t[3]")
+        lib.vfhe_cuda_ntt_get_schedule(logP, nrows, saved)
+        assert lib.vfhe_cuda_ntt_set_schedule(logP, bucket, 0, 0, 0) == 0
+        base_f, base_i = fwd_inv()
+        assert np.array_equal(to_host(base_i), rows)
+        for tb, tpc, cps in scheds:
+            assert lib.vfhe_cuda_ntt_set_schedule(logP, bucket, tb, tpc, cps) == 0
+            f, i = fwd_inv()
+            assert torch.equal(f, base_f), (N, split, tb, tpc, cps)
+            assert torch.equal(i, base_i), (N, split, tb, tpc, cps)
+        assert lib.vfhe_cuda_ntt_set_schedule(logP, bucket, *saved) == 0
+    assert lib.vfhe_cuda_device_faults() == 0

@@ -197,6 +197,13 @@ int vfhe_cuda_keyswitch_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct, 
     return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, nullptr, keys.data(), ws, st);
 }
 
+int vfhe_cuda_device_faults(void) {
+    if (!vc::ensure_ready()) return -1;
+    int f = 0;
+    if (!check_cuda(read_tile_fault(&f), "vfhe_cuda_device_faults")) return -1;
+    return f;
+}
+
 int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_bits, int32_t tiles_per_cta,
                                int32_t ctas_per_sm) {
     const NttSchedule s = {tile_bits, tiles_per_cta, ctas_per_sm};

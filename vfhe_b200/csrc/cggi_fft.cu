@@ -83,41 +83,6 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
     return make_double2(__fma_rn(a.x, b.x, a.y * b.y), __fma_rn(a.y, b.x, -a.x * b.y));
 }
 
-// In-place forward DIF FFT (kernel e^{+2 pi i/M}) of `count` arrays of M points at
-// x + a * stride; THREADS threads, one butterfly per thread per array per stage.
-template <int M, int THREADS>
-__device__ __forceinline__ void fft_fwd(double2* x, int count, int stride, const double2* tw) {
-    for (int h = M / 2; h >= 1; h >>= 1) {
-        for (int bf = threadIdx.x; bf < M / 2 * count; bf += THREADS) {
-            const int a = bf / (M / 2), r = bf - a * (M / 2);
-            const int grp = r / h, j = r - grp * h;
-            const int i0 = grp * 2 * h + j;
-            double2* y = x + a * stride;
-            const double2 u = y[i0], v = y[i0 + h];
-            y[i0] = make_double2(u.x + v.x, u.y + v.y);
-            y[i0 + h] = cmul(make_double2(u.x - v.x, u.y - v.y), tw[j * (M / (2 * h))]);
-        }
-        __syncthreads();
-    }
-}
-
-// In-place inverse DIT FFT (kernel e^{-2 pi i/M}, no 1/M) of `count` arrays.
-template <int M, int THREADS>
-__device__ __forceinline__ void fft_inv(double2* x, int count, int stride, const double2* tw) {
-    for (int h = 1; h <= M / 2; h <<= 1) {
-        for (int bf = threadIdx.x; bf < M / 2 * count; bf += THREADS) {
-            const int a = bf / (M / 2), r = bf - a * (M / 2);
-            const int grp = r / h, j = r - grp * h;
-            const int i0 = grp * 2 * h + j;
-            double2* y = x + a * stride;
-            const double2 u = y[i0], v = cmulc(y[i0 + h], tw[j * (M / (2 * h))]);
-            y[i0] = make_double2(u.x + v.x, u.y + v.y);
-            y[i0 + h] = make_double2(u.x - v.x, u.y - v.y);
-        }
-        __syncthreads();
-    }
-}
-
 // signed digits of v rounded to its top base_log * levels bits (digit 0 most significant)
 __device__ __forceinline__ void decompose(int (&d)[kMaxLevels], uint32_t v, int base_log, int levels) {
     const int total = base_log * levels;
@@ -137,6 +102,25 @@ __device__ __forceinline__ void decompose(int (&d)[kMaxLevels], uint32_t v, int 
     }
 }
 
+// digit `want` of the same signed decomposition, without materialising the others
+__device__ __forceinline__ int digit_of(uint32_t v, int base_log, int levels, int want) {
+    const int total = base_log * levels;
+    uint64_t r = ((uint64_t)v + (1ULL << (31 - total))) >> (32 - total);
+    r &= total >= 32 ? 0xFFFFFFFFULL : ((1ULL << total) - 1);
+    const int half = 1 << (base_log - 1), full = 1 << base_log;
+    int out = 0;
+    for (int l = levels - 1; l >= 0; --l) {
+        int x = (int)(r & (uint64_t)(full - 1));
+        r >>= base_log;
+        if (x >= half) {
+            x -= full;
+            r += 1;
+        }
+        if (l == want) out = x;
+    }
+    return out;
+}
+
 __device__ __forceinline__ int modswitch(uint32_t v, int logN2) {
     return (int)((((uint64_t)v + (1ULL << (31 - logN2))) >> (32 - logN2)) & ((1ULL << logN2) - 1));
 }
@@ -149,181 +133,330 @@ __device__ __forceinline__ uint32_t rot_at(const uint32_t* p, int k, int e) {
     return s < N ? p[s] : (uint32_t)(0u - p[s - N]);
 }
 
+// ---- register-blocked radix-8 FFT passes
+//
+// An M-point transform (M = 2^LOGM) of one array is done by M/8 threads holding 8
+// values each.  Pass p covers index bits [LO, LO + NST): thread t holds the elements
+// pidx<LO>(t, k), k < 8 (k supplies bits LO..LO+2), so all butterflies of the pass are
+// in registers; passes exchange through shared memory with an XOR swizzle that keeps
+// every pass's accesses free of bank conflicts.  Forward: LOGM/3 full passes from the
+// top bits, then one partial pass (LOGM mod 3 stages) at bit 0; the inverse runs the
+// same passes in reverse.  The final forward pass leaves element f = 8t + k in thread
+// t, which is also the order of the key spectra in memory (position k * M/8 + t), so
+// the multiply-accumulate reads both coalesced.
+
+template <int LO>
+__device__ __forceinline__ int pidx(int t, int k) {
+    return ((t >> LO) << (LO + 3)) | (k << LO) | (t & ((1 << LO) - 1));
+}
+
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 7); }
+
+template <int LOGM, int P>
+struct PassOf {
+    static constexpr int FULL = LOGM / 3;
+    static constexpr int LO = P < FULL ? LOGM - 3 * (P + 1) : 0;
+    static constexpr int NST = P < FULL ? 3 : LOGM % 3;
+};
+
+template <int LOGM>
+struct Passes {
+    static constexpr int count = (LOGM + 2) / 3;
+};
+
+// decimation-in-frequency stages of one pass (kernel e^{+2 pi i / M})
+template <int LOGM, int LO, int NST>
+__device__ __forceinline__ void dif(double2 (&v)[8], int t, const double2* __restrict__ tw) {
+#pragma unroll
+    for (int s = NST - 1; s >= 0; --s) {
+        const int bit = 1 << s;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k & bit) continue;
+            const int j = pidx<LO>(t, k) & ((1 << (LO + s)) - 1);
+            const double2 w = __ldg(&tw[j << (LOGM - 1 - LO - s)]);
+            const double2 u = v[k], x = v[k | bit];
+            v[k] = make_double2(u.x + x.x, u.y + x.y);
+            v[k | bit] = cmul(make_double2(u.x - x.x, u.y - x.y), w);
+        }
+    }
+}
+
+// decimation-in-time stages of one pass (kernel e^{-2 pi i / M})
+template <int LOGM, int LO, int NST>
+__device__ __forceinline__ void dit(double2 (&v)[8], int t, const double2* __restrict__ tw) {
+#pragma unroll
+    for (int s = 0; s < NST; ++s) {
+        const int bit = 1 << s;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k & bit) continue;
+            const int j = pidx<LO>(t, k) & ((1 << (LO + s)) - 1);
+            const double2 w = __ldg(&tw[j << (LOGM - 1 - LO - s)]);
+            const double2 u = v[k], x = cmulc(v[k | bit], w);
+            v[k] = make_double2(u.x + x.x, u.y + x.y);
+            v[k | bit] = make_double2(u.x - x.x, u.y - x.y);
+        }
+    }
+}
+
+template <int LO>
+__device__ __forceinline__ void put8(double2* a, const double2 (&v)[8], int t) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[swz(pidx<LO>(t, k))] = v[k];
+}
+
+template <int LO>
+__device__ __forceinline__ void get8(double2 (&v)[8], const double2* a, int t) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = a[swz(pidx<LO>(t, k))];
+}
+
+// forward passes P .. count-1 of array a (pass P-1 left its values at a); barriers are
+// taken by every thread of the block (active == false threads skip the work only)
+template <int LOGM, int P>
+__device__ __forceinline__ void fwd_rest(double2* a, int t, bool active, const double2* tw) {
+    if constexpr (P < Passes<LOGM>::count) {
+        using Q = PassOf<LOGM, P>;
+        double2 v[8];
+        if (active) {
+            get8<Q::LO>(v, a, t);
+            dif<LOGM, Q::LO, Q::NST>(v, t, tw);
+        }
+        __syncthreads();  // all reads of the previous layout done
+        if (active) put8<Q::LO>(a, v, t);
+        __syncthreads();
+        fwd_rest<LOGM, P + 1>(a, t, active, tw);
+    }
+}
+
+// inverse passes P down to 1 (pass P+1 left its values at a); pass 0 is done by the caller
+template <int LOGM, int P>
+__device__ __forceinline__ void inv_rest(double2* a, int t, bool active, const double2* tw) {
+    if constexpr (P >= 1) {
+        using Q = PassOf<LOGM, P>;
+        double2 v[8];
+        if (active) {
+            get8<Q::LO>(v, a, t);
+            dit<LOGM, Q::LO, Q::NST>(v, t, tw);
+        }
+        __syncthreads();
+        if (active) put8<Q::LO>(a, v, t);
+        __syncthreads();
+        inv_rest<LOGM, P - 1>(a, t, active, tw);
+    }
+}
+
 template <int N>
 struct Smem {
     static constexpr int M = N / 2;
-    // acc[2][N] uint32 | spec[2 L][M] double2 | outs[2][M] double2 | tw[M/2] | twist[M]
+    // acc[2][N] uint32 | spec[2 L][M] double2 | outs[2][M] double2
     static constexpr size_t bytes(int levels) {
-        return sizeof(uint32_t) * 2 * N + sizeof(double2) * (2 * levels * M + 2 * M + M / 2 + M);
+        return sizeof(uint32_t) * 2 * N + sizeof(double2) * (2 * levels * M + 2 * M);
     }
 };
 
+// One external product on the block's GLWE: digits of the source (MODE 0: acc X^ai -
+// acc, from shared acc; MODE 1: the GLWE `src` in global memory), forward transforms,
+// multiply-accumulate with the GGSW spectra `key` (key order), inverse transforms;
+// MODE 0 adds the rounded result into acc, MODE 1 writes it to `dst` and the largest
+// distance of an unrounded coefficient to its integer to *frac.
+template <int LOGM, int LEVELS, int MODE>
+__device__ __forceinline__ void ext_product(uint32_t* acc, double2* spec, double2* outs, const double2* __restrict__ key,
+                                            int ai, int base_log, const uint32_t* __restrict__ src,
+                                            uint32_t* __restrict__ dst, double* frac, const double2* __restrict__ tw,
+                                            const double2* __restrict__ twist) {
+    constexpr int M = 1 << LOGM, N = 2 * M, TPA = M / 8, R = 2 * LEVELS;
+    constexpr int NP = Passes<LOGM>::count;
+    const int arr = threadIdx.x / TPA, t = threadIdx.x - arr * TPA;
+    // forward pass 0 straight from the digits (element j = t + k M/8)
+    {
+        using Q = PassOf<LOGM, 0>;
+        const int c = arr / LEVELS, l = arr - c * LEVELS;
+        double2* a = spec + arr * M;
+        // the folded, twisted digits go to this thread's own pass-0 slots first (one at a
+        // time, to keep register pressure low), then come back as the pass's registers
+#pragma unroll 1
+        for (int k = 0; k < 8; ++k) {
+            const int j = pidx<Q::LO>(t, k);
+            uint32_t lo, hi;
+            if (MODE == 0) {
+                const uint32_t* pc = acc + c * N;
+                lo = rot_at<N>(pc, j, ai) - pc[j];
+                hi = rot_at<N>(pc, j + M, ai) - pc[j + M];
+            } else {
+                lo = src[c * N + j];
+                hi = src[c * N + j + M];
+            }
+            a[swz(j)] = cmul(make_double2((double)digit_of(lo, base_log, LEVELS, l),
+                                          (double)digit_of(hi, base_log, LEVELS, l)),
+                             __ldg(&twist[j]));
+        }
+        double2 v[8];
+        get8<Q::LO>(v, a, t);
+        dif<LOGM, Q::LO, Q::NST>(v, t, tw);
+        put8<Q::LO>(a, v, t);
+    }
+    __syncthreads();
+    fwd_rest<LOGM, 1>(spec + arr * M, t, true, tw);
+    // multiply-accumulate fused into inverse pass NP-1 (threads of the two outputs)
+    const bool inv = threadIdx.x < 2 * TPA;
+    const int oc = inv ? arr : 0;
+    {
+        using Q = PassOf<LOGM, NP - 1>;
+        if (inv) {
+            double2* o = outs + oc * M;
+            // products go to this thread's own slots first (one element at a time)
+#pragma unroll 1
+            for (int k = 0; k < 8; ++k) {
+                const int f = pidx<Q::LO>(t, k);
+                double2 acc2 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const double2 kv = __ldg(&key[(r * 2 + oc) * M + k * TPA + t]);
+                    const double2 dv = spec[r * M + swz(f)];
+                    acc2.x = __fma_rn(dv.x, kv.x, __fma_rn(-dv.y, kv.y, acc2.x));
+                    acc2.y = __fma_rn(dv.x, kv.y, __fma_rn(dv.y, kv.x, acc2.y));
+                }
+                o[swz(f)] = acc2;
+            }
+            double2 v[8];
+            get8<Q::LO>(v, o, t);
+            dit<LOGM, Q::LO, Q::NST>(v, t, tw);
+            put8<Q::LO>(o, v, t);
+        }
+        __syncthreads();
+    }
+    inv_rest<LOGM, NP - 2>(outs + oc * M, t, inv, tw);
+    // inverse pass 0: untwist, unfold, round (element j = t + k M/8)
+    {
+        using Q = PassOf<LOGM, 0>;
+        double worst = 0.0;
+        if (inv) {
+            double2 v[8];
+            get8<Q::LO>(v, outs + oc * M, t);
+            dit<LOGM, Q::LO, Q::NST>(v, t, tw);
+            const double inv_m = 1.0 / (double)M;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = pidx<Q::LO>(t, k);
+                const double2 z = cmulc(v[k], __ldg(&twist[j]));
+                const double re = z.x * inv_m, im = z.y * inv_m;
+                const long long lo = __double2ll_rn(re), hi = __double2ll_rn(im);
+                if (MODE == 0) {
+                    acc[oc * N + j] += (uint32_t)lo;
+                    acc[oc * N + j + M] += (uint32_t)hi;
+                } else {
+                    dst[oc * N + j] = (uint32_t)lo;
+                    dst[oc * N + j + M] = (uint32_t)hi;
+                    worst = fmax(worst, fmax(fabs(re - (double)lo), fabs(im - (double)hi)));
+                }
+            }
+        }
+        if (MODE == 1) {
+            // block maximum through the spectra buffer (no longer needed)
+            double* red = reinterpret_cast<double*>(spec);
+            __syncthreads();
+            red[threadIdx.x] = worst;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double m = 0.0;
+                for (int i = 0; i < (int)blockDim.x; ++i) m = fmax(m, red[i]);
+                *frac = m;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// CTAs per SM the register budget is sized for (about 64K / (threads x 2) registers
+// per thread bounds the allocation the compiler may use)
+template <int LOGM, int LEVELS>
+struct BootMinCtas {
+    static constexpr int threads = 2 * LEVELS * (1 << LOGM) / 8;
+    static constexpr int value = threads >= 512 ? 1 : (threads >= 256 ? 2 : 4);
+};
+
 // Blind rotation + sample extraction of B LWEs (in: [B][n+1], mask then body) into
-// out [B][N+1] (extracted mask, body).  bsk_f: [n][2 levels][2][M] spectra.
-template <int N, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_cggi_fft_bootstrap(uint32_t* __restrict__ out,
-                                                                const uint32_t* __restrict__ in, long long B,
-                                                                const double2* __restrict__ bsk_f,
-                                                                const uint32_t* __restrict__ tv, int n, int base_log,
-                                                                int levels, uint32_t offset,
-                                                                const double2* __restrict__ g_tw,
-                                                                const double2* __restrict__ g_twist) {
-    constexpr int M = N / 2;
+// out [B][N+1] (extracted mask, body).  bsk_f: [n][2 levels][2][M] spectra in key order.
+// Block: 2 levels x M/8 threads; persistent over the LWEs.
+template <int LOGM, int LEVELS>
+__global__ void __launch_bounds__(2 * LEVELS * (1 << LOGM) / 8, BootMinCtas<LOGM, LEVELS>::value) k_cggi_fft_bootstrap(
+    uint32_t* __restrict__ out, const uint32_t* __restrict__ in, long long B, const double2* __restrict__ bsk_f,
+    const uint32_t* __restrict__ tv, int n, int base_log, uint32_t offset, const double2* __restrict__ g_tw,
+    const double2* __restrict__ g_twist) {
+    constexpr int M = 1 << LOGM, N = 2 * M, R = 2 * LEVELS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
     double2* spec = reinterpret_cast<double2*>(acc + 2 * N);
-    double2* outs = spec + 2 * levels * M;
-    double2* tw = outs + 2 * M;
-    double2* twist = tw + M / 2;
-    for (int k = threadIdx.x; k < M / 2; k += THREADS) tw[k] = g_tw[k];
-    for (int k = threadIdx.x; k < M; k += THREADS) twist[k] = g_twist[k];
-    int logN2 = 0;
-    while ((1 << logN2) < 2 * N) ++logN2;
-    const double inv_m = 1.0 / (double)M;
-    const int R = 2 * levels;
-    __syncthreads();
-
+    double2* outs = spec + R * M;
+    constexpr int logN2 = LOGM + 2;
     for (long long lwe = blockIdx.x; lwe < B; lwe += gridDim.x) {
         const uint32_t* a = in + lwe * (long long)(n + 1);
         const int rb = modswitch(a[n] + offset, logN2);
         const int e0 = (2 * N - rb) & (2 * N - 1);
-        for (int k = threadIdx.x; k < N; k += THREADS) {
+        for (int k = threadIdx.x; k < N; k += blockDim.x) {
             acc[k] = 0;
             acc[N + k] = rot_at<N>(tv, k, e0);
         }
         __syncthreads();
         for (int i = 0; i < n; ++i) {
             const int ai = modswitch(__ldg(a + i), logN2);
-            // digits of (acc X^ai - acc), folded and twisted, into spec[c * levels + l]
-            for (int jj = threadIdx.x; jj < 2 * M; jj += THREADS) {
-                const int c = jj / M, j = jj - c * M;
-                const uint32_t* p = acc + c * N;
-                const uint32_t lo = rot_at<N>(p, j, ai) - p[j];
-                const uint32_t hi = rot_at<N>(p, j + M, ai) - p[j + M];
-                int dl[kMaxLevels], dh[kMaxLevels];
-                decompose(dl, lo, base_log, levels);
-                decompose(dh, hi, base_log, levels);
-                const double2 w = twist[j];
-                for (int l = 0; l < levels; ++l)
-                    spec[(c * levels + l) * M + j] = cmul(make_double2((double)dl[l], (double)dh[l]), w);
-            }
-            __syncthreads();
-            fft_fwd<M, THREADS>(spec, R, M, tw);
-            // multiply-accumulate against step i's key spectra
-            const double2* key = bsk_f + (long long)i * R * 2 * M;
-            for (int jj = threadIdx.x; jj < 2 * M; jj += THREADS) {
-                const int oc = jj / M, f = jj - oc * M;
-                double2 s = make_double2(0.0, 0.0);
-                for (int r = 0; r < R; ++r) {
-                    const double2 kv = __ldg(key + ((long long)r * 2 + oc) * M + f);
-                    const double2 dv = spec[r * M + f];
-                    s.x = __fma_rn(dv.x, kv.x, __fma_rn(-dv.y, kv.y, s.x));
-                    s.y = __fma_rn(dv.x, kv.y, __fma_rn(dv.y, kv.x, s.y));
-                }
-                outs[oc * M + f] = s;
-            }
-            __syncthreads();
-            fft_inv<M, THREADS>(outs, 2, M, tw);
-            // untwist, unfold, round and add
-            for (int jj = threadIdx.x; jj < 2 * M; jj += THREADS) {
-                const int oc = jj / M, j = jj - oc * M;
-                const double2 z = cmulc(outs[oc * M + j], twist[j]);
-                const long long lo = __double2ll_rn(z.x * inv_m);
-                const long long hi = __double2ll_rn(z.y * inv_m);
-                acc[oc * N + j] += (uint32_t)lo;
-                acc[oc * N + j + M] += (uint32_t)hi;
-            }
-            __syncthreads();
+            ext_product<LOGM, LEVELS, 0>(acc, spec, outs, bsk_f + (long long)i * R * 2 * M, ai, base_log, nullptr,
+                                         nullptr, nullptr, g_tw, g_twist);
         }
         uint32_t* o = out + lwe * (long long)(N + 1);
-        for (int k = threadIdx.x; k < N; k += THREADS) o[k] = k == 0 ? acc[0] : (uint32_t)(0u - acc[N - k]);
+        for (int k = threadIdx.x; k < N; k += blockDim.x) o[k] = k == 0 ? acc[0] : (uint32_t)(0u - acc[N - k]);
         if (threadIdx.x == 0) o[N] = acc[N];
         __syncthreads();
     }
 }
 
-// Spectra of rows of N signed 32-bit coefficients (torus values read as int32):
-// out[r][M] for r < rows.  One CTA per row.
-template <int N, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_rows_to_fourier(double2* __restrict__ outp,
-                                                             const uint32_t* __restrict__ rows,
-                                                             const double2* __restrict__ g_tw,
-                                                             const double2* __restrict__ g_twist) {
-    constexpr int M = N / 2;
-    __shared__ double2 x[M];
-    __shared__ double2 tw[M / 2];
-    for (int k = threadIdx.x; k < M / 2; k += THREADS) tw[k] = g_tw[k];
-    const uint32_t* p = rows + (long long)blockIdx.x * N;
-    for (int j = threadIdx.x; j < M; j += THREADS)
-        x[j] = cmul(make_double2((double)(int32_t)p[j], (double)(int32_t)p[j + M]), g_twist[j]);
-    __syncthreads();
-    fft_fwd<M, THREADS>(x, 1, M, tw);
-    for (int j = threadIdx.x; j < M; j += THREADS) outp[(long long)blockIdx.x * M + j] = x[j];
+// out[B][2N] = ExtProd(ggsw_f, c[B][2N]) rounded; frac[b] = largest distance of an
+// unrounded coefficient to its integer.  Same code path as a blind-rotation step.
+template <int LOGM, int LEVELS>
+__global__ void __launch_bounds__(2 * LEVELS * (1 << LOGM) / 8) k_cggi_fft_extprod(
+    uint32_t* __restrict__ out, const uint32_t* __restrict__ c, const double2* __restrict__ ggsw_f, int base_log,
+    const double2* __restrict__ g_tw, const double2* __restrict__ g_twist, double* __restrict__ frac) {
+    constexpr int M = 1 << LOGM, N = 2 * M, R = 2 * LEVELS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
+    double2* spec = reinterpret_cast<double2*>(acc + 2 * N);
+    double2* outs = spec + R * M;
+    double dummy;
+    ext_product<LOGM, LEVELS, 1>(acc, spec, outs, ggsw_f, 0, base_log, c + (long long)blockIdx.x * 2 * N,
+                                 out + (long long)blockIdx.x * 2 * N, frac ? frac + blockIdx.x : &dummy, g_tw,
+                                 g_twist);
 }
 
-// out[B][2N] = ExtProd(ggsw_f, c[B][2N]) rounded, for measuring FFT error: same code
-// path as one CMUX step with a fixed difference.
-template <int N, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_cggi_fft_extprod(uint32_t* __restrict__ out,
-                                                              const uint32_t* __restrict__ c,
-                                                              const double2* __restrict__ ggsw_f, int base_log,
-                                                              int levels, const double2* __restrict__ g_tw,
-                                                              const double2* __restrict__ g_twist,
-                                                              double* __restrict__ frac_err) {
-    constexpr int M = N / 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2* spec = reinterpret_cast<double2*>(smem_raw);
-    double2* outs = spec + 2 * levels * M;
-    double2* tw = outs + 2 * M;
-    double2* twist = tw + M / 2;
-    const int R = 2 * levels;
-    for (int k = threadIdx.x; k < M / 2; k += THREADS) tw[k] = g_tw[k];
-    for (int k = threadIdx.x; k < M; k += THREADS) twist[k] = g_twist[k];
-    __syncthreads();
-    const uint32_t* cc = c + (long long)blockIdx.x * 2 * N;
-    for (int jj = threadIdx.x; jj < 2 * M; jj += THREADS) {
-        const int comp = jj / M, j = jj - comp * M;
-        int dl[kMaxLevels], dh[kMaxLevels];
-        decompose(dl, cc[comp * N + j], base_log, levels);
-        decompose(dh, cc[comp * N + j + M], base_log, levels);
-        for (int l = 0; l < levels; ++l)
-            spec[(comp * levels + l) * M + j] = cmul(make_double2((double)dl[l], (double)dh[l]), twist[j]);
-    }
-    __syncthreads();
-    fft_fwd<M, THREADS>(spec, R, M, tw);
-    for (int jj = threadIdx.x; jj < 2 * M; jj += THREADS) {
-        const int oc = jj / M, f = jj - oc * M;
-        double2 s = make_double2(0.0, 0.0);
-        for (int r = 0; r < R; ++r) {
-            const double2 kv = ggsw_f[((long long)r * 2 + oc) * M + f];
-            const double2 dv = spec[r * M + f];
-            s.x = __fma_rn(dv.x, kv.x, __fma_rn(-dv.y, kv.y, s.x));
-            s.y = __fma_rn(dv.x, kv.y, __fma_rn(dv.y, kv.x, s.y));
+// Spectra of rows of N signed 32-bit coefficients (torus values read as int32), in key
+// order: out[r][k * M/8 + t] = spectrum element 8 t + k.  One block of M/8 threads per row.
+template <int LOGM>
+__global__ void __launch_bounds__((1 << LOGM) / 8) k_rows_to_fourier(double2* __restrict__ outp,
+                                                                   const uint32_t* __restrict__ rows,
+                                                                   const double2* __restrict__ g_tw,
+                                                                   const double2* __restrict__ g_twist) {
+    constexpr int M = 1 << LOGM, TPA = M / 8, NP = Passes<LOGM>::count;
+    __shared__ double2 x[M];
+    const int t = threadIdx.x;
+    const uint32_t* p = rows + (long long)blockIdx.x * 2 * M;
+    {
+        using Q = PassOf<LOGM, 0>;
+        double2 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int j = pidx<Q::LO>(t, k);
+            v[k] = cmul(make_double2((double)(int32_t)p[j], (double)(int32_t)p[j + M]), __ldg(&g_twist[j]));
         }
-        outs[oc * M + f] = s;
+        dif<LOGM, Q::LO, Q::NST>(v, t, g_tw);
+        put8<Q::LO>(x, v, t);
     }
     __syncthreads();
-    fft_inv<M, THREADS>(outs, 2, M, tw);
-    uint32_t* o = out + (long long)blockIdx.x * 2 * N;
-    double worst = 0.0;
-    for (int jj = threadIdx.x; jj < 2 * M; jj += THREADS) {
-        const int oc = jj / M, j = jj - oc * M;
-        const double2 z = cmulc(outs[oc * M + j], twist[j]);
-        const double re = z.x / (double)M, im = z.y / (double)M;
-        const double rr = rint(re), ri = rint(im);
-        worst = fmax(worst, fmax(fabs(re - rr), fabs(im - ri)));
-        o[oc * N + j] = (uint32_t)(long long)rr;
-        o[oc * N + j + M] = (uint32_t)(long long)ri;
-    }
-    // per-row worst distance to the nearest integer (how close rounding came to failing)
-    __shared__ double red[THREADS];
-    red[threadIdx.x] = worst;
-    __syncthreads();
-    for (int s2 = THREADS / 2; s2 > 0; s2 >>= 1) {
-        if ((int)threadIdx.x < s2) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s2]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0 && frac_err) frac_err[blockIdx.x] = red[0];
+    fwd_rest<LOGM, 1>(x, t, true, g_tw);
+    using QL = PassOf<LOGM, NP - 1>;
+    double2* o = outp + (long long)blockIdx.x * M;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k * TPA + t] = x[swz(pidx<QL::LO>(t, k))];
 }
 
 // LWE key switch: out[b] = (0, in[b].body) - sum_{j,l} d_{b,j,l} KSK[j][l], digits of
@@ -398,51 +531,84 @@ bool check_shape(int N, int levels, int base_log, const char* where) {
     return true;
 }
 
-template <int N>
-int launch_bootstrap(uint32_t* out, const uint32_t* in, long long B, const double2* bsk_f, const uint32_t* tv, int n,
-                     int base_log, int levels, uint32_t offset, const FourierTables* ft, cudaStream_t st) {
-    constexpr int THREADS = N / 4 < 128 ? 128 : N / 4;
-    const size_t smem = Smem<N>::bytes(levels);
-    int e = (int)cudaFuncSetAttribute(k_cggi_fft_bootstrap<N, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int LOGM, int LEVELS>
+int launch_bootstrap_t(uint32_t* out, const uint32_t* in, long long B, const double2* bsk_f, const uint32_t* tv,
+                       int n, int base_log, uint32_t offset, const FourierTables* ft, cudaStream_t st) {
+    constexpr int THREADS = 2 * LEVELS * (1 << LOGM) / 8;
+    const size_t smem = Smem<(2 << LOGM)>::bytes(LEVELS);
+    int e = (int)cudaFuncSetAttribute(k_cggi_fft_bootstrap<LOGM, LEVELS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem);
     if (e) return e;
     int per_sm = 0;
-    e = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cggi_fft_bootstrap<N, THREADS>, THREADS, smem);
+    e = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cggi_fft_bootstrap<LOGM, LEVELS>, THREADS, smem);
     if (e) return e;
     long long grid = (long long)(per_sm > 0 ? per_sm : 1) * sm_count();
     if (grid > B) grid = B;
-    k_cggi_fft_bootstrap<N, THREADS><<<(unsigned)grid, THREADS, smem, st>>>(out, in, B, bsk_f, tv, n, base_log, levels,
-                                                                          offset, ft->d_tw, ft->d_twist);
+    k_cggi_fft_bootstrap<LOGM, LEVELS><<<(unsigned)grid, THREADS, smem, st>>>(out, in, B, bsk_f, tv, n, base_log, offset,
+                                                                            ft->d_tw, ft->d_twist);
     note_launch();
     return (int)cudaGetLastError();
 }
 
-template <int N>
-int launch_to_fourier(double2* outp, const uint32_t* rows, long long count, const FourierTables* ft, cudaStream_t st) {
-    constexpr int THREADS = N / 4 < 128 ? 128 : N / 4;
+template <int LOGM, int LEVELS>
+int launch_extprod_t(uint32_t* out, const uint32_t* c, long long B, const double2* ggsw_f, int base_log,
+                     const FourierTables* ft, double* frac, cudaStream_t st) {
+    constexpr int THREADS = 2 * LEVELS * (1 << LOGM) / 8;
+    const size_t smem = Smem<(2 << LOGM)>::bytes(LEVELS);
+    int e = (int)cudaFuncSetAttribute(k_cggi_fft_extprod<LOGM, LEVELS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem);
+    if (e) return e;
+    k_cggi_fft_extprod<LOGM, LEVELS><<<(unsigned)B, THREADS, smem, st>>>(out, c, ggsw_f, base_log, ft->d_tw,
+                                                                       ft->d_twist, frac);
+    note_launch();
+    return (int)cudaGetLastError();
+}
+
+// (N, levels) -> template instance
+template <template <int, int> class F, typename... A>
+int dispatch_nl(int N, int levels, A... args) {
+    const int logm = N == 512 ? 8 : N == 1024 ? 9 : 10;
+    switch (logm * 8 + levels) {
+        case 8 * 8 + 1: return F<8, 1>::run(args...);
+        case 8 * 8 + 2: return F<8, 2>::run(args...);
+        case 8 * 8 + 3: return F<8, 3>::run(args...);
+        case 8 * 8 + 4: return F<8, 4>::run(args...);
+        case 9 * 8 + 1: return F<9, 1>::run(args...);
+        case 9 * 8 + 2: return F<9, 2>::run(args...);
+        case 9 * 8 + 3: return F<9, 3>::run(args...);
+        case 9 * 8 + 4: return F<9, 4>::run(args...);
+        case 10 * 8 + 1: return F<10, 1>::run(args...);
+        case 10 * 8 + 2: return F<10, 2>::run(args...);
+        case 10 * 8 + 3: return F<10, 3>::run(args...);
+        default: return F<10, 4>::run(args...);
+    }
+}
+
+template <int LOGM, int LEVELS>
+struct BootstrapF {
+    template <typename... A>
+    static int run(A... a) { return launch_bootstrap_t<LOGM, LEVELS>(a...); }
+};
+template <int LOGM, int LEVELS>
+struct ExtprodF {
+    template <typename... A>
+    static int run(A... a) { return launch_extprod_t<LOGM, LEVELS>(a...); }
+};
+
+int launch_to_fourier(int N, double2* outp, const uint32_t* rows, long long count, const FourierTables* ft,
+                      cudaStream_t st) {
     for (long long off = 0; off < count; off += 65535LL * 16) {
         const long long m = count - off < 65535LL * 16 ? count - off : 65535LL * 16;
-        k_rows_to_fourier<N, THREADS><<<(unsigned)m, THREADS, 0, st>>>(outp + off * (N / 2), rows + off * N, ft->d_tw,
-                                                                       ft->d_twist);
+        switch (N) {
+            case 512: k_rows_to_fourier<8><<<(unsigned)m, 32, 0, st>>>(outp + off * 256, rows + off * 512, ft->d_tw, ft->d_twist); break;
+            case 1024: k_rows_to_fourier<9><<<(unsigned)m, 64, 0, st>>>(outp + off * 512, rows + off * 1024, ft->d_tw, ft->d_twist); break;
+            default: k_rows_to_fourier<10><<<(unsigned)m, 128, 0, st>>>(outp + off * 1024, rows + off * 2048, ft->d_tw, ft->d_twist); break;
+        }
         note_launch();
         const int e = (int)cudaGetLastError();
         if (e) return e;
     }
     return 0;
-}
-
-template <int N>
-int launch_extprod(uint32_t* out, const uint32_t* c, long long B, const double2* ggsw_f, int base_log, int levels,
-                   const FourierTables* ft, double* frac, cudaStream_t st) {
-    constexpr int THREADS = N / 4 < 128 ? 128 : N / 4;
-    const size_t smem = sizeof(double2) * (2 * levels * (N / 2) + 2 * (N / 2) + N / 4 + N / 2);
-    int e = (int)cudaFuncSetAttribute(k_cggi_fft_extprod<N, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem);
-    if (e) return e;
-    k_cggi_fft_extprod<N, THREADS><<<(unsigned)B, THREADS, smem, st>>>(out, c, ggsw_f, base_log, levels, ft->d_tw,
-                                                                       ft->d_twist, frac);
-    note_launch();
-    return (int)cudaGetLastError();
 }
 
 }  // namespace
@@ -459,13 +625,7 @@ int vfhe_cuda_cggi_fft_to_fourier(double* d_out, const uint32_t* d_rows, uint64_
     if (!check_shape((int)N, 1, 1, where)) return 1;
     const FourierTables* ft = fourier_tables((int)N);
     if (!ft) return check_cuda(cudaErrorMemoryAllocation, where) ? 0 : 1;
-    cudaStream_t st = (cudaStream_t)stream;
-    int e;
-    switch (N) {
-        case 512: e = launch_to_fourier<512>((double2*)d_out, d_rows, (long long)count, ft, st); break;
-        case 1024: e = launch_to_fourier<1024>((double2*)d_out, d_rows, (long long)count, ft, st); break;
-        default: e = launch_to_fourier<2048>((double2*)d_out, d_rows, (long long)count, ft, st); break;
-    }
+    const int e = launch_to_fourier((int)N, (double2*)d_out, d_rows, (long long)count, ft, (cudaStream_t)stream);
     return check_cuda(e, where) ? 0 : 1;
 }
 
@@ -482,22 +642,8 @@ int vfhe_cuda_cggi_fft_bootstrap_batch(uint32_t* d_out, const uint32_t* d_in, ui
     const FourierTables* ft = fourier_tables((int)N);
     if (!ft) return check_cuda(cudaErrorMemoryAllocation, where) ? 0 : 1;
     const uint32_t offset = (uint32_t)((1ULL << 32) / (4ULL * torus_base));
-    cudaStream_t st = (cudaStream_t)stream;
-    int e;
-    switch (N) {
-        case 512:
-            e = launch_bootstrap<512>(d_out, d_in, (long long)batch, (const double2*)d_bsk_f, d_tv, (int)n,
-                                      (int)base_log, (int)levels, offset, ft, st);
-            break;
-        case 1024:
-            e = launch_bootstrap<1024>(d_out, d_in, (long long)batch, (const double2*)d_bsk_f, d_tv, (int)n,
-                                       (int)base_log, (int)levels, offset, ft, st);
-            break;
-        default:
-            e = launch_bootstrap<2048>(d_out, d_in, (long long)batch, (const double2*)d_bsk_f, d_tv, (int)n,
-                                       (int)base_log, (int)levels, offset, ft, st);
-            break;
-    }
+    const int e = dispatch_nl<BootstrapF>((int)N, (int)levels, d_out, d_in, (long long)batch, (const double2*)d_bsk_f,
+                                          d_tv, (int)n, (int)base_log, offset, ft, (cudaStream_t)stream);
     return check_cuda(e, where) ? 0 : 1;
 }
 
@@ -532,22 +678,8 @@ int vfhe_cuda_cggi_fft_external_product(uint32_t* d_out, const uint32_t* d_c, ui
     }
     const FourierTables* ft = fourier_tables((int)N);
     if (!ft) return check_cuda(cudaErrorMemoryAllocation, where) ? 0 : 1;
-    cudaStream_t st = (cudaStream_t)stream;
-    int e;
-    switch (N) {
-        case 512:
-            e = launch_extprod<512>(d_out, d_c, (long long)batch, (const double2*)d_ggsw_f, (int)base_log,
-                                    (int)levels, ft, d_frac, st);
-            break;
-        case 1024:
-            e = launch_extprod<1024>(d_out, d_c, (long long)batch, (const double2*)d_ggsw_f, (int)base_log,
-                                     (int)levels, ft, d_frac, st);
-            break;
-        default:
-            e = launch_extprod<2048>(d_out, d_c, (long long)batch, (const double2*)d_ggsw_f, (int)base_log,
-                                     (int)levels, ft, d_frac, st);
-            break;
-    }
+    const int e = dispatch_nl<ExtprodF>((int)N, (int)levels, d_out, d_c, (long long)batch, (const double2*)d_ggsw_f,
+                                        (int)base_log, ft, d_frac, (cudaStream_t)stream);
     return check_cuda(e, where) ? 0 : 1;
 }
 

@@ -100,4 +100,8 @@ void forget_launches(uint64_t n);
 // stream capture, so that launches recorded into graphs make no attribute calls.
 int prepare_ntt_kernels();
 
+// Copy the device flag that persistent transform kernels raise when a bounded wait
+// for a tile copy gave up (0 = never).
+int read_tile_fault(int* out);
+
 }  // namespace vc

@@ -193,24 +193,112 @@ __device__ __forceinline__ double load_in(const uint64_t* p, bool in_double, boo
     return reduce ? f_reduce(v, c.q, c.qinv) : v;
 }
 
+// ---- bulk asynchronous tile loads (persistent kernels)
+//
+// A persistent CTA keeps two tile buffers: while it transforms the tiles in one, the
+// bulk-copy engine fills the other with its next group's input (cp.async.bulk from
+// global to shared memory, completion counted in bytes on an mbarrier).  Every wait
+// is bounded: if a copy has not landed after the limit, the kernel records the fault
+// in vc_tile_fault, waits once more, and carries on (results are then wrong, but the
+// kernel ends and the host can read the flag).
+
+__device__ int vc_tile_fault;  // nonzero: a tile copy wait gave up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared, `bytes` (multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int round = 0; round < 2; ++round) {
+        for (int i = 0; i < (1 << 18); ++i)
+            if (mbar_try_wait(bar, parity)) return;
+        if (round == 0) atomicExch(&vc_tile_fault, 1);
+    }
+}
+
+// Thread 0: request the input of tile group `grp` into buf (tiles at buf + l * padded).
+template <int K, bool TABLE>
+__device__ __forceinline__ void issue_group(const RowSet& rows, const PrimeInfo* primes, long long grp,
+                                            int tiles_per_cta, int tiles_per_row, double* buf, uint64_t* bar) {
+    constexpr int TILE = 1 << K, PADDED = TILE + (TILE >> 4);
+    mbar_expect_tx(bar, (uint32_t)(tiles_per_cta * TILE * 8));
+    for (int l = 0; l < tiles_per_cta; ++l) {
+        const Tile rr = locate<TABLE>(rows, primes, K, grp * tiles_per_cta + l, tiles_per_row);
+        bulk_load(buf + l * PADDED, rr.src, TILE * 8, bar);
+    }
+}
+
 // Forward transform of the low K bits of each row.  IN_D: the row holds centred
 // doubles from the column pass; otherwise canonical (or foreign, with reduce_input)
 // uint64 residues.  Output: canonical uint64.
-// PERSIST: CTAs walk the ngroups groups of tiles_per_cta tiles (every thread of a CTA
-// makes the same number of trips); otherwise CTA b takes group b and the grid covers
-// all groups (the loop body runs once, and the compiler keeps the lean straight-line
-// register allocation).
+// PERSIST: a grid of a few CTAs per SM walks the ngroups groups of tiles_per_cta tiles
+// (every thread of a CTA makes the same number of trips), loading each group's input
+// with bulk asynchronous copies into one of two shared buffers while the previous
+// group computes; otherwise CTA b takes group b, reads its input straight from global
+// memory, and the compiler keeps the lean straight-line register allocation.
 template <int K, bool IN_D, bool PERSIST, bool TABLE>
 __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __grid_constant__ RowSet rows,
                                                                      const PrimeInfo* __restrict__ primes,
                                                                      int tiles_per_cta, int tiles_per_row,
                                                                      long long ngroups) {
     constexpr int TPT = 1 << (K - 4);
-    extern __shared__ double fsm[];
+    constexpr int PADDED = (1 << K) + (1 << (K - 4));
+    extern __shared__ __align__(128) double fsm[];
+    __shared__ uint64_t bars[2];
     const int lt = threadIdx.x / TPT;
     const int t = threadIdx.x - lt * TPT;
-    double* sm = fsm + lt * ((1 << K) + (1 << (K - 4)));
-    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    double* bufs[2] = {fsm, fsm + (PERSIST ? tiles_per_cta * PADDED : 0)};
+    if (PERSIST) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            if ((long long)blockIdx.x < ngroups)
+                issue_group<K, TABLE>(rows, primes, blockIdx.x, tiles_per_cta, tiles_per_row, bufs[0], &bars[0]);
+        }
+        __syncthreads();
+    }
+    int trip = 0;
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x, ++trip) {
+    const int cur = PERSIST ? (trip & 1) : 0;
+    double* sm = bufs[cur] + lt * PADDED;
+    if (PERSIST) {
+        const long long nxt = grp + gridDim.x;
+        if (threadIdx.x == 0 && nxt < ngroups) {
+            // the other buffer's last generic writes (exchanges) precede this async write
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue_group<K, TABLE>(rows, primes, nxt, tiles_per_cta, tiles_per_row, bufs[cur ^ 1], &bars[cur ^ 1]);
+        }
+        mbar_wait_bounded(&bars[cur], (uint32_t)((trip >> 1) & 1));
+    }
     const long long tile = grp * tiles_per_cta + lt;
     const Tile r = locate<TABLE>(rows, primes, K, tile, tiles_per_row);
     const PrimeInfo& pi = *r.pi;
@@ -229,8 +317,15 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
     // so their latency overlaps the barrier
     PassTw<L1, K - 1, L1> tw1;
     f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c.tw);
+    if (PERSIST) {
+        const uint64_t* staged = reinterpret_cast<const uint64_t*>(sm);
 #pragma unroll
-    for (int m = 0; m < 16; ++m) x[m] = load_in(r.src + own<L1>(t, m), IN_D, red, c);
+        for (int m = 0; m < 16; ++m) x[m] = load_in(staged + own<L1>(t, m), IN_D, red, c);
+        __syncthreads();  // every input is in registers before the exchanges reuse the buffer
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = load_in(r.src + own<L1>(t, m), IN_D, red, c);
+    }
     f_fwd_bits<K, L1, K - 1, L1>(x, tw1, c);
     PassTw<L2, L1 - 1, L2> tw2;
     f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c.tw);
@@ -277,11 +372,34 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __gr
                                                                      int tiles_per_cta, int tiles_per_row,
                                                                      long long ngroups) {
     constexpr int TPT = 1 << (K - 4);
-    extern __shared__ double fsm[];
+    constexpr int PADDED = (1 << K) + (1 << (K - 4));
+    extern __shared__ __align__(128) double fsm[];
+    __shared__ uint64_t bars[2];
     const int lt = threadIdx.x / TPT;
     const int t = threadIdx.x - lt * TPT;
-    double* sm = fsm + lt * ((1 << K) + (1 << (K - 4)));
-    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    double* bufs[2] = {fsm, fsm + (PERSIST ? tiles_per_cta * PADDED : 0)};
+    if (PERSIST) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            if ((long long)blockIdx.x < ngroups)
+                issue_group<K, TABLE>(rows, primes, blockIdx.x, tiles_per_cta, tiles_per_row, bufs[0], &bars[0]);
+        }
+        __syncthreads();
+    }
+    int trip = 0;
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x, ++trip) {
+    const int cur = PERSIST ? (trip & 1) : 0;
+    double* sm = bufs[cur] + lt * PADDED;
+    if (PERSIST) {
+        const long long nxt = grp + gridDim.x;
+        if (threadIdx.x == 0 && nxt < ngroups) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue_group<K, TABLE>(rows, primes, nxt, tiles_per_cta, tiles_per_row, bufs[cur ^ 1], &bars[cur ^ 1]);
+        }
+        mbar_wait_bounded(&bars[cur], (uint32_t)((trip >> 1) & 1));
+    }
     const long long tile = grp * tiles_per_cta + lt;
     const Tile r = locate<TABLE>(rows, primes, K, tile, tiles_per_row);
     const PrimeInfo& pi = *r.pi;
@@ -295,13 +413,15 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __gr
     constexpr int F1 = 4 < (K - 4) ? 4 : (K - 4);
     constexpr int F2 = 8 < (K - 4) ? 8 : (K - 4);
     constexpr int F3 = 12 < (K - 4) ? 12 : (K - 4);
-    const ulonglong2* in = reinterpret_cast<const ulonglong2*>(r.src + 16 * t);
+    const ulonglong2* in = reinterpret_cast<const ulonglong2*>(
+        (PERSIST ? reinterpret_cast<const uint64_t*>(sm) : r.src) + 16 * t);
 #pragma unroll
     for (int m = 0; m < 16; m += 2) {
         const ulonglong2 v = in[m / 2];
         x[m] = f_from_u64(v.x);
         x[m + 1] = f_from_u64(v.y);
     }
+    if (PERSIST) __syncthreads();  // every input is in registers before the exchanges reuse the buffer
     PassTw<0, 0, 3> tw1;
     f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c.tw);
     f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
@@ -489,9 +609,10 @@ int tile_launch(const RowSet& rows, const PrimeInfo* d_primes, int mode, int til
         if (cap < grid) grid = cap;
     }
     if (grid > 0x7fffffffLL) grid = 0x7fffffffLL;
-    const size_t smem = sizeof(double) * (size_t)tiles_per_cta * ((1 << K) + (1 << (K - 4)));
-    const int threads = TPT * tiles_per_cta;
     const bool persist = grid < ngroups;
+    // persistent CTAs double-buffer their tiles
+    const size_t smem = sizeof(double) * (size_t)tiles_per_cta * ((1 << K) + (1 << (K - 4))) * (persist ? 2 : 1);
+    const int threads = TPT * tiles_per_cta;
     int e = 0;
 #define VC_TILE_LAUNCH(KERN)                                                                              \
     do {                                                                                                  \
@@ -578,6 +699,10 @@ int prepare_k() {
 }
 
 }  // namespace
+
+int read_tile_fault(int* out) {
+    return (int)cudaMemcpyFromSymbol(out, vc_tile_fault, sizeof(int));
+}
 
 int prepare_ntt_kernels() {
     int e = prepare_k<8>();
