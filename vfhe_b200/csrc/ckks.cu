@@ -46,9 +46,10 @@ __device__ __forceinline__ uint64_t inc_prod_slot(const uint64_t* u, const uint6
 }
 
 // d0 = a1 a2, d1 = a1 b2 + b1 a2, d2 = b1 b2 in the NTT domain (mlwe.c:665-709 at rank 1).
+template <int S>
 __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ c1,
                          const uint64_t* __restrict__ c2, const __grid_constant__ LimbPrimes lp,
-                         const PrimeInfo* __restrict__ primes, int L, long long N, int S) {
+                         const PrimeInfo* __restrict__ primes, int L, long long N) {
     const int by = blockIdx.y;
     const int b = by / L, k = by - b * L;
     const PrimeInfo pi = primes[lp.p[k]];
@@ -83,9 +84,10 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
 // (*) the ring's incomplete product, pointwise at split 1)
 // D: [B][nd][ne][N]; K_b: [digits][2][ne][N] (only the first nd digits are used);
 // acc: [B][2][ne][N].  Thread index over N = (block o, slot x).
+template <int S>
 __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
                       const uint64_t* const* __restrict__ keys, const __grid_constant__ LimbPrimes lp,
-                      const PrimeInfo* __restrict__ primes, int nd, int ne, long long N, int S) {
+                      const PrimeInfo* __restrict__ primes, int nd, int ne, long long N) {
     const int by = blockIdx.y;
     const int b = by / ne, i = by - b * ne;
     const PrimeInfo pi = primes[lp.p[i]];
@@ -119,14 +121,29 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
         }
         return;
     }
-    const long long P = N / S;
-    if (pi.fp64 && (S == 2 || S == 4)) {
-        for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < P;
+    if constexpr (S == 1) {
+        // pointwise, primes of any size: 64-bit Barrett products
+        for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
              x += (long long)gridDim.x * blockDim.x) {
-            if (S == 2) mac_slots<2>(oa, ob, d, dstride, ka, kb, kstride, nd, P, x, pi);
-            else mac_slots<4>(oa, ob, d, dstride, ka, kb, kstride, nd, P, x, pi);
+            uint64_t sa = 0, sb = 0;
+            for (int j = 0; j < nd; ++j) {
+                const uint64_t v = d[j * dstride + x];
+                sa = add_mod(sa, mul_mod(v, ka[j * kstride + x], pi), pi.q);
+                sb = add_mod(sb, mul_mod(v, kb[j * kstride + x], pi), pi.q);
+            }
+            oa[x] = neg_mod(sa, pi.q);
+            ob[x] = neg_mod(sb, pi.q);
         }
         return;
+    }
+    const long long P = N / S;
+    if constexpr (S == 2 || S == 4) {
+        if (pi.fp64) {
+            for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < P;
+                 x += (long long)gridDim.x * blockDim.x)
+                mac_slots<S>(oa, ob, d, dstride, ka, kb, kstride, nd, P, x, pi);
+            return;
+        }
     }
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -205,6 +222,11 @@ __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __re
     }
 }
 
+// One k_mac launch for the ring's split degree (each split degree is its own kernel,
+// so the pointwise one keeps its small register footprint).
+void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const LimbPrimes& lpe,
+                int nd, int ne, long long N, uint64_t B, cudaStream_t st);
+
 // Grid for one launch of a per-coefficient kernel; every call site launches exactly
 // one kernel with it, so it also counts the launch.
 dim3 grid_xy(long long n, long long y) {
@@ -213,6 +235,18 @@ dim3 grid_xy(long long n, long long y) {
     if (blocks > 64) blocks = 64;
     if (blocks < 1) blocks = 1;
     return dim3((unsigned)blocks, (unsigned)y, 1);
+}
+
+void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const LimbPrimes& lpe,
+                int nd, int ne, long long N, uint64_t B, cudaStream_t st) {
+    const dim3 g = grid_xy(N, (long long)B * ne);
+    switch (t->pub.split_degree) {
+        case 1: k_mac<1><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
+        case 2: k_mac<2><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
+        case 4: k_mac<4><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
+        case 8: k_mac<8><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
+        default: k_mac<16><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
+    }
 }
 
 bool check_shape(IncNtt* t, const uint32_t* limbs, uint32_t L, uint32_t special, const char* where) {
@@ -343,13 +377,17 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
 
     std::vector<const uint64_t*> kp(B, rlk);
     if (!check_cuda(upload_small(keyptrs, (const uint64_t*)kp.data(), B, st), where)) return 1;
-    k_tensor<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N,
-                                                            (int)t->pub.split_degree);
+    switch (t->pub.split_degree) {
+        case 1: k_tensor<1><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
+        case 2: k_tensor<2><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
+        case 4: k_tensor<4><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
+        case 8: k_tensor<8><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
+        default: k_tensor<16><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
+    }
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
     if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    k_mac<<<grid_xy(N, (long long)B * ne), 256, 0, st>>>(acc, D, (const uint64_t* const*)keyptrs, lpe, t->d_info,
-                                                          nl, ne, N, (int)t->pub.split_degree);
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, lpe, nl, ne, N, B, st);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
@@ -397,8 +435,7 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
         src = Pm;
     }
     if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    k_mac<<<grid_xy(N, (long long)B * ne), 256, 0, st>>>(acc, D, (const uint64_t* const*)keyptrs, lpe, t->d_info,
-                                                          nl, ne, N, (int)t->pub.split_degree);
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, lpe, nl, ne, N, B, st);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
