@@ -14,7 +14,9 @@ def test_candidates_respect_kernel_limits():
         assert (logP if logP <= 13 else 12, 0, 0) in cands  # the built-in schedule is always timed
         for k, tpc, cps in cands:
             assert 8 <= k <= 13 and k <= logP and logP - k <= 5
-            assert tpc in (0, 1, 2, 4, 8) and cps in (0, 2, 4)
+            assert tpc in (0, 1, 2, 4, 8) and cps in (0, 2, 4, -1)
+            if cps == -1:
+                assert 11 <= k <= 13 and 1 <= logP - k <= 3
             if tpc:
                 assert (1 << (k - 4)) * tpc <= max(256, 1 << (k - 4))
 

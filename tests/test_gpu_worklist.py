@@ -57,11 +57,13 @@ def test_schedules_do_not_change_results(cuda):
     ffi, lib = cuda.ffi, cuda.lib
     rng = np.random.default_rng(7)
     st = ffi.cast("void*", torch.cuda.current_stream().cuda_stream)
+    # ctas_per_sm = -1: the fused column + tile transform on a thread-block cluster
     cases = [(2**10, 1, [(0, 2, 0), (0, 1, 2), (0, 4, 1), (0, 8, 0)]),
-             (2**13, 1, [(0, 1, 0), (11, 0, 0), (12, 1, 2)]),
-             (2**14, 1, [(13, 0, 0), (11, 2, 0), (12, 1, 1)]),
-             (2**16, 1, [(13, 0, 0), (12, 0, 2), (11, 4, 0), (11, 2, 0)]),
-             (2**16, 4, [(13, 0, 1), (11, 2, 0)])]
+             (2**13, 1, [(0, 1, 0), (11, 0, 0), (12, 1, 2), (12, 0, -1), (11, 0, -1)]),
+             (2**14, 1, [(13, 0, 0), (11, 2, 0), (12, 1, 1), (12, 0, -1), (11, 0, -1), (13, 0, -1)]),
+             (2**15, 1, [(12, 0, -1), (13, 0, -1)]),
+             (2**16, 1, [(13, 0, 0), (12, 0, 2), (11, 4, 0), (11, 2, 0), (13, 0, -1)]),
+             (2**16, 4, [(13, 0, 1), (11, 2, 0), (12, 0, -1)])]
     for N, split, scheds in cases:
         R = Ring(N, prime_size=[50] * 3, split_degree=split, engine=cuda)
         logP = (N // split).bit_length() - 1

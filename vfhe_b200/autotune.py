@@ -41,6 +41,10 @@ def candidates(logP: int) -> list[tuple[int, int, int]]:
         for tpc in sorted(set(tpcs)):
             for cps in (0, 2, 4):
                 out.append((k, tpc, cps))
+    # fused split transforms on a thread-block cluster of 2^(logP - k) CTAs (ctas_per_sm = -1)
+    for k in (11, 12, 13):
+        if 1 <= logP - k <= 3:
+            out.append((k, 0, -1))
     return out
 
 

@@ -11,6 +11,7 @@
 //     starting from |x| <= q stay below 4q; all residues are reduced at pass end;
 //   inverse (GS: x + y, w (x - y)): sums double, so the sum outputs are reduced after
 //     every second stage and at pass end; products are always <= 3q/4.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -574,6 +575,237 @@ __global__ void __launch_bounds__(256) k_col_f(const __grid_constant__ RowSet ro
 // Largest dynamic shared memory the tile kernels may be given (200 KiB of the 227).
 constexpr size_t kTileSmemMax = 200 * 1024;
 
+// ---- fused split transforms on a thread-block cluster
+//
+// A row of P = 2^(K + K1) residues is held by a cluster of C = 2^K1 CTAs, CTA r owning
+// the contiguous block [r 2^K, (r + 1) 2^K) in its shared memory.  The radix-2^K1
+// column stages (index bits K .. logP-1) pair elements of the same in-block position
+// across the C blocks, so each CTA runs them on a 1/C share of the positions with
+// loads and stores into the other CTAs' shared memory (distributed shared memory);
+// the low K bits are then the usual register-blocked tile passes, fed from shared
+// memory.  The row crosses HBM once in and once out, instead of twice each way for
+// the column kernel + tile kernel pair, and it is one launch.
+namespace cgx = cooperative_groups;
+
+template <int K, int K1, bool TABLE>
+__global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __grid_constant__ RowSet rows,
+                                                                      const PrimeInfo* __restrict__ primes) {
+    constexpr int TPT = 1 << (K - 4), TILE = 1 << K, C = 1 << K1;
+    extern __shared__ __align__(128) double fsm[];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const long long row = blockIdx.x / C;
+    const int t = threadIdx.x;
+    const Tile r = locate<TABLE>(rows, primes, K, row * C + rank, C);
+    const PrimeInfo& pi = *r.pi;
+    FCtx c;
+    c.q = pi.qd;
+    c.qinv = pi.qinv;
+    c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
+    const int logP = rows.logP;
+    const bool red = rows.reduce_input != 0;
+    // phase 1: this CTA's block, natural order, as residues in doubles
+#pragma unroll
+    for (int m = 0; m < 16; ++m) fsm[t + TPT * m] = load_in(r.src + t + TPT * m, false, red, c);
+    cluster.sync();
+    // phase 2: column stages on positions [rank TILE/C, (rank + 1) TILE/C)
+    {
+        double* blk[C];
+#pragma unroll
+        for (int m = 0; m < C; ++m) blk[m] = cluster.map_shared_rank(fsm, m);
+        double2 w[K1 * C / 2];  // stage bb's twiddles (at most C/2) do not depend on the position
+#pragma unroll
+        for (int bb = K1 - 1; bb >= 0; --bb)
+#pragma unroll
+            for (int m = 0; m < C; ++m)
+                if (!(m & (1 << bb))) w[(K1 - 1 - bb) * (C / 2) + (m >> (bb + 1))] =
+                    __ldg(&c.tw[(1 << (logP - K - 1 - bb)) + (m >> (bb + 1))]);
+        for (int j = rank * (TILE / C) + t; j < (rank + 1) * (TILE / C); j += TPT) {
+            double x[C];
+#pragma unroll
+            for (int m = 0; m < C; ++m) x[m] = blk[m][j];
+#pragma unroll
+            for (int bb = K1 - 1; bb >= 0; --bb) {
+#pragma unroll
+                for (int m = 0; m < C; ++m) {
+                    if (m & (1 << bb)) continue;
+                    const double2 ww = w[(K1 - 1 - bb) * (C / 2) + (m >> (bb + 1))];
+                    const double v = f_mulmod(x[m | (1 << bb)], ww.x, ww.y, c.q);
+                    const double u = x[m];
+                    x[m] = __dadd_rn(u, v);
+                    x[m | (1 << bb)] = __dsub_rn(u, v);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < C; ++m) blk[m][j] = f_reduce(x[m], c.q, c.qinv);
+        }
+    }
+    cluster.sync();
+    // phase 3: the tile passes over the low K bits of this block
+    const int hi = rank;
+    double x[16];
+    constexpr int L1 = K - 4;
+    constexpr int L2 = (K - 8) > 0 ? (K - 8) : 0;
+    constexpr int L3 = (K - 12) > 0 ? (K - 12) : 0;
+    PassTw<L1, K - 1, L1> tw1;
+    f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c.tw);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) x[m] = fsm[own<L1>(t, m)];
+    __syncthreads();  // every value is in registers before the exchanges reuse the buffer
+    f_fwd_bits<K, L1, K - 1, L1>(x, tw1, c);
+    PassTw<L2, L1 - 1, L2> tw2;
+    f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c.tw);
+    fput<L1>(fsm, x, t);
+    __syncthreads();
+    fget<L2>(x, fsm, t);
+    f_fwd_bits<K, L2, L1 - 1, L2>(x, tw2, c);
+    if constexpr (L2 > 0) {
+        PassTw<L3, L2 - 1, L3> tw3;
+        f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c.tw);
+        __syncthreads();
+        fput<L2>(fsm, x, t);
+        __syncthreads();
+        fget<L3>(x, fsm, t);
+        f_fwd_bits<K, L3, L2 - 1, L3>(x, tw3, c);
+        if constexpr (L3 > 0) {
+            PassTw<0, L3 - 1, 0> tw4;
+            f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c.tw);
+            __syncthreads();
+            fput<L3>(fsm, x, t);
+            __syncthreads();
+            fget<0>(x, fsm, t);
+            f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
+        }
+    }
+    ulonglong2* out = reinterpret_cast<ulonglong2*>(r.dst + 16 * t);
+#pragma unroll
+    for (int m = 0; m < 16; m += 2) {
+        ulonglong2 v;
+        v.x = f_to_canonical(x[m], c.q, c.qinv, pi.q);
+        v.y = f_to_canonical(x[m + 1], c.q, c.qinv, pi.q);
+        out[m / 2] = v;
+    }
+}
+
+template <int K, int K1, bool TABLE>
+__global__ void __launch_bounds__(TileThreads<K>::value) k_fused_inv_f(const __grid_constant__ RowSet rows,
+                                                                      const PrimeInfo* __restrict__ primes) {
+    constexpr int TPT = 1 << (K - 4), TILE = 1 << K, C = 1 << K1;
+    extern __shared__ __align__(128) double fsm[];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const long long row = blockIdx.x / C;
+    const int t = threadIdx.x;
+    const Tile r = locate<TABLE>(rows, primes, K, row * C + rank, C);
+    const PrimeInfo& pi = *r.pi;
+    FCtx c;
+    c.q = pi.qd;
+    c.qinv = pi.qinv;
+    c.tw = reinterpret_cast<const double2*>(pi.inv_d);
+    const int logP = rows.logP, hi = rank;
+    // phase 1: inverse tile passes over the low K bits of this block
+    double x[16];
+    constexpr int F1 = 4 < (K - 4) ? 4 : (K - 4);
+    constexpr int F2 = 8 < (K - 4) ? 8 : (K - 4);
+    constexpr int F3 = 12 < (K - 4) ? 12 : (K - 4);
+    const ulonglong2* in = reinterpret_cast<const ulonglong2*>(r.src + 16 * t);
+#pragma unroll
+    for (int m = 0; m < 16; m += 2) {
+        const ulonglong2 v = in[m / 2];
+        x[m] = f_from_u64(v.x);
+        x[m + 1] = f_from_u64(v.y);
+    }
+    PassTw<0, 0, 3> tw1;
+    f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c.tw);
+    f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
+    if constexpr (K <= 8) {
+        PassTw<F1, 4, K - 1> tw2;
+        f_inv_tw<K, F1, 4, K - 1, false>(tw2, t, hi, logP, c.tw);
+        fput<0>(fsm, x, t);
+        __syncthreads();
+        fget<F1>(x, fsm, t);
+        f_inv_bits<K, F1, 4, K - 1, false>(x, tw2, c, pi);
+    } else {
+        PassTw<F1, 4, 7> tw2;
+        f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c.tw);
+        fput<0>(fsm, x, t);
+        __syncthreads();
+        fget<F1>(x, fsm, t);
+        f_inv_bits<K, F1, 4, 7, false>(x, tw2, c, pi);
+        if constexpr (K <= 12) {
+            PassTw<F2, 8, K - 1> tw3;
+            f_inv_tw<K, F2, 8, K - 1, false>(tw3, t, hi, logP, c.tw);
+            __syncthreads();
+            fput<F1>(fsm, x, t);
+            __syncthreads();
+            fget<F2>(x, fsm, t);
+            f_inv_bits<K, F2, 8, K - 1, false>(x, tw3, c, pi);
+        } else {
+            PassTw<F2, 8, 11> tw3;
+            f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c.tw);
+            __syncthreads();
+            fput<F1>(fsm, x, t);
+            __syncthreads();
+            fget<F2>(x, fsm, t);
+            f_inv_bits<K, F2, 8, 11, false>(x, tw3, c, pi);
+            PassTw<F3, 12, K - 1> tw4;
+            f_inv_tw<K, F3, 12, K - 1, false>(tw4, t, hi, logP, c.tw);
+            __syncthreads();
+            fput<F2>(fsm, x, t);
+            __syncthreads();
+            fget<F3>(x, fsm, t);
+            f_inv_bits<K, F3, 12, K - 1, false>(x, tw4, c, pi);
+        }
+    }
+    constexpr int LAST = K - 4;
+    __syncthreads();  // the exchanges are over: the block goes back in natural order
+#pragma unroll
+    for (int m = 0; m < 16; ++m) fsm[own<LAST>(t, m)] = x[m];
+    cluster.sync();
+    // phase 2: inverse column stages (P^-1 folded into the last), canonical results
+    {
+        double* blk[C];
+#pragma unroll
+        for (int m = 0; m < C; ++m) blk[m] = cluster.map_shared_rank(fsm, m);
+        for (int j = rank * (TILE / C) + t; j < (rank + 1) * (TILE / C); j += TPT) {
+            double y[C];
+#pragma unroll
+            for (int m = 0; m < C; ++m) y[m] = blk[m][j];
+#pragma unroll
+            for (int bb = 0; bb < K1; ++bb) {
+                const int base = (1 << logP) >> (bb + K + 1);
+                const bool last = bb == K1 - 1;
+#pragma unroll
+                for (int m = 0; m < C; ++m) {
+                    if (m & (1 << bb)) continue;
+                    const double u = y[m], v = y[m | (1 << bb)];
+                    if (last) {
+                        y[m] = f_mulmod(__dadd_rn(u, v), pi.pinv_d, pi.pinv_q, c.q);
+                        y[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), pi.ilast_d, pi.ilast_q, c.q);
+                    } else {
+                        const double2 w = __ldg(&c.tw[base + (m >> (bb + 1))]);
+                        y[m] = __dadd_rn(u, v);
+                        y[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), w.x, w.y, c.q);
+                    }
+                }
+                if (!last && (bb & 1)) {
+#pragma unroll
+                    for (int m = 0; m < C; ++m)
+                        if (!(m & (1 << bb))) y[m] = f_reduce(y[m], c.q, c.qinv);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < C; ++m)
+                reinterpret_cast<uint64_t*>(blk[m])[j] = f_to_canonical(y[m], c.q, c.qinv, pi.q);
+        }
+    }
+    cluster.sync();
+    // phase 3: this CTA's block to global memory
+    const uint64_t* done = reinterpret_cast<const uint64_t*>(fsm);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) r.dst[t + TPT * m] = done[t + TPT * m];
+}
+
 template <typename KernelT>
 int set_smem(KernelT kern, size_t bytes) {
     if (bytes <= 48 * 1024) return 0;
@@ -654,6 +886,59 @@ int col_launch(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, int 
     return (int)cudaGetLastError();
 }
 
+template <int K, int K1, bool TABLE>
+int fused_launch_t(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t st) {
+    constexpr int TPT = 1 << (K - 4), C = 1 << K1;
+    const size_t smem = sizeof(double) * (size_t)((1 << K) + (1 << (K - 4)));
+    const long long nrows = rowset_rows(rows);
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3((unsigned)(nrows * C), 1, 1);
+    cfg.blockDim = dim3(TPT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int e;
+    if (inverse) {
+        e = set_smem(k_fused_inv_f<K, K1, TABLE>, smem);
+        if (!e) e = (int)cudaLaunchKernelEx(&cfg, k_fused_inv_f<K, K1, TABLE>, rows, d_primes);
+    } else {
+        e = set_smem(k_fused_fwd_f<K, K1, TABLE>, smem);
+        if (!e) e = (int)cudaLaunchKernelEx(&cfg, k_fused_fwd_f<K, K1, TABLE>, rows, d_primes);
+    }
+    if (e) return e;
+    note_launch();
+    return (int)cudaGetLastError();
+}
+
+template <int K, int K1>
+int fused_launch(const RowSet& rows, const PrimeInfo* d, bool inverse, cudaStream_t st) {
+    return rows.table ? fused_launch_t<K, K1, true>(rows, d, inverse, st)
+                      : fused_launch_t<K, K1, false>(rows, d, inverse, st);
+}
+
+// fused cluster transform for K in 11..13 and K1 in 1..3 (cluster of 2..8 CTAs)
+int fused_dispatch(int K, int K1, const RowSet& rows, const PrimeInfo* d, bool inverse, cudaStream_t st) {
+    switch (K * 4 + K1) {
+        case 11 * 4 + 1: return fused_launch<11, 1>(rows, d, inverse, st);
+        case 11 * 4 + 2: return fused_launch<11, 2>(rows, d, inverse, st);
+        case 11 * 4 + 3: return fused_launch<11, 3>(rows, d, inverse, st);
+        case 12 * 4 + 1: return fused_launch<12, 1>(rows, d, inverse, st);
+        case 12 * 4 + 2: return fused_launch<12, 2>(rows, d, inverse, st);
+        case 12 * 4 + 3: return fused_launch<12, 3>(rows, d, inverse, st);
+        case 13 * 4 + 1: return fused_launch<13, 1>(rows, d, inverse, st);
+        case 13 * 4 + 2: return fused_launch<13, 2>(rows, d, inverse, st);
+        case 13 * 4 + 3: return fused_launch<13, 3>(rows, d, inverse, st);
+        default: return (int)cudaErrorInvalidValue;
+    }
+}
+
 int tile_dispatch(int K, const RowSet& rows, const PrimeInfo* d, int mode, int tpr, const NttSchedule& sc,
                   cudaStream_t st) {
     switch (K) {
@@ -689,12 +974,26 @@ int prepare_kp() {
     return e;
 }
 
+template <int K, int K1>
+int prepare_fused() {
+    int e = set_smem(k_fused_fwd_f<K, K1, false>, kTileSmemMax);
+    if (!e) e = set_smem(k_fused_fwd_f<K, K1, true>, kTileSmemMax);
+    if (!e) e = set_smem(k_fused_inv_f<K, K1, false>, kTileSmemMax);
+    if (!e) e = set_smem(k_fused_inv_f<K, K1, true>, kTileSmemMax);
+    return e;
+}
+
 template <int K>
 int prepare_k() {
     int e = prepare_kp<K, false, false>();
     if (!e) e = prepare_kp<K, false, true>();
     if (!e) e = prepare_kp<K, true, false>();
     if (!e) e = prepare_kp<K, true, true>();
+    if constexpr (K >= 11) {
+        if (!e) e = prepare_fused<K, 1>();
+        if (!e) e = prepare_fused<K, 2>();
+        if (!e) e = prepare_fused<K, 3>();
+    }
     return e;
 }
 
@@ -718,7 +1017,11 @@ bool set_ntt_schedule(int logP, int rows_log2, const NttSchedule& s) {
     if (logP < 8 || logP > kSchedMaxLogP || rows_log2 < 0 || rows_log2 >= kSchedRowBuckets) return false;
     if (s.tile_bits != 0 && (s.tile_bits < 8 || s.tile_bits > 13 || s.tile_bits > logP || logP - s.tile_bits > 5))
         return false;
-    if (s.tiles_per_cta < 0 || s.tiles_per_cta > 64 || s.ctas_per_sm < 0 || s.ctas_per_sm > 64) return false;
+    if (s.tiles_per_cta < 0 || s.tiles_per_cta > 64 || s.ctas_per_sm < -1 || s.ctas_per_sm > 64) return false;
+    if (s.ctas_per_sm == -1) {  // fused cluster transform: K in 11..13, logP - K in 1..3
+        const int K = s.tile_bits;
+        if (K < 11 || K > 13 || logP - K < 1 || logP - K > 3) return false;
+    }
     g_sched[logP][rows_log2] = s;
     return true;
 }
@@ -740,6 +1043,8 @@ int launch_ntt_f64(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, 
     if (K > logP || logP - K > 5) K = logP <= 13 ? logP : 12;
     if (K == logP) return tile_dispatch(logP, rows, d_primes, inverse ? 2 : 0, 1, sc, stream);
     const int K1 = logP - K;
+    if (sc.ctas_per_sm == -1 && K >= 11 && K <= 13 && K1 >= 1 && K1 <= 3)
+        return fused_dispatch(K, K1, rows, d_primes, inverse, stream);
     RowSet second = rows;
     for (int i = 0; i < rows.nlimbs; ++i) second.in[i] = rows.out[i];
     second.in_batch_stride = rows.batch_stride;
