@@ -163,7 +163,10 @@ void* new_incomplete_ntt_list(uint64_t* primes, uint64_t split_degree, uint64_t 
 
 void incNTT_extend_with_primes(void* ntt, uint64_t* new_primes, uint64_t count) {
     VC_ENTER("incNTT_extend_with_primes");
-    if (!ntt || count == 0) return;
+    if (!ntt || count == 0) {
+        if (!ntt) set_error(vc_where_, "null pool");
+        return;
+    }
     ntt_extend(as_ntt(ntt), new_primes, count);
 }
 

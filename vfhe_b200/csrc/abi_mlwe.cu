@@ -184,7 +184,7 @@ void* lwe_alloc_key(uint64_t n, uint64_t l, void* ntt) {
     VC_ENTER_RET("lwe_alloc_key", nullptr);
     (void)vc_where_;
     LweKey* k = new LweKey();
-    k->block = (uint64_t*)managed_alloc(sizeof(uint64_t) * (l * n ? l * n : 1));
+    k->block = (uint64_t*)managed_alloc(sizeof(uint64_t) * ((l * n) != 0 ? l * n : 1));
     k->pub.s = (uint64_t**)malloc(sizeof(uint64_t*) * (l ? l : 1));
     for (uint64_t i = 0; i < l; ++i) k->pub.s[i] = k->block + i * n;
     k->pub.n = n;
@@ -679,14 +679,12 @@ void mlwe_RNSc_GHS_hybrid_keyswitch(void* out, void* in, void* ksk, uint64_t lvl
     }
     RNS_MLWE o = as_mlwe(out), i = as_mlwe(in);
     RNS_MLWE** K = (RNS_MLWE**)ksk;
-    RNS_MLWE** first = K;
     uint64_t c0 = 0;
     while (c0 < i->r && K[c0] == nullptr) ++c0;
     if (c0 == i->r) {
         set_error(vc_where_, "every key-switch component is NULL");
         return;
     }
-    (void)first;
     const uint64_t extended = K[c0][0]->b->rns_mask;
     const uint64_t divide_mask = extended & ~i->b->rns_mask;
     set_masks(o, extended);

@@ -83,26 +83,8 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
     return make_double2(__fma_rn(a.x, b.x, a.y * b.y), __fma_rn(a.y, b.x, -a.x * b.y));
 }
 
-// signed digits of v rounded to its top base_log * levels bits (digit 0 most significant)
-__device__ __forceinline__ void decompose(int (&d)[kMaxLevels], uint32_t v, int base_log, int levels) {
-    const int total = base_log * levels;
-    uint64_t r = ((uint64_t)v + (1ULL << (31 - total))) >> (32 - total);
-    r &= total >= 32 ? 0xFFFFFFFFULL : ((1ULL << total) - 1);
-    const int half = 1 << (base_log - 1), full = 1 << base_log;
-#pragma unroll
-    for (int l = kMaxLevels - 1; l >= 0; --l) {
-        if (l >= levels) continue;
-        int x = (int)(r & (uint64_t)(full - 1));
-        r >>= base_log;
-        if (x >= half) {
-            x -= full;
-            r += 1;
-        }
-        d[l] = x;
-    }
-}
-
-// digit `want` of the same signed decomposition, without materialising the others
+// Digit `want` of the signed decomposition of v rounded to its top base_log * levels
+// bits (digit 0 most significant), without materialising the others
 __device__ __forceinline__ int digit_of(uint32_t v, int base_log, int levels, int want) {
     const int total = base_log * levels;
     uint64_t r = ((uint64_t)v + (1ULL << (31 - total))) >> (32 - total);

@@ -891,8 +891,7 @@ int fused_launch_t(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, 
     constexpr int TPT = 1 << (K - 4), C = 1 << K1;
     const size_t smem = sizeof(double) * (size_t)((1 << K) + (1 << (K - 4)));
     const long long nrows = rowset_rows(rows);
-    cudaLaunchConfig_t cfg;
-    memset(&cfg, 0, sizeof cfg);
+    cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(nrows * C), 1, 1);
     cfg.blockDim = dim3(TPT, 1, 1);
     cfg.dynamicSmemBytes = smem;
