@@ -649,11 +649,13 @@ def run_cuda_arm(args) -> None:
     for _ in range(3):
         eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, 8, l16, 24, sp)
     torch.cuda.synchronize()
+    profile_range(None, "ntt16", True)
     ev0.record(stream)
     for _ in range(reps):
         eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, 8, l16, 24, sp)
     ev1.record(stream)
     torch.cuda.synchronize()
+    profile_range(None, "ntt16", False)
     ms16 = ev0.elapsed_time(ev1) / reps
     limbs16 = 8 * 24 / (ms16 * 1e-3)
     del b16
@@ -744,7 +746,7 @@ def main() -> None:
     ap.add_argument("--cggi-million", action="store_true",
                     help="also bootstrap 10^6 LWEs and count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
-    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "cggi_fft", "cggi_rns", "worklist"],
+    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "ntt16", "cggi_fft", "cggi_rns", "worklist"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()
     global PROFILE_LEG

@@ -40,6 +40,12 @@ struct PrimeInfo {
     double pinv_d, pinv_q;
     double ilast_d, ilast_q;
     int fp64;
+    // The same FP64 twiddles of the four lowest stages (index bits 0..3) in lane-major
+    // order: block g of 16 residues needs 15 of them (slot s = 2^(3-b) - 1 + h for bit b),
+    // stored at ((g >> 5) * 15 + s) * 32 + (g & 31), so that a warp whose lanes hold 32
+    // consecutive blocks reads 32 consecutive (w, fl(w/q)) pairs per slot.
+    const double* fwd_lane;
+    const double* inv_lane;
 };
 
 VC_HD uint64_t umulhi(uint64_t a, uint64_t b) {

@@ -34,7 +34,64 @@ __device__ __forceinline__ int own(int t, int m) {
 struct FCtx {
     double q, qinv;
     const double2* tw;
+    const double2* lt;  // lane-major twiddles of bits 0..3 (PrimeInfo::fwd_lane / inv_lane)
 };
+
+// Position of slot (bit b, h) of 16-residue block g in a lane-major twiddle table.
+__device__ __forceinline__ int lane_tw_index(int g, int b, int h) {
+    return (((g >> 5) * 15 + ((1 << (3 - b)) - 1) + h) << 5) + (g & 31);
+}
+
+// A thread's 16 consecutive residues (p = row + 16 t): 32-byte accesses when the row is
+// 32-byte aligned (a warp then touches each sector once per instruction), else 16-byte.
+__device__ __forceinline__ void load16_u64(double (&x)[16], const uint64_t* p) {
+    if ((reinterpret_cast<uintptr_t>(p) & 31) == 0) {
+#pragma unroll
+        for (int m = 0; m < 16; m += 4) {
+            uint64_t a, b, c, d;
+            // ordered like an ordinary load: rows may be transformed in place
+            asm volatile("ld.global.v4.u64 {%0, %1, %2, %3}, [%4];"
+                         : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+                         : "l"(p + m)
+                         : "memory");
+            x[m] = f_from_u64(a);
+            x[m + 1] = f_from_u64(b);
+            x[m + 2] = f_from_u64(c);
+            x[m + 3] = f_from_u64(d);
+        }
+    } else {
+        const ulonglong2* in = reinterpret_cast<const ulonglong2*>(p);
+#pragma unroll
+        for (int m = 0; m < 16; m += 2) {
+            const ulonglong2 v = in[m / 2];
+            x[m] = f_from_u64(v.x);
+            x[m + 1] = f_from_u64(v.y);
+        }
+    }
+}
+
+// Canonical residues of x[0..15] to p[0..15] (same access widths as load16_u64).
+__device__ __forceinline__ void store16_canonical(uint64_t* p, const double (&x)[16], double q, double qinv,
+                                                  uint64_t qi) {
+    if ((reinterpret_cast<uintptr_t>(p) & 31) == 0) {
+#pragma unroll
+        for (int m = 0; m < 16; m += 4) {
+            const uint64_t a = f_to_canonical(x[m], q, qinv, qi), b = f_to_canonical(x[m + 1], q, qinv, qi);
+            const uint64_t c = f_to_canonical(x[m + 2], q, qinv, qi), d = f_to_canonical(x[m + 3], q, qinv, qi);
+            asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p + m), "l"(a), "l"(b), "l"(c), "l"(d)
+                         : "memory");
+        }
+    } else {
+        ulonglong2* out = reinterpret_cast<ulonglong2*>(p);
+#pragma unroll
+        for (int m = 0; m < 16; m += 2) {
+            ulonglong2 v;
+            v.x = f_to_canonical(x[m], q, qinv, qi);
+            v.y = f_to_canonical(x[m + 1], q, qinv, qi);
+            out[m / 2] = v;
+        }
+    }
+}
 
 // Twiddles of one pass.  In the field at LO, the butterfly of residue m at tile bit
 // b = LO + bb uses index (... + (i >> (b+1))), which depends on m only through
@@ -60,14 +117,23 @@ struct PassTw {
 };
 
 template <int K, int LO, int BHI, int BLO>
-__device__ __forceinline__ void f_fwd_tw(PassTw<LO, BHI, BLO>& T, int t, int hi, int logP, const double2* tw) {
+__device__ __forceinline__ void f_fwd_tw(PassTw<LO, BHI, BLO>& T, int t, int hi, int logP, const FCtx& c) {
 #pragma unroll
     for (int b = BHI; b >= BLO; --b) {
         const int bb = b - LO;
-        const int base = (1 << (logP - 1 - b)) + (hi << (K - b - 1));
+        if constexpr (LO == 0) {
+            // one twiddle per thread and slot: the lane-major copy keeps the warp's loads contiguous
+            const int g = (hi << (K - 4)) + t;
 #pragma unroll
-        for (int h = 0; h < (1 << (3 - bb)); ++h)
-            T.w[PassTw<LO, BHI, BLO>::offset(b) + h] = __ldg(&tw[base + (own<LO>(t, h << (bb + 1)) >> (b + 1))]);
+            for (int h = 0; h < (1 << (3 - bb)); ++h)
+                T.w[PassTw<LO, BHI, BLO>::offset(b) + h] = __ldg(&c.lt[lane_tw_index(g, b, h)]);
+        } else {
+            const int base = (1 << (logP - 1 - b)) + (hi << (K - b - 1));
+#pragma unroll
+            for (int h = 0; h < (1 << (3 - bb)); ++h)
+                T.w[PassTw<LO, BHI, BLO>::offset(b) + h] =
+                    __ldg(&c.tw[base + (own<LO>(t, h << (bb + 1)) >> (b + 1))]);
+        }
     }
 }
 
@@ -93,15 +159,23 @@ __device__ __forceinline__ void f_fwd_bits(double (&x)[16], const PassTw<LO, BHI
 // Inverse stages at bits BLO..BHI of the field at LO.  FINAL: the global last bit folds
 // P^-1 (constants pinv and ilast, centred with their fl(./q) companions).
 template <int K, int LO, int BLO, int BHI, bool FINAL>
-__device__ __forceinline__ void f_inv_tw(PassTw<LO, BLO, BHI>& T, int t, int hi, int logP, const double2* tw) {
+__device__ __forceinline__ void f_inv_tw(PassTw<LO, BLO, BHI>& T, int t, int hi, int logP, const FCtx& c) {
 #pragma unroll
     for (int b = BLO; b <= BHI; ++b) {
         if (FINAL && b == BHI) break;  // the last stage uses the P^-1 constants
         const int bb = b - LO;
-        const int base = ((1 << logP) >> (b + 1)) + (hi << (K - b - 1));
+        if constexpr (LO == 0) {
+            const int g = (hi << (K - 4)) + t;
 #pragma unroll
-        for (int h = 0; h < (1 << (3 - bb)); ++h)
-            T.w[PassTw<LO, BLO, BHI>::offset(b) + h] = __ldg(&tw[base + (own<LO>(t, h << (bb + 1)) >> (b + 1))]);
+            for (int h = 0; h < (1 << (3 - bb)); ++h)
+                T.w[PassTw<LO, BLO, BHI>::offset(b) + h] = __ldg(&c.lt[lane_tw_index(g, b, h)]);
+        } else {
+            const int base = ((1 << logP) >> (b + 1)) + (hi << (K - b - 1));
+#pragma unroll
+            for (int h = 0; h < (1 << (3 - bb)); ++h)
+                T.w[PassTw<LO, BLO, BHI>::offset(b) + h] =
+                    __ldg(&c.tw[base + (own<LO>(t, h << (bb + 1)) >> (b + 1))]);
+        }
     }
 }
 
@@ -187,6 +261,14 @@ struct TileThreads {
     static constexpr int value = (1 << (K - 4)) > 256 ? (1 << (K - 4)) : 256;
 };
 
+// Resident CTAs per SM asked of the compiler for the tile kernels: three 256-thread
+// CTAs (at most 85 registers) measured ~4% faster than the unconstrained 64-register
+// build at 2^16 points; the 512-thread tiles keep their own choice.
+template <int K>
+struct TileMinBlocks {
+    static constexpr int value = TileThreads<K>::value >= 512 ? 1 : 3;
+};
+
 __device__ __forceinline__ double load_in(const uint64_t* p, bool in_double, bool reduce, const FCtx& c) {
     const uint64_t raw = *p;
     if (in_double) return __longlong_as_double((long long)raw);
@@ -266,7 +348,7 @@ __device__ __forceinline__ void issue_group(const RowSet& rows, const PrimeInfo*
 // group computes; otherwise CTA b takes group b, reads its input straight from global
 // memory, and the compiler keeps the lean straight-line register allocation.
 template <int K, bool IN_D, bool PERSIST, bool TABLE>
-__global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __grid_constant__ RowSet rows,
+__global__ void __launch_bounds__(TileThreads<K>::value, TileMinBlocks<K>::value) k_tile_fwd_f(const __grid_constant__ RowSet rows,
                                                                      const PrimeInfo* __restrict__ primes,
                                                                      int tiles_per_cta, int tiles_per_row,
                                                                      long long ngroups) {
@@ -307,6 +389,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
     c.q = pi.qd;
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
+    c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
     const int logP = rows.logP, hi = r.hi;
     double x[16];
 
@@ -317,7 +400,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
     // each pass's twiddles are requested before the exchange that precedes the pass,
     // so their latency overlaps the barrier
     PassTw<L1, K - 1, L1> tw1;
-    f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c.tw);
+    f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c);
     if (PERSIST) {
         const uint64_t* staged = reinterpret_cast<const uint64_t*>(sm);
 #pragma unroll
@@ -329,14 +412,14 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
     }
     f_fwd_bits<K, L1, K - 1, L1>(x, tw1, c);
     PassTw<L2, L1 - 1, L2> tw2;
-    f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c.tw);
+    f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c);
     fput<L1>(sm, x, t);
     __syncthreads();
     fget<L2>(x, sm, t);
     f_fwd_bits<K, L2, L1 - 1, L2>(x, tw2, c);
     if constexpr (L2 > 0) {
         PassTw<L3, L2 - 1, L3> tw3;
-        f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c.tw);
+        f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c);
         __syncthreads();
         fput<L2>(sm, x, t);
         __syncthreads();
@@ -344,7 +427,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
         f_fwd_bits<K, L3, L2 - 1, L3>(x, tw3, c);
         if constexpr (L3 > 0) {
             PassTw<0, L3 - 1, 0> tw4;
-            f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c.tw);
+            f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c);
             __syncthreads();
             fput<L3>(sm, x, t);
             __syncthreads();
@@ -352,14 +435,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
             f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
         }
     }
-    ulonglong2* out = reinterpret_cast<ulonglong2*>(r.dst + 16 * t);
-#pragma unroll
-    for (int m = 0; m < 16; m += 2) {
-        ulonglong2 v;
-        v.x = f_to_canonical(x[m], c.q, c.qinv, pi.q);
-        v.y = f_to_canonical(x[m + 1], c.q, c.qinv, pi.q);
-        out[m / 2] = v;
-    }
+    store16_canonical(r.dst + 16 * t, x, c.q, c.qinv, pi.q);
     if (!PERSIST) break;
     __syncthreads();  // the next trip rewrites shared memory
     }
@@ -368,7 +444,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_fwd_f(const __gr
 // Inverse transform of the low K bits.  FINAL (K == logP): P^-1 folded in, canonical
 // output; otherwise centred doubles are written for the column pass.
 template <int K, bool FINAL, bool PERSIST, bool TABLE>
-__global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __grid_constant__ RowSet rows,
+__global__ void __launch_bounds__(TileThreads<K>::value, TileMinBlocks<K>::value) k_tile_inv_f(const __grid_constant__ RowSet rows,
                                                                      const PrimeInfo* __restrict__ primes,
                                                                      int tiles_per_cta, int tiles_per_row,
                                                                      long long ngroups) {
@@ -408,41 +484,45 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __gr
     c.q = pi.qd;
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.inv_d);
+    c.lt = reinterpret_cast<const double2*>(pi.inv_lane);
     const int logP = rows.logP, hi = r.hi;
     double x[16];
 
     constexpr int F1 = 4 < (K - 4) ? 4 : (K - 4);
     constexpr int F2 = 8 < (K - 4) ? 8 : (K - 4);
     constexpr int F3 = 12 < (K - 4) ? 12 : (K - 4);
-    const ulonglong2* in = reinterpret_cast<const ulonglong2*>(
-        (PERSIST ? reinterpret_cast<const uint64_t*>(sm) : r.src) + 16 * t);
+    if (PERSIST) {
+        const ulonglong2* in = reinterpret_cast<const ulonglong2*>(reinterpret_cast<const uint64_t*>(sm) + 16 * t);
 #pragma unroll
-    for (int m = 0; m < 16; m += 2) {
-        const ulonglong2 v = in[m / 2];
-        x[m] = f_from_u64(v.x);
-        x[m + 1] = f_from_u64(v.y);
+        for (int m = 0; m < 16; m += 2) {
+            const ulonglong2 v = in[m / 2];
+            x[m] = f_from_u64(v.x);
+            x[m + 1] = f_from_u64(v.y);
+        }
+    } else {
+        load16_u64(x, r.src + 16 * t);
     }
     if (PERSIST) __syncthreads();  // every input is in registers before the exchanges reuse the buffer
     PassTw<0, 0, 3> tw1;
-    f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c.tw);
+    f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c);
     f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
     if constexpr (K <= 8) {
         PassTw<F1, 4, K - 1> tw2;
-        f_inv_tw<K, F1, 4, K - 1, FINAL>(tw2, t, hi, logP, c.tw);
+        f_inv_tw<K, F1, 4, K - 1, FINAL>(tw2, t, hi, logP, c);
         fput<0>(sm, x, t);
         __syncthreads();
         fget<F1>(x, sm, t);
         f_inv_bits<K, F1, 4, K - 1, FINAL>(x, tw2, c, pi);
     } else {
         PassTw<F1, 4, 7> tw2;
-        f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c.tw);
+        f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c);
         fput<0>(sm, x, t);
         __syncthreads();
         fget<F1>(x, sm, t);
         f_inv_bits<K, F1, 4, 7, false>(x, tw2, c, pi);
         if constexpr (K <= 12) {
             PassTw<F2, 8, K - 1> tw3;
-            f_inv_tw<K, F2, 8, K - 1, FINAL>(tw3, t, hi, logP, c.tw);
+            f_inv_tw<K, F2, 8, K - 1, FINAL>(tw3, t, hi, logP, c);
             __syncthreads();
             fput<F1>(sm, x, t);
             __syncthreads();
@@ -450,14 +530,14 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_tile_inv_f(const __gr
             f_inv_bits<K, F2, 8, K - 1, FINAL>(x, tw3, c, pi);
         } else {
             PassTw<F2, 8, 11> tw3;
-            f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c.tw);
+            f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c);
             __syncthreads();
             fput<F1>(sm, x, t);
             __syncthreads();
             fget<F2>(x, sm, t);
             f_inv_bits<K, F2, 8, 11, false>(x, tw3, c, pi);
             PassTw<F3, 12, K - 1> tw4;
-            f_inv_tw<K, F3, 12, K - 1, FINAL>(tw4, t, hi, logP, c.tw);
+            f_inv_tw<K, F3, 12, K - 1, FINAL>(tw4, t, hi, logP, c);
             __syncthreads();
             fput<F2>(sm, x, t);
             __syncthreads();
@@ -602,6 +682,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
     c.q = pi.qd;
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
+    c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
     const int logP = rows.logP;
     const bool red = rows.reduce_input != 0;
     // phase 1: this CTA's block, natural order, as residues in doubles
@@ -648,20 +729,20 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
     constexpr int L2 = (K - 8) > 0 ? (K - 8) : 0;
     constexpr int L3 = (K - 12) > 0 ? (K - 12) : 0;
     PassTw<L1, K - 1, L1> tw1;
-    f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c.tw);
+    f_fwd_tw<K, L1, K - 1, L1>(tw1, t, hi, logP, c);
 #pragma unroll
     for (int m = 0; m < 16; ++m) x[m] = fsm[own<L1>(t, m)];
     __syncthreads();  // every value is in registers before the exchanges reuse the buffer
     f_fwd_bits<K, L1, K - 1, L1>(x, tw1, c);
     PassTw<L2, L1 - 1, L2> tw2;
-    f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c.tw);
+    f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c);
     fput<L1>(fsm, x, t);
     __syncthreads();
     fget<L2>(x, fsm, t);
     f_fwd_bits<K, L2, L1 - 1, L2>(x, tw2, c);
     if constexpr (L2 > 0) {
         PassTw<L3, L2 - 1, L3> tw3;
-        f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c.tw);
+        f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c);
         __syncthreads();
         fput<L2>(fsm, x, t);
         __syncthreads();
@@ -669,7 +750,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
         f_fwd_bits<K, L3, L2 - 1, L3>(x, tw3, c);
         if constexpr (L3 > 0) {
             PassTw<0, L3 - 1, 0> tw4;
-            f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c.tw);
+            f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c);
             __syncthreads();
             fput<L3>(fsm, x, t);
             __syncthreads();
@@ -677,14 +758,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
             f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
         }
     }
-    ulonglong2* out = reinterpret_cast<ulonglong2*>(r.dst + 16 * t);
-#pragma unroll
-    for (int m = 0; m < 16; m += 2) {
-        ulonglong2 v;
-        v.x = f_to_canonical(x[m], c.q, c.qinv, pi.q);
-        v.y = f_to_canonical(x[m + 1], c.q, c.qinv, pi.q);
-        out[m / 2] = v;
-    }
+    store16_canonical(r.dst + 16 * t, x, c.q, c.qinv, pi.q);
 }
 
 template <int K, int K1, bool TABLE>
@@ -702,39 +776,34 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_inv_f(const __g
     c.q = pi.qd;
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.inv_d);
+    c.lt = reinterpret_cast<const double2*>(pi.inv_lane);
     const int logP = rows.logP, hi = rank;
     // phase 1: inverse tile passes over the low K bits of this block
     double x[16];
     constexpr int F1 = 4 < (K - 4) ? 4 : (K - 4);
     constexpr int F2 = 8 < (K - 4) ? 8 : (K - 4);
     constexpr int F3 = 12 < (K - 4) ? 12 : (K - 4);
-    const ulonglong2* in = reinterpret_cast<const ulonglong2*>(r.src + 16 * t);
-#pragma unroll
-    for (int m = 0; m < 16; m += 2) {
-        const ulonglong2 v = in[m / 2];
-        x[m] = f_from_u64(v.x);
-        x[m + 1] = f_from_u64(v.y);
-    }
+    load16_u64(x, r.src + 16 * t);
     PassTw<0, 0, 3> tw1;
-    f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c.tw);
+    f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c);
     f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
     if constexpr (K <= 8) {
         PassTw<F1, 4, K - 1> tw2;
-        f_inv_tw<K, F1, 4, K - 1, false>(tw2, t, hi, logP, c.tw);
+        f_inv_tw<K, F1, 4, K - 1, false>(tw2, t, hi, logP, c);
         fput<0>(fsm, x, t);
         __syncthreads();
         fget<F1>(x, fsm, t);
         f_inv_bits<K, F1, 4, K - 1, false>(x, tw2, c, pi);
     } else {
         PassTw<F1, 4, 7> tw2;
-        f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c.tw);
+        f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c);
         fput<0>(fsm, x, t);
         __syncthreads();
         fget<F1>(x, fsm, t);
         f_inv_bits<K, F1, 4, 7, false>(x, tw2, c, pi);
         if constexpr (K <= 12) {
             PassTw<F2, 8, K - 1> tw3;
-            f_inv_tw<K, F2, 8, K - 1, false>(tw3, t, hi, logP, c.tw);
+            f_inv_tw<K, F2, 8, K - 1, false>(tw3, t, hi, logP, c);
             __syncthreads();
             fput<F1>(fsm, x, t);
             __syncthreads();
@@ -742,14 +811,14 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_inv_f(const __g
             f_inv_bits<K, F2, 8, K - 1, false>(x, tw3, c, pi);
         } else {
             PassTw<F2, 8, 11> tw3;
-            f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c.tw);
+            f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c);
             __syncthreads();
             fput<F1>(fsm, x, t);
             __syncthreads();
             fget<F2>(x, fsm, t);
             f_inv_bits<K, F2, 8, 11, false>(x, tw3, c, pi);
             PassTw<F3, 12, K - 1> tw4;
-            f_inv_tw<K, F3, 12, K - 1, false>(tw4, t, hi, logP, c.tw);
+            f_inv_tw<K, F3, 12, K - 1, false>(tw4, t, hi, logP, c);
             __syncthreads();
             fput<F2>(fsm, x, t);
             __syncthreads();

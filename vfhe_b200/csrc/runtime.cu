@@ -294,15 +294,31 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
         inv_d[2 * i] = centred(inv[2 * i]);
         inv_d[2 * i + 1] = inv_d[2 * i] / (double)q;
     }
+    // lane-major copies of the bit 0..3 twiddles (layout described with PrimeInfo)
+    const uint64_t nblk = P / 16, lane_pairs = ((nblk + 31) / 32) * 15 * 32;
+    std::vector<double> fwd_l(2 * lane_pairs, 0.0), inv_l(2 * lane_pairs, 0.0);
+    for (uint64_t g = 0; g < nblk && fp64; ++g)
+        for (int b = 0; b < 4; ++b)
+            for (uint64_t h = 0; h < (1u << (3 - b)); ++h) {
+                const uint64_t src = (P >> (b + 1)) + (g << (3 - b)) + h;
+                const uint64_t dst = (((g >> 5) * 15 + ((1u << (3 - b)) - 1) + h) << 5) + (g & 31);
+                fwd_l[2 * dst] = fwd_d[2 * src];
+                fwd_l[2 * dst + 1] = fwd_d[2 * src + 1];
+                inv_l[2 * dst] = inv_d[2 * src];
+                inv_l[2 * dst + 1] = inv_d[2 * src + 1];
+            }
     void* blk = nullptr;
-    const size_t bytes = sizeof(uint64_t) * 10 * P;
+    const size_t bytes = sizeof(uint64_t) * (10 * P + 4 * lane_pairs);
     if (!check_cuda(cudaMalloc(&blk, bytes), "table alloc")) return false;
     uint64_t* d = (uint64_t*)blk;
     if (!check_cuda(cudaMemcpy(d, fwd.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
         !check_cuda(cudaMemcpy(d + 2 * P, inv.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
         !check_cuda(cudaMemcpy(d + 4 * P, tw.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
         !check_cuda(cudaMemcpy(d + 6 * P, fwd_d.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
-        !check_cuda(cudaMemcpy(d + 8 * P, inv_d.data(), 16 * P, cudaMemcpyHostToDevice), "table upload"))
+        !check_cuda(cudaMemcpy(d + 8 * P, inv_d.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
+        !check_cuda(cudaMemcpy(d + 10 * P, fwd_l.data(), 16 * lane_pairs, cudaMemcpyHostToDevice), "table upload") ||
+        !check_cuda(cudaMemcpy(d + 10 * P + 2 * lane_pairs, inv_l.data(), 16 * lane_pairs, cudaMemcpyHostToDevice),
+                    "table upload"))
         return false;
     t->dev_blocks.push_back(blk);
 
@@ -324,6 +340,8 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
     o.twist = d + 4 * P;
     o.fwd_d = reinterpret_cast<const double*>(d + 6 * P);
     o.inv_d = reinterpret_cast<const double*>(d + 8 * P);
+    o.fwd_lane = reinterpret_cast<const double*>(d + 10 * P);
+    o.inv_lane = reinterpret_cast<const double*>(d + 10 * P + 2 * lane_pairs);
     o.fp64 = fp64 ? 1 : 0;
     o.qd = (double)q;
     o.qinv = 1.0 / (double)q;
