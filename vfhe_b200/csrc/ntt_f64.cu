@@ -152,8 +152,12 @@ __device__ __forceinline__ void f_fwd_bits(double (&x)[16], const PassTw<LO, BHI
             x[m | (1 << bb)] = __dsub_rn(u, v);
         }
     }
+    // The pass at bit 0 is the transform's last and is followed by f_to_canonical, whose
+    // own reduction takes its outputs (|x| < 4q < 2^52) directly.
+    if constexpr (LO != 0) {
 #pragma unroll
-    for (int m = 0; m < 16; ++m) x[m] = f_reduce(x[m], c.q, c.qinv);
+        for (int m = 0; m < 16; ++m) x[m] = f_reduce(x[m], c.q, c.qinv);
+    }
 }
 
 // Inverse stages at bits BLO..BHI of the field at LO.  FINAL: the global last bit folds
@@ -561,8 +565,9 @@ __global__ void __launch_bounds__(TileThreads<K>::value, TileMinBlocks<K>::value
 // owns j = m * 2^KT + c, m < 2^K1.
 // Forward (first pass): canonical/foreign uint64 in, centred doubles out.
 // Inverse (last pass): centred doubles in, canonical uint64 out.
+// Up to radix 16 the kernel fits 64 registers, so four 256-thread CTAs share an SM.
 template <int K1, bool INV>
-__global__ void __launch_bounds__(256) k_col_f(const __grid_constant__ RowSet rows,
+__global__ void __launch_bounds__(256, (K1 >= 5 ? 2 : 4)) k_col_f(const __grid_constant__ RowSet rows,
                                                const PrimeInfo* __restrict__ primes, long long ncols, int KT) {
     constexpr int R = 1 << K1;
     const long long gc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
