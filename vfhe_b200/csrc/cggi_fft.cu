@@ -40,7 +40,10 @@ namespace {
 
 constexpr int kMaxLevels = 4;
 
-// twiddles e^{2 pi i k / M} (k < M/2) and the twist zeta^j (j < M), per N
+// Twiddles per stage and the twist zeta^j (j < M), per N.  The stage whose butterflies
+// span 2^(b+1) points uses e^{2 pi i j / 2^(b+1)}, j < 2^b, stored contiguously at
+// offset 2^b - 1 (M - 1 entries in all), so that the threads of a warp, whose j are
+// consecutive or broadcast, read consecutive entries.
 struct FourierTables {
     int N = 0;
     double2* d_tw = nullptr;
@@ -55,25 +58,37 @@ const FourierTables* fourier_tables(int N) {
     for (auto& t : g_ft)
         if (t.N == N) return &t;
     const int M = N / 2;
-    std::vector<double2> tw(M / 2), twist(M);
+    std::vector<double2> tw(M), twist(M);
     const long double pi = 3.141592653589793238462643383279502884L;
-    for (int k = 0; k < M / 2; ++k) {
-        const long double ang = 2.0L * pi * (long double)k / (long double)M;
-        tw[k] = make_double2((double)cosl(ang), (double)sinl(ang));
-    }
+    tw[M - 1] = make_double2(0.0, 0.0);  // padding
+    for (int b = 0; (1 << b) < M; ++b)
+        for (int j = 0; j < (1 << b); ++j) {
+            const long double ang = 2.0L * pi * (long double)j / (long double)(2 << b);
+            tw[(1 << b) - 1 + j] = make_double2((double)cosl(ang), (double)sinl(ang));
+        }
     for (int j = 0; j < M; ++j) {
         const long double ang = pi * (long double)j / (long double)N;
         twist[j] = make_double2((double)cosl(ang), (double)sinl(ang));
     }
     FourierTables t;
     t.N = N;
-    if (cudaMalloc(&t.d_tw, sizeof(double2) * (M / 2)) != cudaSuccess ||
+    if (cudaMalloc(&t.d_tw, sizeof(double2) * M) != cudaSuccess ||
         cudaMalloc(&t.d_twist, sizeof(double2) * M) != cudaSuccess ||
-        cudaMemcpy(t.d_tw, tw.data(), sizeof(double2) * (M / 2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(t.d_tw, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(t.d_twist, twist.data(), sizeof(double2) * M, cudaMemcpyHostToDevice) != cudaSuccess)
         return nullptr;
     g_ft.push_back(t);
     return &g_ft.back();
+}
+
+// Table loads issued where they stand: ordinary (coherent) loads that neither the
+// compiler nor the assembler moves across the exchange barriers.  Through the read-only
+// path they count as invariant, and every level's key and twiddle loads of a step would
+// be hoisted to its top, keeping well over a hundred values live in registers.
+__device__ __forceinline__ double2 ld_table(const double2* p) {
+    double2 v;
+    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -81,26 +96,6 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
     return make_double2(__fma_rn(a.x, b.x, a.y * b.y), __fma_rn(a.y, b.x, -a.x * b.y));
-}
-
-// Digit `want` of the signed decomposition of v rounded to its top base_log * levels
-// bits (digit 0 most significant), without materialising the others
-__device__ __forceinline__ int digit_of(uint32_t v, int base_log, int levels, int want) {
-    const int total = base_log * levels;
-    uint64_t r = ((uint64_t)v + (1ULL << (31 - total))) >> (32 - total);
-    r &= total >= 32 ? 0xFFFFFFFFULL : ((1ULL << total) - 1);
-    const int half = 1 << (base_log - 1), full = 1 << base_log;
-    int out = 0;
-    for (int l = levels - 1; l >= 0; --l) {
-        int x = (int)(r & (uint64_t)(full - 1));
-        r >>= base_log;
-        if (x >= half) {
-            x -= full;
-            r += 1;
-        }
-        if (l == want) out = x;
-    }
-    return out;
 }
 
 __device__ __forceinline__ int modswitch(uint32_t v, int logN2) {
@@ -148,34 +143,40 @@ struct Passes {
 
 // decimation-in-frequency stages of one pass (kernel e^{+2 pi i / M})
 template <int LOGM, int LO, int NST>
-__device__ __forceinline__ void dif(double2 (&v)[8], int t, const double2* __restrict__ tw) {
+__device__ __forceinline__ void dif(double2 (&v)[8], int t, const double2* tw) {
 #pragma unroll
     for (int s = NST - 1; s >= 0; --s) {
         const int bit = 1 << s;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (k & bit) continue;
-            const int j = pidx<LO>(t, k) & ((1 << (LO + s)) - 1);
-            const double2 w = __ldg(&tw[j << (LOGM - 1 - LO - s)]);
             const double2 u = v[k], x = v[k | bit];
             v[k] = make_double2(u.x + x.x, u.y + x.y);
-            v[k | bit] = cmul(make_double2(u.x - x.x, u.y - x.y), w);
+            if (LO + s == 0) {  // twiddle index 0: the factor is exactly 1
+                v[k | bit] = make_double2(u.x - x.x, u.y - x.y);
+            } else {
+                const int j = pidx<LO>(t, k) & ((1 << (LO + s)) - 1);
+                v[k | bit] = cmul(make_double2(u.x - x.x, u.y - x.y), tw[(1 << (LO + s)) - 1 + j]);
+            }
         }
     }
 }
 
 // decimation-in-time stages of one pass (kernel e^{-2 pi i / M})
 template <int LOGM, int LO, int NST>
-__device__ __forceinline__ void dit(double2 (&v)[8], int t, const double2* __restrict__ tw) {
+__device__ __forceinline__ void dit(double2 (&v)[8], int t, const double2* tw) {
 #pragma unroll
     for (int s = 0; s < NST; ++s) {
         const int bit = 1 << s;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (k & bit) continue;
-            const int j = pidx<LO>(t, k) & ((1 << (LO + s)) - 1);
-            const double2 w = __ldg(&tw[j << (LOGM - 1 - LO - s)]);
-            const double2 u = v[k], x = cmulc(v[k | bit], w);
+            double2 x = v[k | bit];
+            if (LO + s != 0) {  // (twiddle index 0 is exactly 1)
+                const int j = pidx<LO>(t, k) & ((1 << (LO + s)) - 1);
+                x = cmulc(x, tw[(1 << (LO + s)) - 1 + j]);
+            }
+            const double2 u = v[k];
             v[k] = make_double2(u.x + x.x, u.y + x.y);
             v[k | bit] = make_double2(u.x - x.x, u.y - x.y);
         }
@@ -212,203 +213,273 @@ __device__ __forceinline__ void fwd_rest(double2* a, int t, bool active, const d
     }
 }
 
-// inverse passes P down to 1 (pass P+1 left its values at a); pass 0 is done by the caller
-template <int LOGM, int P>
-__device__ __forceinline__ void inv_rest(double2* a, int t, bool active, const double2* tw) {
-    if constexpr (P >= 1) {
-        using Q = PassOf<LOGM, P>;
-        double2 v[8];
-        if (active) {
-            get8<Q::LO>(v, a, t);
-            dit<LOGM, Q::LO, Q::NST>(v, t, tw);
-        }
-        __syncthreads();
-        if (active) put8<Q::LO>(a, v, t);
-        __syncthreads();
-        inv_rest<LOGM, P - 1>(a, t, active, tw);
-    }
+// ---- group-split external product
+//
+// The GLWE of one LWE is handled by two groups of TPA = M/8 threads, group c owning
+// component c: it forms the LEVELS digit polynomials of component c (one after another,
+// each transformed in registers with exchanges through the group's own two shared
+// buffers under a named barrier of TPA threads), and multiplies each spectrum with the
+// GGSW rows (c, level) of both outputs, keeping the two partial sums in registers.  The
+// groups then swap the partial sums of each other's output through shared memory (the
+// only point where they meet) and each runs the inverse transform of output c, adding
+// the rounded result into its own accumulator component.  Every thread works in every
+// phase, and a group never waits for the other group except at the swap.
+
+__device__ __forceinline__ void group_bar(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
-template <int N>
-struct Smem {
-    static constexpr int M = N / 2;
-    // acc[2][N] uint32 | spec[2 L][M] double2 | outs[2][M] double2
-    static constexpr size_t bytes(int levels) {
-        return sizeof(uint32_t) * 2 * N + sizeof(double2) * (2 * levels * M + 2 * M);
-    }
+// Signed gadget digits without a per-digit carry loop: adding B/2 to every base-B
+// digit of the rounded value r (mod B^levels) makes digit l of the sum, minus B/2, the
+// balanced digit in [-B/2, B/2) (the representation is unique, so it equals the
+// carry-propagating decomposition).  Digit 0 is the most significant.
+struct Gadget {
+    int total;       // base_log * levels
+    int base_log;
+    uint32_t mask;   // 2^total - 1
+    uint32_t half;   // sum over digits of B/2 at each digit position
 };
 
-// One external product on the block's GLWE: digits of the source (MODE 0: acc X^ai -
-// acc, from shared acc; MODE 1: the GLWE `src` in global memory), forward transforms,
-// multiply-accumulate with the GGSW spectra `key` (key order), inverse transforms;
-// MODE 0 adds the rounded result into acc, MODE 1 writes it to `dst` and the largest
-// distance of an unrounded coefficient to its integer to *frac.
-template <int LOGM, int LEVELS, int MODE>
-__device__ __forceinline__ void ext_product(uint32_t* acc, double2* spec, double2* outs, const double2* __restrict__ key,
-                                            int ai, int base_log, const uint32_t* __restrict__ src,
-                                            uint32_t* __restrict__ dst, double* frac, const double2* __restrict__ tw,
-                                            const double2* __restrict__ twist) {
-    constexpr int M = 1 << LOGM, N = 2 * M, TPA = M / 8, R = 2 * LEVELS;
-    constexpr int NP = Passes<LOGM>::count;
-    const int arr = threadIdx.x / TPA, t = threadIdx.x - arr * TPA;
-    // forward pass 0 straight from the digits (element j = t + k M/8)
-    {
-        using Q = PassOf<LOGM, 0>;
-        const int c = arr / LEVELS, l = arr - c * LEVELS;
-        double2* a = spec + arr * M;
-        // the folded, twisted digits go to this thread's own pass-0 slots first (one at a
-        // time, to keep register pressure low), then come back as the pass's registers
-#pragma unroll 1
-        for (int k = 0; k < 8; ++k) {
-            const int j = pidx<Q::LO>(t, k);
-            uint32_t lo, hi;
-            if (MODE == 0) {
-                const uint32_t* pc = acc + c * N;
-                lo = rot_at<N>(pc, j, ai) - pc[j];
-                hi = rot_at<N>(pc, j + M, ai) - pc[j + M];
-            } else {
-                lo = src[c * N + j];
-                hi = src[c * N + j + M];
-            }
-            a[swz(j)] = cmul(make_double2((double)digit_of(lo, base_log, LEVELS, l),
-                                          (double)digit_of(hi, base_log, LEVELS, l)),
-                             __ldg(&twist[j]));
-        }
-        double2 v[8];
-        get8<Q::LO>(v, a, t);
-        dif<LOGM, Q::LO, Q::NST>(v, t, tw);
-        put8<Q::LO>(a, v, t);
-    }
-    __syncthreads();
-    fwd_rest<LOGM, 1>(spec + arr * M, t, true, tw);
-    // multiply-accumulate fused into inverse pass NP-1 (threads of the two outputs)
-    const bool inv = threadIdx.x < 2 * TPA;
-    const int oc = inv ? arr : 0;
-    {
-        using Q = PassOf<LOGM, NP - 1>;
-        if (inv) {
-            double2* o = outs + oc * M;
-            // products go to this thread's own slots first (one element at a time)
-#pragma unroll 1
-            for (int k = 0; k < 8; ++k) {
-                const int f = pidx<Q::LO>(t, k);
-                double2 acc2 = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const double2 kv = __ldg(&key[(r * 2 + oc) * M + k * TPA + t]);
-                    const double2 dv = spec[r * M + swz(f)];
-                    acc2.x = __fma_rn(dv.x, kv.x, __fma_rn(-dv.y, kv.y, acc2.x));
-                    acc2.y = __fma_rn(dv.x, kv.y, __fma_rn(dv.y, kv.x, acc2.y));
-                }
-                o[swz(f)] = acc2;
-            }
-            double2 v[8];
-            get8<Q::LO>(v, o, t);
-            dit<LOGM, Q::LO, Q::NST>(v, t, tw);
-            put8<Q::LO>(o, v, t);
-        }
-        __syncthreads();
-    }
-    inv_rest<LOGM, NP - 2>(outs + oc * M, t, inv, tw);
-    // inverse pass 0: untwist, unfold, round (element j = t + k M/8)
-    {
-        using Q = PassOf<LOGM, 0>;
-        double worst = 0.0;
-        if (inv) {
-            double2 v[8];
-            get8<Q::LO>(v, outs + oc * M, t);
-            dit<LOGM, Q::LO, Q::NST>(v, t, tw);
-            const double inv_m = 1.0 / (double)M;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int j = pidx<Q::LO>(t, k);
-                const double2 z = cmulc(v[k], __ldg(&twist[j]));
-                const double re = z.x * inv_m, im = z.y * inv_m;
-                const long long lo = __double2ll_rn(re), hi = __double2ll_rn(im);
-                if (MODE == 0) {
-                    acc[oc * N + j] += (uint32_t)lo;
-                    acc[oc * N + j + M] += (uint32_t)hi;
-                } else {
-                    dst[oc * N + j] = (uint32_t)lo;
-                    dst[oc * N + j + M] = (uint32_t)hi;
-                    worst = fmax(worst, fmax(fabs(re - (double)lo), fabs(im - (double)hi)));
-                }
-            }
-        }
-        if (MODE == 1) {
-            // block maximum through the spectra buffer (no longer needed)
-            double* red = reinterpret_cast<double*>(spec);
-            __syncthreads();
-            red[threadIdx.x] = worst;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double m = 0.0;
-                for (int i = 0; i < (int)blockDim.x; ++i) m = fmax(m, red[i]);
-                *frac = m;
-            }
-        }
-        __syncthreads();
+__host__ __device__ inline Gadget make_gadget(int base_log, int levels) {
+    Gadget g;
+    g.total = base_log * levels;
+    g.base_log = base_log;
+    g.mask = g.total >= 32 ? 0xFFFFFFFFu : ((1u << g.total) - 1u);
+    g.half = 0;
+    for (int l = 0; l < levels; ++l) g.half += 1u << (base_log * l + base_log - 1);
+    return g;
+}
+
+__device__ __forceinline__ uint32_t gadget_prepare(uint32_t v, const Gadget& g) {
+    const uint32_t r = g.total >= 32 ? v : (uint32_t)(((uint64_t)v + (1ULL << (31 - g.total))) >> (32 - g.total));
+    return (r + g.half) & g.mask;
+}
+
+template <int LEVELS>
+__device__ __forceinline__ double gadget_digit(uint32_t prepared, const Gadget& g, int l) {
+    const int sh = g.base_log * (LEVELS - 1 - l);
+    const int d = (int)((prepared >> sh) & ((1u << g.base_log) - 1u)) - (1 << (g.base_log - 1));
+    return (double)d;
+}
+
+// Exchange through buffer `b`: registers in the layout of pass PFROM, out in pass PTO's.
+template <int LOGM, int PFROM, int PTO>
+__device__ __forceinline__ void exchange(double2 (&v)[8], double2* b, int t, int bar) {
+    put8<PassOf<LOGM, PFROM>::LO>(b, v, t);
+    group_bar(bar, (1 << LOGM) / 8);
+    get8<PassOf<LOGM, PTO>::LO>(v, b, t);
+}
+
+// forward passes P .. count-1, registers holding pass P-1's output; exchange e uses buffer e & 1
+template <int LOGM, int P, int E>
+__device__ __forceinline__ void group_fwd(double2 (&v)[8], double2* bufs, int t, int bar, const double2* tw) {
+    if constexpr (P < Passes<LOGM>::count) {
+        exchange<LOGM, P - 1, P>(v, bufs + (E & 1) * (1 << LOGM), t, bar);
+        dif<LOGM, PassOf<LOGM, P>::LO, PassOf<LOGM, P>::NST>(v, t, tw);
+        group_fwd<LOGM, P + 1, E + 1>(v, bufs, t, bar, tw);
     }
 }
 
-// CTAs per SM the register budget is sized for (about 64K / (threads x 2) registers
-// per thread bounds the allocation the compiler may use)
+// inverse passes P down to 0, registers holding pass P+1's output
+template <int LOGM, int P, int E>
+__device__ __forceinline__ void group_inv(double2 (&v)[8], double2* bufs, int t, int bar, const double2* tw) {
+    if constexpr (P >= 0) {
+        exchange<LOGM, P + 1, P>(v, bufs + (E & 1) * (1 << LOGM), t, bar);
+        dit<LOGM, PassOf<LOGM, P>::LO, PassOf<LOGM, P>::NST>(v, t, tw);
+        group_inv<LOGM, P - 1, E + 1>(v, bufs, t, bar, tw);
+    }
+}
+
 template <int LOGM, int LEVELS>
-struct BootMinCtas {
-    static constexpr int threads = 2 * LEVELS * (1 << LOGM) / 8;
-    static constexpr int value = threads >= 512 ? 1 : (threads >= 256 ? 2 : 4);
+struct GroupSplit {
+    static constexpr int M = 1 << LOGM, N = 2 * M, TPA = M / 8, THREADS = 2 * TPA;
+    static constexpr int NP = Passes<LOGM>::count;
+    static constexpr int FWD_EX = LEVELS * (NP - 1);  // exchanges of the forward transforms
+    // acc[2][N] uint32 | bufs[2 groups][2][M] double2 | xbufs[2][M] double2 | twiddles[M]
+    static constexpr size_t smem = sizeof(uint32_t) * 2 * N + sizeof(double2) * 7 * M;
+    // resident blocks the register budget is sized for: about 168 registers a thread
+    static constexpr int min_ctas = 65536 / (THREADS * 168) > 0 ? 65536 / (THREADS * 168) : 1;
 };
+
+// One external product on the block's GLWE, by group c (thread t of TPA).  Source
+// (MODE 0): acc X^ai - acc from the block's accumulator; (MODE 1) the GLWE `src`.
+// Result: MODE 0 adds the rounded output c into acc component c; MODE 1 writes it to
+// dst and returns the largest distance of an unrounded coefficient to its integer.
+// bufs: this group's two exchange buffers; xbufs: the two groups' receive buffers
+// (xbufs + c M collects output c's share from the other group).  The caller has made
+// the accumulator's last writes visible and the receive buffers free (__syncthreads).
+template <int LOGM, int LEVELS, int MODE>
+__device__ __forceinline__ double group_ext_product(uint32_t* acc, double2* bufs, double2* xbufs, int c, int t,
+                                                    const double2* __restrict__ key, int ai, const Gadget& gd,
+                                                    const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                                    const double2* tw, const double2* __restrict__ twist) {
+    using G = GroupSplit<LOGM, LEVELS>;
+    constexpr int M = G::M, N = G::N, TPA = G::TPA, NP = G::NP;
+    // Fresh copies of the thread coordinates: every shared-memory and table address of
+    // the step derives from them, and without this the compiler hoists all of those
+    // addresses out of the caller's step loop and keeps them live in registers.
+    asm volatile("mov.b32 %0, %0;" : "+r"(t));
+    asm volatile("mov.b32 %0, %0;" : "+r"(c));
+    const int bar = 1 + c;
+    // rounded, digit-prepared source coefficients j and j + M (j = k TPA + t: pass-0 layout)
+    uint32_t plo[8], phi[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int j = k * TPA + t;
+        uint32_t lo, hi;
+        if (MODE == 0) {
+            const uint32_t* pc = acc + c * N;
+            lo = rot_at<N>(pc, j, ai) - pc[j];
+            hi = rot_at<N>(pc, j + M, ai) - pc[j + M];
+        } else {
+            lo = src[c * N + j];
+            hi = src[c * N + j + M];
+        }
+        plo[k] = gadget_prepare(lo, gd);
+        phi[k] = gadget_prepare(hi, gd);
+    }
+    // output c's partial sum stays in registers; output 1 - c's goes straight into the
+    // other group's receive buffer (same positions for every level, so no races)
+    double2 pm[8];
+    double2* give = xbufs + (1 - c) * M;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pm[k] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < LEVELS; ++l) {
+        double2 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            v[k] = cmul(make_double2(gadget_digit<LEVELS>(plo[k], gd, l), gadget_digit<LEVELS>(phi[k], gd, l)),
+                        ld_table(&twist[k * TPA + t]));
+        dif<LOGM, PassOf<LOGM, 0>::LO, PassOf<LOGM, 0>::NST>(v, t, tw);
+        if (l == 0) group_fwd<LOGM, 1, 0>(v, bufs, t, bar, tw);
+        else if (l == 1) group_fwd<LOGM, 1, (NP - 1)>(v, bufs, t, bar, tw);
+        else if (l == 2) group_fwd<LOGM, 1, 2 * (NP - 1)>(v, bufs, t, bar, tw);
+        else group_fwd<LOGM, 1, 3 * (NP - 1)>(v, bufs, t, bar, tw);
+        // spectrum element 8 t + k meets key position k TPA + t (key order)
+        const double2* km = key + (long long)((c * LEVELS + l) * 2 + c) * M;
+        const double2* ko = key + (long long)((c * LEVELS + l) * 2 + (1 - c)) * M;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double2 ka = ld_table(&km[k * TPA + t]);
+            pm[k].x = __fma_rn(v[k].x, ka.x, __fma_rn(-v[k].y, ka.y, pm[k].x));
+            pm[k].y = __fma_rn(v[k].x, ka.y, __fma_rn(v[k].y, ka.x, pm[k].y));
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double2 kb = ld_table(&ko[k * TPA + t]);
+            double2* g = give + swz(pidx<0>(t, k));
+            const double2 o = l == 0 ? make_double2(0.0, 0.0) : *g;
+            *g = make_double2(__fma_rn(v[k].x, kb.x, __fma_rn(-v[k].y, kb.y, o.x)),
+                              __fma_rn(v[k].x, kb.y, __fma_rn(v[k].y, kb.x, o.y)));
+        }
+    }
+    __syncthreads();  // both groups' contributions to each other's output are in place
+    double2 v[8];
+    {
+        const double2* mine = xbufs + c * M;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double2 other = mine[swz(pidx<0>(t, k))];
+            v[k] = make_double2(pm[k].x + other.x, pm[k].y + other.y);
+        }
+    }
+    dit<LOGM, PassOf<LOGM, NP - 1>::LO, PassOf<LOGM, NP - 1>::NST>(v, t, tw);
+    group_inv<LOGM, NP - 2, G::FWD_EX>(v, bufs, t, bar, tw);
+    // untwist, unfold, round (element j = k TPA + t)
+    const double inv_m = 1.0 / (double)M;
+    double worst = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int j = k * TPA + t;
+        const double2 z = cmulc(v[k], __ldg(&twist[j]));
+        const double re = z.x * inv_m, im = z.y * inv_m;
+        const long long lo = __double2ll_rn(re), hi = __double2ll_rn(im);
+        if (MODE == 0) {
+            acc[c * N + j] += (uint32_t)lo;
+            acc[c * N + j + M] += (uint32_t)hi;
+        } else {
+            dst[c * N + j] = (uint32_t)lo;
+            dst[c * N + j + M] = (uint32_t)hi;
+            worst = fmax(worst, fmax(fabs(re - (double)lo), fabs(im - (double)hi)));
+        }
+    }
+    return worst;
+}
 
 // Blind rotation + sample extraction of B LWEs (in: [B][n+1], mask then body) into
 // out [B][N+1] (extracted mask, body).  bsk_f: [n][2 levels][2][M] spectra in key order.
-// Block: 2 levels x M/8 threads; persistent over the LWEs.
+// Block: two groups of M/8 threads (one per GLWE component); persistent over the LWEs.
 template <int LOGM, int LEVELS>
-__global__ void __launch_bounds__(2 * LEVELS * (1 << LOGM) / 8, BootMinCtas<LOGM, LEVELS>::value) k_cggi_fft_bootstrap(
-    uint32_t* __restrict__ out, const uint32_t* __restrict__ in, long long B, const double2* __restrict__ bsk_f,
-    const uint32_t* __restrict__ tv, int n, int base_log, uint32_t offset, const double2* __restrict__ g_tw,
-    const double2* __restrict__ g_twist) {
-    constexpr int M = 1 << LOGM, N = 2 * M, R = 2 * LEVELS;
+__global__ void __launch_bounds__(GroupSplit<LOGM, LEVELS>::THREADS, GroupSplit<LOGM, LEVELS>::min_ctas)
+    k_cggi_fft_bootstrap(uint32_t* __restrict__ out, const uint32_t* __restrict__ in, long long B,
+                         const double2* __restrict__ bsk_f, const uint32_t* __restrict__ tv, int n, Gadget gd,
+                         uint32_t offset, const double2* __restrict__ g_tw, const double2* __restrict__ g_twist) {
+    using G = GroupSplit<LOGM, LEVELS>;
+    constexpr int M = G::M, N = G::N, TPA = G::TPA, R = 2 * LEVELS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
-    double2* spec = reinterpret_cast<double2*>(acc + 2 * N);
-    double2* outs = spec + R * M;
+    double2* bufs_all = reinterpret_cast<double2*>(acc + 2 * N);
+    const int c = threadIdx.x / TPA, t = threadIdx.x - c * TPA;
+    double2* bufs = bufs_all + c * 2 * M;
+    double2* xbufs = bufs_all + 4 * M;
+    // the transforms' per-stage twiddles, read from shared memory (a warp's lookups are
+    // consecutive or broadcast entries: one wavefront, against up to 16 L1 sectors)
+    double2* stw = bufs_all + 6 * M;
+    for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = g_tw[k];
+    __syncthreads();
     constexpr int logN2 = LOGM + 2;
     for (long long lwe = blockIdx.x; lwe < B; lwe += gridDim.x) {
         const uint32_t* a = in + lwe * (long long)(n + 1);
         const int rb = modswitch(a[n] + offset, logN2);
         const int e0 = (2 * N - rb) & (2 * N - 1);
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            acc[k] = 0;
-            acc[N + k] = rot_at<N>(tv, k, e0);
-        }
-        __syncthreads();
+        for (int k = t; k < N; k += TPA) acc[c * N + k] = c == 0 ? 0u : rot_at<N>(tv, k, e0);
         for (int i = 0; i < n; ++i) {
+            // accumulator writes visible; last step's receive-buffer reads done
+            __syncthreads();
             const int ai = modswitch(__ldg(a + i), logN2);
-            ext_product<LOGM, LEVELS, 0>(acc, spec, outs, bsk_f + (long long)i * R * 2 * M, ai, base_log, nullptr,
-                                         nullptr, nullptr, g_tw, g_twist);
+            group_ext_product<LOGM, LEVELS, 0>(acc, bufs, xbufs, c, t, bsk_f + (long long)i * R * 2 * M, ai, gd,
+                                               nullptr, nullptr, stw, g_twist);
         }
+        group_bar(1 + c, TPA);
         uint32_t* o = out + lwe * (long long)(N + 1);
-        for (int k = threadIdx.x; k < N; k += blockDim.x) o[k] = k == 0 ? acc[0] : (uint32_t)(0u - acc[N - k]);
-        if (threadIdx.x == 0) o[N] = acc[N];
-        __syncthreads();
+        if (c == 0) {
+            for (int k = t; k < N; k += TPA) o[k] = k == 0 ? acc[0] : (uint32_t)(0u - acc[N - k]);
+        } else if (t == 0) {
+            o[N] = acc[N];
+        }
+        group_bar(1 + c, TPA);  // extraction reads done before the next LWE rewrites acc
     }
 }
 
 // out[B][2N] = ExtProd(ggsw_f, c[B][2N]) rounded; frac[b] = largest distance of an
 // unrounded coefficient to its integer.  Same code path as a blind-rotation step.
 template <int LOGM, int LEVELS>
-__global__ void __launch_bounds__(2 * LEVELS * (1 << LOGM) / 8) k_cggi_fft_extprod(
-    uint32_t* __restrict__ out, const uint32_t* __restrict__ c, const double2* __restrict__ ggsw_f, int base_log,
+__global__ void __launch_bounds__(GroupSplit<LOGM, LEVELS>::THREADS) k_cggi_fft_extprod(
+    uint32_t* __restrict__ out, const uint32_t* __restrict__ c_in, const double2* __restrict__ ggsw_f, Gadget gd,
     const double2* __restrict__ g_tw, const double2* __restrict__ g_twist, double* __restrict__ frac) {
-    constexpr int M = 1 << LOGM, N = 2 * M, R = 2 * LEVELS;
+    using G = GroupSplit<LOGM, LEVELS>;
+    constexpr int M = G::M, N = G::N, TPA = G::TPA;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
-    double2* spec = reinterpret_cast<double2*>(acc + 2 * N);
-    double2* outs = spec + R * M;
-    double dummy;
-    ext_product<LOGM, LEVELS, 1>(acc, spec, outs, ggsw_f, 0, base_log, c + (long long)blockIdx.x * 2 * N,
-                                 out + (long long)blockIdx.x * 2 * N, frac ? frac + blockIdx.x : &dummy, g_tw,
-                                 g_twist);
+    double2* bufs_all = reinterpret_cast<double2*>(acc + 2 * N);
+    const int c = threadIdx.x / TPA, t = threadIdx.x - c * TPA;
+    double2* stw = bufs_all + 6 * M;
+    for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = g_tw[k];
+    __syncthreads();
+    const double worst = group_ext_product<LOGM, LEVELS, 1>(
+        acc, bufs_all + c * 2 * M, bufs_all + 4 * M, c, t, ggsw_f, 0, gd,
+        c_in + (long long)blockIdx.x * 2 * N, out + (long long)blockIdx.x * 2 * N, stw, g_twist);
+    // block maximum through the exchange buffers (no longer needed)
+    double* red = reinterpret_cast<double*>(bufs_all);
+    __syncthreads();
+    red[threadIdx.x] = worst;
+    __syncthreads();
+    if (threadIdx.x == 0 && frac) {
+        double m = 0.0;
+        for (int i = 0; i < (int)blockDim.x; ++i) m = fmax(m, red[i]);
+        frac[blockIdx.x] = m;
+    }
 }
 
 // Spectra of rows of N signed 32-bit coefficients (torus values read as int32), in key
@@ -516,18 +587,18 @@ bool check_shape(int N, int levels, int base_log, const char* where) {
 template <int LOGM, int LEVELS>
 int launch_bootstrap_t(uint32_t* out, const uint32_t* in, long long B, const double2* bsk_f, const uint32_t* tv,
                        int n, int base_log, uint32_t offset, const FourierTables* ft, cudaStream_t st) {
-    constexpr int THREADS = 2 * LEVELS * (1 << LOGM) / 8;
-    const size_t smem = Smem<(2 << LOGM)>::bytes(LEVELS);
+    using G = GroupSplit<LOGM, LEVELS>;
     int e = (int)cudaFuncSetAttribute(k_cggi_fft_bootstrap<LOGM, LEVELS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem);
+                                      (int)G::smem);
     if (e) return e;
     int per_sm = 0;
-    e = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cggi_fft_bootstrap<LOGM, LEVELS>, THREADS, smem);
+    e = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cggi_fft_bootstrap<LOGM, LEVELS>, G::THREADS,
+                                                           G::smem);
     if (e) return e;
     long long grid = (long long)(per_sm > 0 ? per_sm : 1) * sm_count();
     if (grid > B) grid = B;
-    k_cggi_fft_bootstrap<LOGM, LEVELS><<<(unsigned)grid, THREADS, smem, st>>>(out, in, B, bsk_f, tv, n, base_log, offset,
-                                                                            ft->d_tw, ft->d_twist);
+    k_cggi_fft_bootstrap<LOGM, LEVELS><<<(unsigned)grid, G::THREADS, G::smem, st>>>(
+        out, in, B, bsk_f, tv, n, make_gadget(base_log, LEVELS), offset, ft->d_tw, ft->d_twist);
     note_launch();
     return (int)cudaGetLastError();
 }
@@ -535,13 +606,12 @@ int launch_bootstrap_t(uint32_t* out, const uint32_t* in, long long B, const dou
 template <int LOGM, int LEVELS>
 int launch_extprod_t(uint32_t* out, const uint32_t* c, long long B, const double2* ggsw_f, int base_log,
                      const FourierTables* ft, double* frac, cudaStream_t st) {
-    constexpr int THREADS = 2 * LEVELS * (1 << LOGM) / 8;
-    const size_t smem = Smem<(2 << LOGM)>::bytes(LEVELS);
+    using G = GroupSplit<LOGM, LEVELS>;
     int e = (int)cudaFuncSetAttribute(k_cggi_fft_extprod<LOGM, LEVELS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem);
+                                      (int)G::smem);
     if (e) return e;
-    k_cggi_fft_extprod<LOGM, LEVELS><<<(unsigned)B, THREADS, smem, st>>>(out, c, ggsw_f, base_log, ft->d_tw,
-                                                                       ft->d_twist, frac);
+    k_cggi_fft_extprod<LOGM, LEVELS><<<(unsigned)B, G::THREADS, G::smem, st>>>(
+        out, c, ggsw_f, make_gadget(base_log, LEVELS), ft->d_tw, ft->d_twist, frac);
     note_launch();
     return (int)cudaGetLastError();
 }
