@@ -642,25 +642,32 @@ def run_cuda_arm(args) -> None:
     # 64 polynomials (805 MB, larger than L2, so every transform streams from HBM)
     from vfhe_b200.arith import Ring
 
-    R16 = Ring(2**16, prime_size=[50] * 24, split_degree=1, engine=eng)
-    b16 = torch.empty((NTT16_POLYS, 24, 2**16), dtype=torch.int64, device="cuda")
-    for k, q in enumerate(R16.primes):
-        b16[:, k].random_(0, q)
-    l16 = ffi.new("uint32_t[]", R16.prime_indices)
-    p16 = ffi.cast("uint64_t*", b16.data_ptr())
-    for _ in range(3):
-        eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, NTT16_POLYS, l16, 24, sp)
-    torch.cuda.synchronize()
-    profile_range(None, "ntt16", True)
-    ev0.record(stream)
-    for _ in range(reps):
-        eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, NTT16_POLYS, l16, 24, sp)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    profile_range(None, "ntt16", False)
-    ms16 = ev0.elapsed_time(ev1) / reps
-    limbs16 = NTT16_POLYS * 24 / (ms16 * 1e-3)
-    del b16
+    def ntt16_rate(split: int, profile: bool) -> tuple[float, float]:
+        R16 = Ring(2**16, prime_size=[50] * 24, split_degree=split, engine=eng)
+        b16 = torch.empty((NTT16_POLYS, 24, 2**16), dtype=torch.int64, device="cuda")
+        for k, q in enumerate(R16.primes):
+            b16[:, k].random_(0, q)
+        l16 = ffi.new("uint32_t[]", R16.prime_indices)
+        p16 = ffi.cast("uint64_t*", b16.data_ptr())
+        for _ in range(3):
+            eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, NTT16_POLYS, l16, 24, sp)
+        torch.cuda.synchronize()
+        if profile:
+            profile_range(None, "ntt16", True)
+        ev0.record(stream)
+        for _ in range(reps):
+            eng.lib.vfhe_cuda_ntt_batch(R16.NTT, 0, p16, p16, NTT16_POLYS, l16, 24, sp)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if profile:
+            profile_range(None, "ntt16", False)
+        ms = ev0.elapsed_time(ev1) / reps
+        del b16
+        return ms, NTT16_POLYS * 24 / (ms * 1e-3)
+
+    ms16, limbs16 = ntt16_rate(1, True)
+    # the reference's default split for 50-bit primes: four 2^14-point blocks per limb
+    ms16s4, limbs16s4 = ntt16_rate(4, False)
     eng.check("bench")
 
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
@@ -713,6 +720,8 @@ def run_cuda_arm(args) -> None:
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "decoded_max_error": err,
+        "ntt_2p16_L24_split4": {"limbs_per_s": limbs16s4, "polys": NTT16_POLYS, "ms_per_launch": ms16s4,
+                                "frac_hbm": 16 * 2**16 * limbs16s4 / 1e9 / peak},
         "ntt_2p16_L24": {"limbs_per_s": limbs16, "polys": NTT16_POLYS, "ms_per_launch": ms16,
                          "frac_hbm": 16 * 2**16 * limbs16 / 1e9 / peak},
     }

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "abi_common.cuh"
@@ -84,12 +85,16 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
 // (*) the ring's incomplete product, pointwise at split 1)
 // D: [B][nd][ne][N]; K_b: [digits][2][ne][N] (only the first nd digits are used);
 // acc: [B][2][ne][N].  Thread index over N = (block o, slot x).
+// order (may be null): ciphertext processed by the by-th group of rows, so that the
+// ciphertexts sharing a key run back to back and the key stays in L2 between them.
 template <int S>
 __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
-                      const uint64_t* const* __restrict__ keys, const __grid_constant__ LimbPrimes lp,
-                      const PrimeInfo* __restrict__ primes, int nd, int ne, long long N) {
+                      const uint64_t* const* __restrict__ keys, const uint64_t* __restrict__ order,
+                      const __grid_constant__ LimbPrimes lp, const PrimeInfo* __restrict__ primes, int nd, int ne,
+                      long long N) {
     const int by = blockIdx.y;
-    const int b = by / ne, i = by - b * ne;
+    const int bo = by / ne, i = by - bo * ne;
+    const int b = order ? (int)order[bo] : bo;
     const PrimeInfo pi = primes[lp.p[i]];
     const uint64_t* key = keys[b];
     const long long dstride = (long long)ne * N;       // between digits of D
@@ -99,6 +104,45 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
     const uint64_t* kb = ka + dstride;
     uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
     uint64_t* ob = oa + dstride;
+    if (S == 1 && pi.fp64 &&
+        (((reinterpret_cast<uintptr_t>(d) | reinterpret_cast<uintptr_t>(ka) | reinterpret_cast<uintptr_t>(oa)) & 15) ==
+         0)) {
+        // pointwise products, two residues per thread (16-byte accesses: the kernel streams
+        // the digits from HBM), partial sums reduced every four digits
+        const double q = pi.qd, qinv = pi.qinv;
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
+#pragma unroll 2
+            for (int j = 0; j < nd; ++j) {
+                // digits are read once: streaming loads leave L2 to the keys
+                const ulonglong2 dv = __ldcs(reinterpret_cast<const ulonglong2*>(d + j * dstride + x));
+                const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(ka + j * kstride + x);
+                const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(kb + j * kstride + x);
+                const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
+                const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
+                const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
+                sa0 = __dadd_rn(sa0, f_mulmod(v0, wa0, __dmul_rn(wa0, qinv), q));
+                sa1 = __dadd_rn(sa1, f_mulmod(v1, wa1, __dmul_rn(wa1, qinv), q));
+                sb0 = __dadd_rn(sb0, f_mulmod(v0, wb0, __dmul_rn(wb0, qinv), q));
+                sb1 = __dadd_rn(sb1, f_mulmod(v1, wb1, __dmul_rn(wb1, qinv), q));
+                if ((j & 3) == 3) {
+                    sa0 = f_reduce(sa0, q, qinv);
+                    sa1 = f_reduce(sa1, q, qinv);
+                    sb0 = f_reduce(sb0, q, qinv);
+                    sb1 = f_reduce(sb1, q, qinv);
+                }
+            }
+            ulonglong2 ra, rb;
+            ra.x = f_to_canonical(-sa0, q, qinv, pi.q);
+            ra.y = f_to_canonical(-sa1, q, qinv, pi.q);
+            rb.x = f_to_canonical(-sb0, q, qinv, pi.q);
+            rb.y = f_to_canonical(-sb1, q, qinv, pi.q);
+            *reinterpret_cast<ulonglong2*>(oa + x) = ra;
+            *reinterpret_cast<ulonglong2*>(ob + x) = rb;
+        }
+        return;
+    }
     if (S == 1 && pi.fp64) {
         // pointwise products: the streaming loop, partial sums reduced every four digits
         const double q = pi.qd, qinv = pi.qinv;
@@ -183,10 +227,13 @@ __global__ void k_moddown(uint64_t* __restrict__ out, const uint64_t* __restrict
             if (ps) v = add_mod(v, ps[(long long)i * N + x], pi.q);
             return v;
         };
+        // unrolled so that several limbs' loads are in flight at once
         if (!rescale) {
+#pragma unroll 4
             for (int i = 0; i < nl; ++i) o[(long long)i * N + x] = limb(i);
         } else {
             const uint64_t t2 = add_mod(limb(nl - 1), mc.half_top, mc.q_top);
+#pragma unroll 4
             for (int i = 0; i < nl - 1; ++i) {
                 const PrimeInfo& pi = primes[mc.prime[i]];
                 uint64_t v = add_mod(limb(i), mc.half_r[i], pi.q);
@@ -224,8 +271,8 @@ __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __re
 
 // One k_mac launch for the ring's split degree (each split degree is its own kernel,
 // so the pointwise one keeps its small register footprint).
-void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const LimbPrimes& lpe,
-                int nd, int ne, long long N, uint64_t B, cudaStream_t st);
+void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
+                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st);
 
 // Grid for one launch of a per-coefficient kernel; every call site launches exactly
 // one kernel with it, so it also counts the launch.
@@ -237,15 +284,16 @@ dim3 grid_xy(long long n, long long y) {
     return dim3((unsigned)blocks, (unsigned)y, 1);
 }
 
-void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const LimbPrimes& lpe,
-                int nd, int ne, long long N, uint64_t B, cudaStream_t st) {
-    const dim3 g = grid_xy(N, (long long)B * ne);
+void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
+                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st) {
+    // the pointwise kernel handles two residues per thread
+    const dim3 g = grid_xy(t->pub.split_degree == 1 ? (N + 1) / 2 : N, (long long)B * ne);
     switch (t->pub.split_degree) {
-        case 1: k_mac<1><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
-        case 2: k_mac<2><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
-        case 4: k_mac<4><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
-        case 8: k_mac<8><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
-        default: k_mac<16><<<g, 256, 0, st>>>(acc, D, keys, lpe, t->d_info, nd, ne, N); break;
+        case 1: k_mac<1><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
+        case 2: k_mac<2><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
+        case 4: k_mac<4><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
+        case 8: k_mac<8><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
+        default: k_mac<16><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
     }
 }
 
@@ -347,7 +395,7 @@ uint64_t ckks_mul_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
 
 uint64_t ckks_rot_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
     const uint64_t ne = L + 1;
-    return B * N * (2 * L + L * ne + 2 * ne) + 2 * B + 64;
+    return B * N * (2 * L + L * ne + 2 * ne) + 3 * B + 64;
 }
 
 int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const uint64_t* ct2, uint64_t B,
@@ -387,7 +435,7 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
     if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, lpe, nl, ne, N, B, st);
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
@@ -426,7 +474,17 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     uint64_t* acc = D + B * (uint64_t)nl * ne * N;      // [B][2][ne][N]
     uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
     uint64_t* d_gens = keyptrs + B;                     // [B]
+    uint64_t* d_order = d_gens + B;                     // [B]
     if (!check_cuda(upload_small(keyptrs, (const uint64_t*)gks, B, st), where)) return 1;
+    // ciphertexts grouped by key (stable), so each key is read from HBM about once
+    std::vector<uint64_t> order(B);
+    for (uint64_t b = 0; b < B; ++b) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [gks](uint64_t x, uint64_t y) {
+        return reinterpret_cast<uintptr_t>(gks[x]) < reinterpret_cast<uintptr_t>(gks[y]);
+    });
+    bool identity = true;
+    for (uint64_t b = 0; b < B && identity; ++b) identity = order[b] == b;
+    if (!identity && !check_cuda(upload_small(d_order, order.data(), B, st), where)) return 1;
     const uint64_t* src = ct;
     if (gens) {
         if (!check_cuda(upload_small(d_gens, gens, B, st), where)) return 1;
@@ -435,7 +493,7 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
         src = Pm;
     }
     if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, lpe, nl, ne, N, B, st);
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
