@@ -34,6 +34,9 @@ N_DEG = 2**14
 PRIME_SIZES = [50] + [40] * 8 + [50]
 PAIRS = 256
 NTT16_POLYS = 64  # polynomials per N = 2^16, L = 24 transform launch
+# DRAM bytes (read + write) of one digit-transform launch, per schedule, from an ncu
+# capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum over its kernels)
+MEASURED_TRAFFIC = {"k_col_f<4,0> + k_tile_fwd_f<10,1>": 1230588672}
 STEPS_SET = [1 << i for i in range(13)]
 SCALE = 2.0**40
 SEED = 20261203
@@ -627,12 +630,23 @@ def run_cuda_arm(args) -> None:
         eng.lib.vfhe_cuda_ntt_batch(s.special_rings[0].NTT, 0, ptr, ptr, PAIRS, limbs, ne, sp)
     torch.cuda.synchronize()
     reps = 20
+    profile_range(None, "digits", True)
     ev0.record(stream)
     for _ in range(reps):
         eng.lib.vfhe_cuda_ntt_batch(s.special_rings[0].NTT, 0, ptr, ptr, PAIRS, limbs, ne, sp)
     ev1.record(stream)
     torch.cuda.synchronize()
+    profile_range(None, "digits", False)
     ntt_ms = ev0.elapsed_time(ev1) / reps
+    sched = ffi.new("int32_t[3]")
+    eng.lib.vfhe_cuda_ntt_get_schedule(14, PAIRS * ne, sched)
+    kt = sched[0] or 12
+    if kt >= 14:
+        kname = f"k_tile_fwd_f<{kt},0>"
+    elif sched[2] == -1:
+        kname = f"k_fused_fwd_f<{kt},{14 - kt}> (thread-block cluster)"
+    else:
+        kname = f"k_col_f<{14 - kt},0> + k_tile_fwd_f<{kt},1>"
     alg_bytes = PAIRS * ne * 16 * N_DEG
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ntt_ms * 1e-3) / 1e9
@@ -713,9 +727,9 @@ def run_cuda_arm(args) -> None:
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
                 "d2h_bytes_per_step": int(hout[0].numel() * 8), "ms_per_step": e2e_ms,
                 "pipelining": "copy-in, compute and copy-out of consecutive steps overlap (two buffer sets)"},
-        "roofline": {"bound": "hbm", "kernel": "forward FP64 NTT, k_col_f<2,0> + k_tile_fwd_f<12,1> (digit transforms, 2560 rows x 2^14)",
+        "roofline": {"bound": "hbm", "kernel": f"forward FP64 NTT, {kname} (digit transforms, {PAIRS * ne} rows x 2^14)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": None, "launch_ms": ntt_ms,
+                     "peak_source": peak_kind, "traffic": MEASURED_TRAFFIC.get(kname), "launch_ms": ntt_ms,
                      "algorithmic_bytes": alg_bytes},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
@@ -757,7 +771,7 @@ def main() -> None:
     ap.add_argument("--cggi-million", action="store_true",
                     help="also bootstrap 10^6 LWEs and count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
-    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "ntt16", "cggi_fft", "cggi_rns", "worklist"],
+    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()
     global PROFILE_LEG

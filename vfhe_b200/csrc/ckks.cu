@@ -215,6 +215,54 @@ __global__ void k_moddown(uint64_t* __restrict__ out, const uint64_t* __restrict
     const int use_pass = c == 0 ? use_pass_a : use_pass_b;
     const uint64_t* ps = use_pass ? pass + (long long)b * pass_stride + (c == 0 ? pass_off_a : pass_off_b) : nullptr;
     const PrimeInfo psp = primes[mc.special];
+    if (((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(o) |
+          reinterpret_cast<uintptr_t>(ps ? ps : a)) & 15) == 0) {
+        // two coefficients per thread with 16-byte accesses; acc and the pass-through
+        // rows are read once (streaming loads)
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            const ulonglong2 sp = __ldcs(reinterpret_cast<const ulonglong2*>(a + (long long)nl * N + x));
+            const uint64_t t0 = add_mod(sp.x, mc.half_p, mc.p), t1 = add_mod(sp.y, mc.half_p, mc.p);
+            auto limb2 = [&](int i, unsigned long long& v0, unsigned long long& v1) {
+                const PrimeInfo& pi = primes[mc.prime[i]];
+                const ulonglong2 av = __ldcs(reinterpret_cast<const ulonglong2*>(a + (long long)i * N + x));
+                v0 = shoup(sub_mod(add_mod(av.x, mc.half_sp[i], pi.q), reduce64(t0, pi), pi.q), mc.inv_sp[i],
+                           mc.inv_sp_sh[i], pi.q);
+                v1 = shoup(sub_mod(add_mod(av.y, mc.half_sp[i], pi.q), reduce64(t1, pi), pi.q), mc.inv_sp[i],
+                           mc.inv_sp_sh[i], pi.q);
+                if (ps) {
+                    const ulonglong2 pv = __ldcs(reinterpret_cast<const ulonglong2*>(ps + (long long)i * N + x));
+                    v0 = add_mod(v0, pv.x, pi.q);
+                    v1 = add_mod(v1, pv.y, pi.q);
+                }
+            };
+            if (!rescale) {
+#pragma unroll 2
+                for (int i = 0; i < nl; ++i) {
+                    ulonglong2 r;
+                    limb2(i, r.x, r.y);
+                    *reinterpret_cast<ulonglong2*>(o + (long long)i * N + x) = r;
+                }
+            } else {
+                unsigned long long u0, u1;
+                limb2(nl - 1, u0, u1);
+                const uint64_t s0 = add_mod(u0, mc.half_top, mc.q_top), s1 = add_mod(u1, mc.half_top, mc.q_top);
+#pragma unroll 2
+                for (int i = 0; i < nl - 1; ++i) {
+                    const PrimeInfo& pi = primes[mc.prime[i]];
+                    unsigned long long v0, v1;
+                    limb2(i, v0, v1);
+                    ulonglong2 r;
+                    r.x = shoup(sub_mod(add_mod(v0, mc.half_r[i], pi.q), reduce64(s0, pi), pi.q), mc.inv_r[i],
+                                mc.inv_r_sh[i], pi.q);
+                    r.y = shoup(sub_mod(add_mod(v1, mc.half_r[i], pi.q), reduce64(s1, pi), pi.q), mc.inv_r[i],
+                                mc.inv_r_sh[i], pi.q);
+                    *reinterpret_cast<ulonglong2*>(o + (long long)i * N + x) = r;
+                }
+            }
+        }
+        return;
+    }
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
          x += (long long)gridDim.x * blockDim.x) {
         const uint64_t t = add_mod(a[(long long)nl * N + x], mc.half_p, mc.p);
@@ -439,7 +487,7 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
-    k_moddown<<<grid_xy(N, (long long)B * 2), 256, 0, st>>>(out, acc, T, 3LL * nl * N, (long long)nl * N,
+    k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, T, 3LL * nl * N, (long long)nl * N,
                                                             2LL * nl * N, 1, 1, mc, t->d_info, nl, 1, N);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
@@ -497,7 +545,7 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
-    k_moddown<<<grid_xy(N, (long long)B * 2), 256, 0, st>>>(out, acc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
+    k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
                                                             mc, t->d_info, nl, 0, N);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
