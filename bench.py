@@ -34,9 +34,9 @@ N_DEG = 2**14
 PRIME_SIZES = [50] + [40] * 8 + [50]
 PAIRS = 256
 NTT16_POLYS = 64  # polynomials per N = 2^16, L = 24 transform launch
-# DRAM bytes (read + write) of one digit-transform launch, per schedule, from an ncu
-# capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum over its kernels)
-MEASURED_TRAFFIC = {"k_col_f<4,0> + k_tile_fwd_f<10,1>": 1230588672}
+# DRAM bytes (read + write) of one digit-transform launch, per (schedule, rows), from an
+# ncu capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum over its kernels)
+MEASURED_TRAFFIC = {("k_col_f<4,0> + k_tile_fwd_f<10,1>", 2560): 1230588672}
 STEPS_SET = [1 << i for i in range(13)]
 SCALE = 2.0**40
 SEED = 20261203
@@ -729,7 +729,7 @@ def run_cuda_arm(args) -> None:
                 "pipelining": "copy-in, compute and copy-out of consecutive steps overlap (two buffer sets)"},
         "roofline": {"bound": "hbm", "kernel": f"forward FP64 NTT, {kname} (digit transforms, {PAIRS * ne} rows x 2^14)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": MEASURED_TRAFFIC.get(kname), "launch_ms": ntt_ms,
+                     "peak_source": peak_kind, "traffic": MEASURED_TRAFFIC.get((kname, PAIRS * ne)), "launch_ms": ntt_ms,
                      "algorithmic_bytes": alg_bytes},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
