@@ -349,6 +349,29 @@ int vfhe_cuda_ckks_rotate_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct
                                 const uint64_t *gens, const uint64_t *const *d_gks, void *workspace,
                                 void *stream);
 
+/* Batched rank-1 MLWE (RLWE / CKKS) encryption on the GPU, the batched form of
+ * mlwe_RNSc_sample (modules/mlwe/c/src/mlwe.c:190-241, reached from
+ * CKKS_Scheme.encrypt, modules/fhe/python/src/vfhe/fhe/ckks.py:100-104):
+ *   d_out [batch][2][L][N]  coefficient domain: a uniform, b = a s + e + m
+ *   d_msg [batch][L][N]     coefficient-domain plaintexts (NULL: encryptions of zero)
+ *   d_sk  [L][N]            the secret key limbs in the NTT domain (MLWE_Key.s_RNS)
+ * e is a rounded Gaussian of width sigma per coefficient, the same integer in every
+ * limb, as polynomial_gen_gaussian_RNSc_polynomial (rns_polynomial.c:255-271).
+ * Randomness: the engine's ChaCha20 stream (RFC 8439 block function; keyed from
+ * /dev/urandom, or by vfhe_prng_set_deterministic_seed), so outputs match the
+ * reference's in distribution, not bit for bit.  1 <= batch * nlimbs <= 65535. */
+int vfhe_cuda_rlwe_encrypt_batch(void *ntt, uint64_t *d_out, const uint64_t *d_msg, uint64_t batch,
+                                 const uint32_t *limbs, uint32_t nlimbs, const uint64_t *d_sk,
+                                 double sigma, void *stream);
+
+/* ChaCha20 keystream blocks counter0 .. counter0 + nblocks - 1 for a 256-bit key
+ * (8 little-endian words) and a 64-bit nonce, in the original layout (64-bit block
+ * counter in state words 12-13, nonce in 14-15), into d_out[nblocks][16] words: the
+ * generator every sampling kernel of the engine uses.  No counterpart in the reference
+ * (its generators are AES-CTR and BLAKE3, modules/misc/c/src/prng.c:91-137). */
+int vfhe_cuda_prng_blocks(uint32_t *d_out, uint64_t nblocks, const uint32_t *key, uint64_t counter0,
+                          uint64_t nonce, void *stream);
+
 /* Batched CGGI16 functional bootstrap with the RNS gadget (CGGI16.functional_bootstrap,
  * modules/fhe/python/src/vfhe/fhe/cggi16.py:46-128, over mgsw_CMUX, mgsw.c:52-72).
  * `batch` LWE ciphertexts of dimension n over the L0 (1 or 2) primes limbs[] are

@@ -12,7 +12,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .arith import Ring
+from .arith import Polynomial, Ring
 from .mlwe import MLWE, MLWE_Set
 from .native import Engine, EngineError, cuda_engine
 
@@ -83,6 +83,37 @@ class CkksBatch:
             self.ffi.cast("void*", ws.data_ptr()), self._stream(stream))
         self._check(rc, "ckks_rotate_batch")
         return out
+
+
+    def encrypt(self, key, msgs: torch.Tensor | None, batch: int | None = None, sigma: float | None = None,
+                out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """Batched encryption under ``key`` (an MLWE_Key of rank 1 at this ring):
+        [B][2][L][N] coefficient-domain ciphertexts of the coefficient-domain plaintext
+        rows ``msgs`` [B][L][N] (None: ``batch`` encryptions of zero); the batched form
+        of CKKS_Scheme.encrypt / mlwe_RNSc_sample (vfhe_cuda_rlwe_encrypt_batch)."""
+        B = msgs.shape[0] if msgs is not None else int(batch)
+        N = self.ring.N
+        if out is None:
+            out = torch.empty((B, 2, self.L, N), dtype=torch.int64, device="cuda")
+        sk = self._secret_rows(key)
+        rc = self.lib.vfhe_cuda_rlwe_encrypt_batch(
+            self.ring.NTT, _ptr(self.ffi, out), _ptr(self.ffi, msgs) if msgs is not None else self.ffi.NULL, B,
+            self._limbs, self.L, _ptr(self.ffi, sk), float(key.sigma_err if sigma is None else sigma),
+            self._stream(stream))
+        self._check(rc, "rlwe_encrypt_batch")
+        return out
+
+    def _secret_rows(self, key) -> torch.Tensor:
+        """The key's secret polynomial at this ring's limbs, NTT domain [L][N] (cached)."""
+        cache = getattr(self, "_sk_cache", None)
+        if cache is not None and cache[0] is key:
+            return cache[1]
+        assert len(key.key) == 1, "rank-1 keys only"
+        p = Polynomial(self.ring).from_array(key.key[0])
+        p.to_NTT()
+        sk = to_device(p.rows())
+        self._sk_cache = (key, sk)
+        return sk
 
 
 class CggiBatch:

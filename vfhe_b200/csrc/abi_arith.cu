@@ -246,8 +246,8 @@ void polynomial_gen_random_RNSc_polynomial(void* out) {
     Poly* o = as_poly(out);
     prefetch_poly(o);
     EwSet s = poly_set(o, nullptr, nullptr, o->pub.rns_mask);
-    const uint64_t ctr = prng_advance((uint64_t)s.n * (s.nlimbs ? s.nlimbs : 1));
-    VC_CHECK(launch_sample_uniform(s, prng_seed(), ctr, pool_of(o)->d_info, stream()));
+    const uint64_t ctr = prng_advance((uint64_t)((s.n + 3) / 4) * (uint64_t)(s.nlimbs ? s.nlimbs : 1));
+    VC_CHECK(launch_sample_uniform(s, prng_key(), ctr, pool_of(o)->d_info, stream()));
     VC_FINISH();
 }
 
@@ -257,8 +257,8 @@ void polynomial_gen_gaussian_RNSc_polynomial(void* out, double sigma) {
     Poly* o = as_poly(out);
     prefetch_poly(o);
     EwSet s = poly_set(o, nullptr, nullptr, o->pub.rns_mask);
-    const uint64_t ctr = prng_advance((uint64_t)s.n);
-    VC_CHECK(launch_sample_gaussian(s, sigma, prng_seed(), ctr, pool_of(o)->d_info, stream()));
+    const uint64_t ctr = prng_advance((uint64_t)((s.n + 3) / 4));
+    VC_CHECK(launch_sample_gaussian(s, sigma, prng_key(), ctr, pool_of(o)->d_info, stream()));
     VC_FINISH();
 }
 

@@ -74,19 +74,19 @@ void set_masks(RNS_MLWE m, uint64_t mask) {
     m->b->rns_mask = mask;
 }
 
-__global__ void k_gauss_int(int64_t* out, long long n, double sigma, uint64_t seed, uint64_t ctr) {
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n;
-         x += (long long)gridDim.x * blockDim.x) {
-        uint64_t z1 = seed ^ ((ctr + x) * 0xd1b54a32d192ed03ULL), z2 = z1 + 0x632be59bd9b4e019ULL;
-        z1 = (z1 ^ (z1 >> 30)) * 0xbf58476d1ce4e5b9ULL;
-        z1 = (z1 ^ (z1 >> 27)) * 0x94d049bb133111ebULL;
-        z1 ^= z1 >> 31;
-        z2 = (z2 ^ (z2 >> 30)) * 0xbf58476d1ce4e5b9ULL;
-        z2 = (z2 ^ (z2 >> 27)) * 0x94d049bb133111ebULL;
-        z2 ^= z2 >> 31;
-        const double u1 = ((double)(z1 >> 11) + 1.0) * (1.0 / 9007199254740992.0);
-        const double u2 = (double)(z2 >> 11) * (1.0 / 9007199254740992.0);
-        out[x] = (int64_t)(sigma * sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+// Gaussian integers (truncated Box-Muller draws), four per ChaCha20 block from ctr on.
+__global__ void k_gauss_int(int64_t* out, long long n, double sigma, const __grid_constant__ PrngKey key,
+                            uint64_t ctr) {
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; 4 * j < n;
+         j += (long long)gridDim.x * blockDim.x) {
+        uint32_t blk[16];
+        chacha20_block(key, ctr + j, kStreamInteger, blk);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (4 * j + e >= n) break;
+            out[4 * j + e] = (int64_t)(sigma * sqrt(-2.0 * log(unit_open_low(block_u64(blk, 2 * e)))) *
+                                       cospi(2.0 * unit_closed_low(block_u64(blk, 2 * e + 1))));
+        }
     }
 }
 
@@ -122,16 +122,17 @@ __global__ void k_lwe_subto(uint64_t* const* oa, uint64_t* ob, const uint64_t* c
 
 // lwe_sample (lwe.c:95-121) with the engine's PRNG: uniform a, rounded Gaussian e.
 __global__ void k_lwe_uniform(uint64_t* const* a, const PrimeInfo* __restrict__ primes, long long n,
-                              uint64_t seed, uint64_t ctr) {
+                              const __grid_constant__ PrngKey key, uint64_t ctr) {
     const int i = blockIdx.y;
     const uint64_t q = primes[i].q;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+    const long long per_row = (n + 3) / 4;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per_row;
          j += (long long)gridDim.x * blockDim.x) {
-        uint64_t z = seed ^ ((ctr + (uint64_t)i * n + j) * 0xd1b54a32d192ed03ULL);
-        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-        z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-        z ^= z >> 31;
-        a[i][j] = __umul64hi(z, q);
+        uint32_t blk[16];
+        chacha20_block(key, ctr + (uint64_t)i * per_row + j, kStreamUniform, blk);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (4 * j + e < n) a[i][4 * j + e] = uniform_mod(block_u64(blk, 2 * e), block_u64(blk, 2 * e + 1), q);
     }
 }
 
@@ -214,8 +215,8 @@ void* lwe_new_key(uint64_t n, uint64_t l, void* ntt, double sec_sigma, double er
     LweKey* k = (LweKey*)lwe_alloc_key(n, l, ntt);
     if (!k) return nullptr;
     int64_t* d = (int64_t*)device_alloc(n * 8);
-    k_gauss_int<<<grid2((long long)n, 1), 256, 0, stream()>>>(d, (long long)n, sec_sigma, prng_seed(),
-                                                               prng_advance(n));
+    k_gauss_int<<<grid2((long long)n, 1), 256, 0, stream()>>>(d, (long long)n, sec_sigma, prng_key(),
+                                                               prng_advance((n + 3) / 4));
     std::vector<int64_t> h(n);
     VC_CHECK(cudaMemcpyAsync(h.data(), d, n * 8, cudaMemcpyDeviceToHost, stream()));
     vc::sync(vc_where_);
@@ -234,13 +235,20 @@ void* lwe_new_sparse_ternary_key(uint64_t n, uint64_t l, void* ntt, uint64_t h, 
     if (!k) return nullptr;
     IncNtt* t = as_ntt(ntt);
     std::vector<int> v(n, 0);
-    uint64_t seed = prng_seed() ^ prng_advance(n);
-    uint64_t placed = 0, guard = 0;
-    while (placed < h && placed < n && guard++ < 64 * (n + 1)) {
-        seed = seed * 6364136223846793005ULL + 1442695040888963407ULL;
-        const uint64_t pos = (seed >> 11) % n;
+    // h distinct positions with random signs, drawn on the host from the engine's
+    // ChaCha20 stream (8 draws per block; a position is floor(r n / 2^63), r 63 bits)
+    const PrngKey key = prng_key();
+    const uint64_t nblocks = n + 16;  // 8 (n + 16) draws: far more than h distinct positions need
+    const uint64_t ctr = prng_advance(nblocks);
+    uint64_t placed = 0, draw = 0;
+    uint32_t blk[16];
+    while (placed < h && placed < n && draw < 8 * nblocks) {
+        if (draw % 8 == 0) chacha20_block(key, ctr + draw / 8, kStreamTernary, blk);
+        const uint64_t r = block_u64(blk, (int)(draw % 8));
+        ++draw;
+        const uint64_t pos = (uint64_t)(((unsigned __int128)(r >> 1) * n) >> 63);
         if (v[pos]) continue;
-        v[pos] = ((seed >> 7) & 1) ? 1 : -1;
+        v[pos] = (r & 1) ? 1 : -1;
         ++placed;
     }
     for (uint64_t j = 0; j < l; ++j)
@@ -260,7 +268,7 @@ void lwe_sample(void* c, uint64_t* m, void* key) {
     std::vector<uint64_t*> rows(s->pub.a, s->pub.a + l);
     uint64_t** d_rows = stage_ptrs(rows);
     k_lwe_uniform<<<grid2((long long)n, (int)l), 256, 0, stream()>>>(d_rows, t->d_info, (long long)n,
-                                                                      prng_seed(), prng_advance(n * l));
+                                                                      prng_key(), prng_advance((n + 3) / 4 * l));
     // phase of the fresh (a, b = 0) sample gives -<a, s>; b = e + <a, s> + m
     std::vector<uint64_t> zero(l, 0);
     memcpy(s->pub.b, zero.data(), l * 8);
@@ -270,7 +278,7 @@ void lwe_sample(void* c, uint64_t* m, void* key) {
     k_lwe_phase<<<(unsigned)l, 256, 0, stream()>>>(d_out, (const uint64_t* const*)d_rows, s->pub.b, d_s,
                                                    t->d_info, (long long)n);
     int64_t* d_e = (int64_t*)managed_alloc(8);
-    k_gauss_int<<<1, 32, 0, stream()>>>(d_e, 1, k->pub.sigma, prng_seed(), prng_advance(1));
+    k_gauss_int<<<1, 32, 0, stream()>>>(d_e, 1, k->pub.sigma, prng_key(), prng_advance(1));
     vc::sync(vc_where_);
     for (uint64_t i = 0; i < l; ++i) {
         const uint64_t q = t->info[i].q;
@@ -415,7 +423,7 @@ void* mlwe_new_RNS_gaussian_key(uint64_t N, uint64_t r, uint64_t l, double key_s
     std::vector<uint64_t> arr(N * r);
     int64_t* d = (int64_t*)device_alloc(N * r * 8);
     k_gauss_int<<<grid2((long long)(N * r), 1), 256, 0, stream()>>>(d, (long long)(N * r), key_sigma,
-                                                                     prng_seed(), prng_advance(N * r));
+                                                                     prng_key(), prng_advance((N * r + 3) / 4));
     VC_CHECK(cudaMemcpyAsync(arr.data(), d, N * r * 8, cudaMemcpyDeviceToHost, stream()));
     vc::sync(vc_where_);
     device_free(d);

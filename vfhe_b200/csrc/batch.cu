@@ -18,6 +18,10 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
 int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const uint32_t* limbs, uint32_t L,
                 uint32_t special, const uint64_t* gens, const uint64_t* const* gks, uint64_t* ws, cudaStream_t st);
 uint64_t cggi_ws_elems(uint64_t N, uint64_t B, uint64_t n, uint32_t L0);
+int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, const uint32_t* limbs, uint32_t L,
+                 const uint64_t* sk, double sigma, cudaStream_t st);
+int prng_blocks(uint32_t* out, uint64_t nblocks, const uint32_t* key8, uint64_t counter0, uint64_t nonce,
+                cudaStream_t st);
 int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* in_a, const uint64_t* in_b,
                    uint64_t B, uint32_t n, const uint32_t* limbs, uint32_t L0, uint32_t special, const uint64_t* bk,
                    const uint64_t* tv, uint64_t torus_base, uint64_t* ws, cudaStream_t st);
@@ -142,6 +146,24 @@ int vfhe_cuda_ckks_mul_relin_rescale_batch(void* ntt, uint64_t* d_out, const uin
     if (!ws) ws = engine_workspace(vfhe_cuda_ckks_mul_workspace_bytes(ntt, batch, nlimbs), st);
     if (!ws) return 1;
     return ckks_mul_relin_rescale(t, d_out, d_ct1, d_ct2, batch, limbs, nlimbs, special, d_rlk, ws, st);
+}
+
+int vfhe_cuda_rlwe_encrypt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_msg, uint64_t batch,
+                                 const uint32_t* limbs, uint32_t nlimbs, const uint64_t* d_sk, double sigma,
+                                 void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    return rlwe_encrypt(as_ntt(ntt), d_out, d_msg, batch, limbs, nlimbs, d_sk, sigma, (cudaStream_t)stream_);
+}
+
+int vfhe_cuda_prng_blocks(uint32_t* d_out, uint64_t nblocks, const uint32_t* key, uint64_t counter0, uint64_t nonce,
+                          void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    if (!d_out || !key) {
+        set_error("vfhe_cuda_prng_blocks", "null buffer or key");
+        return 1;
+    }
+    if (nblocks == 0) return 0;
+    return prng_blocks(d_out, nblocks, key, counter0, nonce, (cudaStream_t)stream_);
 }
 
 uint64_t vfhe_cuda_ckks_rotate_workspace_bytes(void* ntt, uint64_t batch, uint32_t nlimbs) {

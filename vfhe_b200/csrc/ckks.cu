@@ -410,6 +410,109 @@ int blocks_transform(IncNtt* t, uint64_t* data, uint64_t count, const uint32_t* 
     return launch_ntt(rs, t->d_info, inverse, st);
 }
 
+// ---- batched RLWE encryption (mlwe_RNSc_sample, modules/mlwe/c/src/mlwe.c:190-241)
+//
+// out [B][2][L][N]: the a rows are drawn uniform directly in the NTT domain (the
+// transform is a bijection, so that is the same distribution as the reference's
+// coefficient-domain draw followed by a transform) and the b rows receive the rounded
+// Gaussian integer of each coefficient reduced into every limb
+// (polynomial_gen_gaussian_RNSc_polynomial, rns_polynomial.c:255-271).  ChaCha20
+// blocks: Gaussian g0 + b ceil(N/4) + j, uniform u0 + (b L + i) ceil(N/4) + j.
+__global__ void k_encrypt_sample(uint64_t* __restrict__ out, const __grid_constant__ LimbPrimes lp,
+                                 const PrimeInfo* __restrict__ primes, int L, long long N, double sigma,
+                                 const __grid_constant__ PrngKey key, uint64_t g0, uint64_t u0) {
+    const long long b = blockIdx.y;
+    const long long per = (N + 3) / 4;
+    uint64_t* a = out + b * 2 * L * N;
+    uint64_t* e = a + (long long)L * N;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per;
+         j += (long long)gridDim.x * blockDim.x) {
+        uint32_t blk[16];
+        chacha20_block(key, g0 + (uint64_t)(b * per + j), kStreamGaussian, blk);
+        int64_t ev[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            ev[k] = (int64_t)llrint(sigma * sqrt(-2.0 * log(unit_open_low(block_u64(blk, 2 * k)))) *
+                                    cospi(2.0 * unit_closed_low(block_u64(blk, 2 * k + 1))));
+        for (int i = 0; i < L; ++i) {
+            const PrimeInfo& pi = primes[lp.p[i]];
+            chacha20_block(key, u0 + (uint64_t)((b * L + i) * per + j), kStreamUniform, blk);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const long long x = 4 * j + k;
+                if (x >= N) break;
+                a[(long long)i * N + x] = uniform_mod(block_u64(blk, 2 * k), block_u64(blk, 2 * k + 1), pi.q);
+                e[(long long)i * N + x] = reduce_signed(ev[k], pi);
+            }
+        }
+    }
+}
+
+// b = e + s a in the NTT domain: the ring's incomplete product over S blocks of P
+// slots (rns_polynomial.c:358-396), with the key broadcast to every ciphertext.
+template <int S>
+__global__ void k_encrypt_combine(uint64_t* __restrict__ out, const uint64_t* __restrict__ sk,
+                                  const __grid_constant__ LimbPrimes lp, const PrimeInfo* __restrict__ primes, int L,
+                                  long long N) {
+    const long long b = blockIdx.y / L;
+    const int i = blockIdx.y - (int)(b * L);
+    const PrimeInfo pi = primes[lp.p[i]];
+    const uint64_t q = pi.q;
+    const long long P = N / S;
+    const uint64_t* a = out + (b * 2 * L + i) * N;
+    uint64_t* eb = out + (b * 2 * L + L + i) * N;
+    const uint64_t* s = sk + (long long)i * N;
+    const ulonglong2* tw = reinterpret_cast<const ulonglong2*>(pi.twist);
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < P;
+         x += (long long)gridDim.x * blockDim.x) {
+        uint64_t av[S], sv[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            av[j] = a[j * P + x];
+            sv[j] = s[j * P + x];
+        }
+#pragma unroll
+        for (int o = 0; o < S; ++o) {
+            uint64_t acc = 0, wrap = 0;
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                if (j <= o) acc = add_mod(acc, mul_mod(sv[j], av[o - j], pi), q);
+                else wrap = add_mod(wrap, mul_mod(sv[j], av[o - j + S], pi), q);
+            }
+            if (S > 1) {
+                const ulonglong2 w = tw[x];
+                acc = add_mod(acc, shoup(wrap, w.x, w.y, q), q);
+            }
+            eb[o * P + x] = add_mod(eb[o * P + x], acc, q);
+        }
+    }
+}
+
+// b += m (coefficient domain); msg: [B][L][N].
+__global__ void k_encrypt_add_msg(uint64_t* __restrict__ out, const uint64_t* __restrict__ msg,
+                                  const __grid_constant__ LimbPrimes lp, const PrimeInfo* __restrict__ primes, int L,
+                                  long long N) {
+    const long long b = blockIdx.y / L;
+    const int i = blockIdx.y - (int)(b * L);
+    const uint64_t q = primes[lp.p[i]].q;
+    uint64_t* eb = out + (b * 2 * L + L + i) * N;
+    const uint64_t* m = msg + (b * L + i) * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+         x += (long long)gridDim.x * blockDim.x)
+        eb[x] = add_mod(eb[x], m[x], q);
+}
+
+__global__ void k_prng_blocks(uint32_t* __restrict__ out, uint64_t nblocks, const __grid_constant__ PrngKey key,
+                              uint64_t counter0, uint64_t nonce) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nblocks;
+         j += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t blk[16];
+        chacha20_block(key, counter0 + j, nonce, blk);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) out[j * 16 + k] = blk[k];
+    }
+}
+
 
 }  // namespace
 
@@ -548,6 +651,76 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
                                                             mc, t->d_info, nl, 0, N);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, const uint32_t* limbs, uint32_t L,
+                 const uint64_t* sk, double sigma, cudaStream_t st) {
+    const char* where = "vfhe_cuda_rlwe_encrypt_batch";
+    if (!t || !limbs || L == 0 || L > (uint32_t)kMaxLimbs || !out || !sk || B == 0 || B > 65535 / L ||
+        !(sigma >= 0.0)) {
+        set_error(where, "bad pool, limb list, buffers, batch (1 <= batch * nlimbs <= 65535) or sigma");
+        return 1;
+    }
+    for (uint32_t k = 0; k < L; ++k)
+        if (limbs[k] >= t->pub.l) {
+            set_error(where, "limb index outside the pool");
+            return 1;
+        }
+    const long long N = (long long)t->pub.N;
+    const int nl = (int)L;
+    LimbPrimes lp;
+    memset(&lp, 0, sizeof lp);
+    for (int i = 0; i < nl; ++i) lp.p[i] = limbs[i];
+    const uint64_t per = (uint64_t)((N + 3) / 4);
+    const uint64_t g0 = prng_advance(B * per * (1 + (uint64_t)L));
+    const uint64_t u0 = g0 + B * per;
+    k_encrypt_sample<<<grid_xy((long long)per, (long long)B), 256, 0, st>>>(out, lp, t->d_info, nl, N, sigma,
+                                                                            prng_key(), g0, u0);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    // forward transforms of the noise rows (b components)
+    RowSet rs;
+    memset(&rs, 0, sizeof rs);
+    for (int i = 0; i < nl; ++i) {
+        rs.in[i] = out + ((long long)nl + i) * N;
+        rs.out[i] = out + ((long long)nl + i) * N;
+        rs.prime[i] = limbs[i];
+    }
+    rs.nlimbs = nl;
+    rs.split = (int)t->pub.split_degree;
+    rs.logP = t->logP;
+    rs.batch = (int)B;
+    rs.batch_stride = 2LL * nl * N;
+    rs.in_batch_stride = rs.batch_stride;
+    mark_fp64(rs, t);
+    if (!check_cuda(launch_ntt(rs, t->d_info, false, st), where)) return 1;
+    const dim3 g = grid_xy(N / (long long)t->pub.split_degree, (long long)B * nl);
+    switch (t->pub.split_degree) {
+        case 1: k_encrypt_combine<1><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        case 2: k_encrypt_combine<2><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        case 4: k_encrypt_combine<4><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        case 8: k_encrypt_combine<8><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        default: k_encrypt_combine<16><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+    }
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    // both components back to the coefficient domain
+    if (!check_cuda(blocks_transform(t, out, 2 * B, limbs, nl, true, st), where)) return 1;
+    if (msg) {
+        k_encrypt_add_msg<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(out, msg, lp, t->d_info, nl, N);
+        if (!check_cuda(cudaGetLastError(), where)) return 1;
+    }
+    return 0;
+}
+
+int prng_blocks(uint32_t* out, uint64_t nblocks, const uint32_t* key8, uint64_t counter0, uint64_t nonce,
+                cudaStream_t st) {
+    PrngKey k;
+    memcpy(k.w, key8, sizeof k.w);
+    long long blocks = (long long)((nblocks + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    k_prng_blocks<<<(unsigned)blocks, 256, 0, st>>>(out, nblocks, k, counter0, nonce);
+    note_launch();
+    return check_cuda(cudaGetLastError(), "vfhe_cuda_prng_blocks") ? 0 : 1;
 }
 
 }  // namespace vc

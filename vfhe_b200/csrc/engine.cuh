@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/vfhe_cuda.h"
+#include "chacha.cuh"
 #include "modarith.cuh"
 #include "ntt.cuh"
 
@@ -181,14 +182,16 @@ struct DivideArgs {
 int launch_divide(const EwSet& set, const DivideArgs& d, const PrimeInfo* d_primes, cudaStream_t st);
 
 // Uniform residues / rounded Gaussian integers from the engine's counter PRNG.
-int launch_sample_uniform(const EwSet& set, uint64_t seed, uint64_t counter,
+int launch_sample_uniform(const EwSet& set, const PrngKey& key, uint64_t counter,
                           const PrimeInfo* d_primes, cudaStream_t st);
-int launch_sample_gaussian(const EwSet& set, double sigma, uint64_t seed, uint64_t counter,
+int launch_sample_gaussian(const EwSet& set, double sigma, const PrngKey& key, uint64_t counter,
                            const PrimeInfo* d_primes, cudaStream_t st);
 
-// PRNG stream position (vfhe_prng_set_deterministic_seed).
-uint64_t prng_seed();
-uint64_t prng_advance(uint64_t count);
+// Engine randomness (chacha.cuh): the ChaCha20 key (256 bits from /dev/urandom, or
+// expanded from the seed given to vfhe_prng_set_deterministic_seed) and the next free
+// block counter; prng_advance reserves `blocks` consecutive blocks and returns the first.
+PrngKey prng_key();
+uint64_t prng_advance(uint64_t blocks);
 void prng_set(uint64_t seed, bool deterministic);
 
 }  // namespace vc

@@ -167,45 +167,53 @@ __global__ void k_divide(const __grid_constant__ EwSet set, DivideArgs d, const 
     }
 }
 
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-    z += 0x9e3779b97f4a7c15ULL;
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-    return z ^ (z >> 31);
-}
-__device__ __forceinline__ uint64_t rand64(uint64_t seed, uint64_t ctr) {
-    return mix64(mix64(seed ^ (ctr * 0xd1b54a32d192ed03ULL)) + ctr);
-}
-
+// Uniform residues, four per ChaCha20 block (128 bits each, so the residues are within
+// q / 2^128 of uniform).  Row r (limb k of polynomial b) owns blocks
+// counter + r ceil(n/4) ...; thread j fills elements 4j .. 4j+3 of its row.
 __global__ void k_uniform(const __grid_constant__ EwSet set, const PrimeInfo* __restrict__ primes,
-                          uint64_t seed, uint64_t counter) {
+                          const __grid_constant__ PrngKey key, uint64_t counter) {
     int k;
     long long boff;
     limb_coords(set, k, boff);
     const uint64_t q = primes[set.prime[k]].q;
     uint64_t* out = set.out[k] + boff;
-    const uint64_t base = counter + (uint64_t)blockIdx.y * (uint64_t)set.n;
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < set.n;
-         x += (long long)gridDim.x * blockDim.x)
-        out[x] = __umul64hi(rand64(seed, base + x), q);
+    const long long per_row = (set.n + 3) / 4;
+    const uint64_t base = counter + (uint64_t)blockIdx.y * (uint64_t)per_row;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per_row;
+         j += (long long)gridDim.x * blockDim.x) {
+        uint32_t blk[16];
+        chacha20_block(key, base + j, kStreamUniform, blk);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (4 * j + e < set.n) out[4 * j + e] = uniform_mod(block_u64(blk, 2 * e), block_u64(blk, 2 * e + 1), q);
+    }
 }
 
-// Rounded Gaussian integers shared by every limb of a coefficient, reduced per limb.
+// Rounded Gaussian integers shared by every limb of a coefficient, reduced per limb
+// (polynomial_gen_gaussian_RNSc_polynomial, rns_polynomial.c:255-271: Box-Muller with
+// the cosine branch, then round).  Polynomial b owns blocks counter + b ceil(n/4) ...,
+// four coefficients per block; every limb row of the polynomial recomputes the same
+// blocks, so the integer is the same in each limb.
 __global__ void k_gaussian(const __grid_constant__ EwSet set, const PrimeInfo* __restrict__ primes,
-                           double sigma, uint64_t seed, uint64_t counter) {
+                           double sigma, const __grid_constant__ PrngKey key, uint64_t counter) {
     int k;
     long long boff;
     limb_coords(set, k, boff);
     const PrimeInfo pi = primes[set.prime[k]];
     uint64_t* out = set.out[k] + boff;
-    const uint64_t base = counter + (uint64_t)(blockIdx.y / set.nlimbs) * (uint64_t)set.n;
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < set.n;
-         x += (long long)gridDim.x * blockDim.x) {
-        const uint64_t r1 = rand64(seed, 2 * (base + x)), r2 = rand64(seed, 2 * (base + x) + 1);
-        const double u1 = ((double)(r1 >> 11) + 1.0) * (1.0 / 9007199254740992.0);
-        const double u2 = (double)(r2 >> 11) * (1.0 / 9007199254740992.0);
-        const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-        out[x] = reduce_signed((int64_t)llrint(sigma * z), pi);
+    const long long per_poly = (set.n + 3) / 4;
+    const uint64_t base = counter + (uint64_t)(blockIdx.y / set.nlimbs) * (uint64_t)per_poly;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per_poly;
+         j += (long long)gridDim.x * blockDim.x) {
+        uint32_t blk[16];
+        chacha20_block(key, base + j, kStreamGaussian, blk);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (4 * j + e >= set.n) break;
+            const double z = sqrt(-2.0 * log(unit_open_low(block_u64(blk, 2 * e)))) *
+                             cospi(2.0 * unit_closed_low(block_u64(blk, 2 * e + 1)));
+            out[4 * j + e] = reduce_signed((int64_t)llrint(sigma * z), pi);
+        }
     }
 }
 
@@ -291,17 +299,17 @@ int launch_divide(const EwSet& set, const DivideArgs& d, const PrimeInfo* d_prim
     return (int)cudaGetLastError();
 }
 
-int launch_sample_uniform(const EwSet& set, uint64_t seed, uint64_t counter, const PrimeInfo* d_primes,
+int launch_sample_uniform(const EwSet& set, const PrngKey& key, uint64_t counter, const PrimeInfo* d_primes,
                           cudaStream_t st) {
     if (set.nlimbs <= 0) return 0;
-    k_uniform<<<ew_grid(set), kThreads, 0, st>>>(set, d_primes, seed, counter);
+    k_uniform<<<ew_grid(set), kThreads, 0, st>>>(set, d_primes, key, counter);
     return (int)cudaGetLastError();
 }
 
-int launch_sample_gaussian(const EwSet& set, double sigma, uint64_t seed, uint64_t counter,
+int launch_sample_gaussian(const EwSet& set, double sigma, const PrngKey& key, uint64_t counter,
                            const PrimeInfo* d_primes, cudaStream_t st) {
     if (set.nlimbs <= 0) return 0;
-    k_gaussian<<<ew_grid(set), kThreads, 0, st>>>(set, d_primes, sigma, seed, counter);
+    k_gaussian<<<ew_grid(set), kThreads, 0, st>>>(set, d_primes, sigma, key, counter);
     return (int)cudaGetLastError();
 }
 

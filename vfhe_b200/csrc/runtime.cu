@@ -3,6 +3,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include <atomic>
 #include <map>
@@ -152,36 +153,69 @@ void prefetch_to_device(const void* p, size_t bytes) {
 
 // ---------------------------------------------------------------- PRNG state
 namespace {
-uint64_t g_seed = 0;
+PrngKey g_key;
 uint64_t g_counter = 0;
 bool g_seeded = false;
-uint64_t entropy_seed() {
-    uint64_t s = 0;
+std::mutex g_prng_mu;
+
+uint64_t splitmix_next(uint64_t& x) {
+    uint64_t z = (x += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+PrngKey expand_seed(uint64_t seed) {
+    PrngKey k;
+    uint64_t x = seed;
+    for (int i = 0; i < 4; ++i) {
+        const uint64_t v = splitmix_next(x);
+        k.w[2 * i] = (uint32_t)v;
+        k.w[2 * i + 1] = (uint32_t)(v >> 32);
+    }
+    return k;
+}
+
+// 256 bits from the operating system's entropy source; without one the key still
+// differs per process (address, time) and the engine records an error.
+PrngKey entropy_key() {
+    PrngKey k;
+    memset(&k, 0, sizeof k);
     FILE* f = fopen("/dev/urandom", "rb");
+    bool ok = false;
     if (f) {
-        if (fread(&s, sizeof s, 1, f) != 1) s = 0;
+        ok = fread(k.w, sizeof k.w, 1, f) == 1;
         fclose(f);
     }
-    return s ^ 0x9e3779b97f4a7c15ULL;
+    if (!ok) {
+        set_error("prng", "/dev/urandom unavailable: key from process address and time only");
+        k = expand_seed((uint64_t)(uintptr_t)&k ^ (uint64_t)time(nullptr));
+    }
+    return k;
 }
 }  // namespace
 
-uint64_t prng_seed() {
+PrngKey prng_key() {
+    std::lock_guard<std::mutex> lk(g_prng_mu);
     if (!g_seeded) {
-        g_seed = entropy_seed();
+        g_key = entropy_key();
         g_counter = 0;
         g_seeded = true;
     }
-    return g_seed;
+    return g_key;
 }
-uint64_t prng_advance(uint64_t count) {
-    prng_seed();
-    uint64_t c = g_counter;
-    g_counter += count;
+uint64_t prng_advance(uint64_t blocks) {
+    prng_key();
+    std::lock_guard<std::mutex> lk(g_prng_mu);
+    const uint64_t c = g_counter;
+    g_counter += blocks;
     return c;
 }
+// Deterministic mode (tests): the 64-bit seed expanded to a key by splitmix64.
 void prng_set(uint64_t seed, bool det) {
-    g_seed = det ? seed : entropy_seed();
+    const PrngKey k = det ? expand_seed(seed) : entropy_key();
+    std::lock_guard<std::mutex> lk(g_prng_mu);
+    g_key = k;
     g_counter = 0;
     g_seeded = true;
 }
