@@ -442,6 +442,50 @@ def rns_cggi_leg(eng, count: int = 1024, cpu_bootstraps: int = 2) -> dict:
     return res
 
 
+def encrypt_leg(eng, s, key, msgs, reps: int = 5, cpu_encryptions: int = 8) -> dict:
+    """Batched CKKS encryption (vfhe_cuda_rlwe_encrypt_batch) of the workload's batch of
+    coefficient-domain plaintexts at N = 2^14, L = 9, and the reference library's own
+    CKKS_Scheme.encrypt (mlwe_RNSc_sample) on one host core."""
+    import torch
+
+    from vfhe_b200.batch import CkksBatch
+
+    enc = CkksBatch(s.rings[0], s.special_rings[0].prime_indices[-1], eng)
+    out = enc.encrypt(key, msgs)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        enc.encrypt(key, msgs, out=out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    B = msgs.shape[0]
+    res = {"workload": f"{B} ciphertexts, N=2^14, L=9, ternary key, sigma 3.2, ChaCha20 randomness",
+           "ciphertexts_per_s": B / (ms * 1e-3), "ms_per_batch": ms}
+    lib, name = _ref_library()
+    if lib.exists() and cpu_encryptions > 0:
+        from vfhe_b200.native import Engine
+
+        from vfhe_b200.arith import Ring
+        from vfhe_b200.fhe import CKKS_Scheme
+        from vfhe_b200.native import use_engine
+
+        ref = Engine(lib)
+        with use_engine(ref):
+            rs = CKKS_Scheme(Ring(N_DEG, prime_size=PRIME_SIZES, split_degree=1), scaling_factor=SCALE,
+                             special_primes=1)
+            rkey = rs.key_gen_uniform_ternary(3.2, np.random.default_rng(SEED + 13))
+            pt = rs.encode([0.5] * (N_DEG // 2))
+            t0 = time.perf_counter()
+            for _ in range(cpu_encryptions):
+                rs.encrypt(pt, rkey)
+            res["cpu_reference_ms_per_ciphertext"] = 1e3 * (time.perf_counter() - t0) / cpu_encryptions
+        res["cpu_reference"] = f"reference's {name} engine, one core, {cpu_encryptions} encryptions"
+    return res
+
+
 def serving_leg(eng, requests: int, rates=(50.0, 200.0, 1000.0)) -> dict:
     """Poisson request streams of mixed CKKS (N 2^13..2^16, L 4..24: multiply+relin+
     rescale or rotate) and CGGI16 bootstrap batches (1..1024 LWEs, n = 630, N = 1024),
@@ -683,6 +727,7 @@ def run_cuda_arm(args) -> None:
     # the reference's default split for 50-bit primes: four 2^14-point blocks per limb
     ms16s4, limbs16s4 = ntt16_rate(4, False)
     eng.check("bench")
+    encrypt = encrypt_leg(eng, s, key, d1[:, 1].contiguous(), reps=5)
 
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
     serving = None if args.no_serving else serving_leg(eng, args.serving_requests)
@@ -745,6 +790,7 @@ def run_cuda_arm(args) -> None:
         line["serving"] = serving
     if cggi_fft is not None:
         line["cggi_fft_bootstrap"] = cggi_fft
+    line["ckks_encrypt"] = encrypt
     if rns_cggi is not None:
         line["cggi16_rns_bootstrap"] = rns_cggi
     if world == 1 and not args.no_cpu_baseline:
