@@ -364,6 +364,21 @@ int vfhe_cuda_rlwe_encrypt_batch(void *ntt, uint64_t *d_out, const uint64_t *d_m
                                  const uint32_t *limbs, uint32_t nlimbs, const uint64_t *d_sk,
                                  double sigma, void *stream);
 
+/* Key-switching keys generated on the GPU, the batched _gen_ksk_components
+ * (modules/mlwe/python/src/vfhe/mlwe/mlwe.py:145-177) behind gen_rlk / gen_ksk /
+ * gen_ksk_automorphism: for each of the nsrc source polynomials j and each of the
+ * L extended limbs i, digit j L + i is an RLWE encryption under d_sk of
+ * src_j (P mod q_i) e_i, written in the NTT domain:
+ *   d_out [nsrc * L][2][L][N]   the key tensor layout of the batched CKKS calls
+ *   d_src [nsrc][L][N]          source polynomials in the NTT domain (e.g. -s^2, or
+ *                               the permuted key for a Galois key)
+ *   factors[L]                  host array: P mod q_i (P = product of special primes)
+ *   d_sk  [L][N]                the output key's secret limbs, NTT domain
+ * Limbs are the extended (special) ring's.  1 <= nsrc * L * L <= 65535. */
+int vfhe_cuda_gen_ksk_batch(void *ntt, uint64_t *d_out, const uint64_t *d_src, uint64_t nsrc,
+                            const uint32_t *limbs, uint32_t nlimbs, const uint64_t *factors,
+                            const uint64_t *d_sk, double sigma, void *stream);
+
 /* ChaCha20 keystream blocks counter0 .. counter0 + nblocks - 1 for a 256-bit key
  * (8 little-endian words) and a 64-bit nonce, in the original layout (64-bit block
  * counter in state words 12-13, nonce in 14-15), into d_out[nblocks][16] words: the

@@ -147,6 +147,52 @@ class CggiBatch:
         return out_a, out_b
 
 
+def gen_ksk_batch(scheme, key_out, polys: list, lvl: int, sigma: float | None = None,
+                  engine: Engine | None = None, stream=None) -> torch.Tensor:
+    """Key-switching key generated on the GPU (vfhe_cuda_gen_ksk_batch): the batched
+    _gen_ksk_components of the scheme (mlwe.py:145-177) for the source polynomials
+    ``polys`` at level ``lvl``, as the device tensor [len(polys) * (L+1)][2][L+1][N]
+    (NTT domain) that key_tensor() gives for a key generated one digit at a time."""
+    engine = engine or cuda_engine()
+    ffi, lib = engine.ffi, engine.lib
+    sring = scheme.special_rings[lvl]
+    P = sring.modulus_ratio(scheme.rings[lvl])
+    factors = ffi.new("uint64_t[]", [int(P % q) for q in sring.primes])
+    src = []
+    for poly in polys:
+        if poly.ring != sring:
+            poly = Polynomial(sring).from_bigint_array(poly.get_polynomial(signed=True))
+        else:
+            poly = poly.copy()
+        poly.to_NTT()
+        src.append(poly.rows())
+    d_src = to_device(np.stack(src))
+    skp = Polynomial(sring).from_array(key_out.key[0])
+    skp.to_NTT()
+    d_sk = to_device(skp.rows())
+    L, N = sring.ell, sring.N
+    out = torch.empty((len(polys) * L, 2, L, N), dtype=torch.int64, device="cuda")
+    limbs = ffi.new("uint32_t[]", list(sring.prime_indices))
+    st = stream or torch.cuda.current_stream()
+    rc = lib.vfhe_cuda_gen_ksk_batch(sring.NTT, _ptr(ffi, out), _ptr(ffi, d_src), len(polys), limbs, L, factors,
+                                     _ptr(ffi, d_sk), float(key_out.sigma_err if sigma is None else sigma),
+                                     ffi.cast("void*", st.cuda_stream))
+    if rc != 0:
+        engine.check("gen_ksk_batch")
+        raise EngineError("gen_ksk_batch")
+    return out
+
+
+def gen_rlk_batch(scheme, key, lvl: int = 0, **kw) -> torch.Tensor:
+    """Relinearisation key (gen_rlk for a rank-1 key) generated on the GPU."""
+    return gen_ksk_batch(scheme, key, scheme.quadratic_key_polys(key), lvl, **kw)
+
+
+def gen_galois_key_batch(scheme, key, gen: int, lvl: int = 0, **kw) -> torch.Tensor:
+    """Automorphism key for X -> X^gen (gen_ksk_automorphism) generated on the GPU."""
+    return gen_ksk_batch(scheme, key, [p.automorphism(gen) for p in key.poly], lvl, **kw)
+
+
 def bootstrap_key_tensor(bk) -> torch.Tensor:
     """Device copy of a CGGI16_Key: [n][2 L0][2][L0+1][N] (MGSW rows in encryption order)."""
     arr = np.stack([np.stack([np.stack([c.component_rows(0), c.component_rows(1)]) for c in m.obj]) for m in bk.bk])

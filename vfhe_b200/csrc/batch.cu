@@ -22,6 +22,8 @@ int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, cons
                  const uint64_t* sk, double sigma, cudaStream_t st);
 int prng_blocks(uint32_t* out, uint64_t nblocks, const uint32_t* key8, uint64_t counter0, uint64_t nonce,
                 cudaStream_t st);
+int rlwe_gen_ksk(IncNtt* t, uint64_t* out, const uint64_t* src, uint64_t nsrc, const uint32_t* limbs, uint32_t L,
+                 const uint64_t* factors, const uint64_t* sk, double sigma, cudaStream_t st);
 int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* in_a, const uint64_t* in_b,
                    uint64_t B, uint32_t n, const uint32_t* limbs, uint32_t L0, uint32_t special, const uint64_t* bk,
                    const uint64_t* tv, uint64_t torus_base, uint64_t* ws, cudaStream_t st);
@@ -153,6 +155,13 @@ int vfhe_cuda_rlwe_encrypt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_m
                                  void* stream_) {
     if (!vc::ensure_ready()) return 1;
     return rlwe_encrypt(as_ntt(ntt), d_out, d_msg, batch, limbs, nlimbs, d_sk, sigma, (cudaStream_t)stream_);
+}
+
+int vfhe_cuda_gen_ksk_batch(void* ntt, uint64_t* d_out, const uint64_t* d_src, uint64_t nsrc, const uint32_t* limbs,
+                            uint32_t nlimbs, const uint64_t* factors, const uint64_t* d_sk, double sigma,
+                            void* stream_) {
+    if (!vc::ensure_ready()) return 1;
+    return rlwe_gen_ksk(as_ntt(ntt), d_out, d_src, nsrc, limbs, nlimbs, factors, d_sk, sigma, (cudaStream_t)stream_);
 }
 
 int vfhe_cuda_prng_blocks(uint32_t* d_out, uint64_t nblocks, const uint32_t* key, uint64_t counter0, uint64_t nonce,

@@ -502,6 +502,29 @@ __global__ void k_encrypt_add_msg(uint64_t* __restrict__ out, const uint64_t* __
         eb[x] = add_mod(eb[x], m[x], q);
 }
 
+// Gadget messages of a key-switching key, added in the NTT domain: digit d = j L + i of
+// source polynomial j gets factor_i * src_j (limb i only) in its b row
+// (_gen_ksk_components, modules/mlwe/python/src/vfhe/mlwe/mlwe.py:145-177: the message
+// poly_j * (P mod q_i) e_i, whose transform is factor_i times the limb-i transform).
+struct GadgetFactors {
+    uint64_t f[kMaxLimbs];
+};
+
+__global__ void k_gadget_add(uint64_t* __restrict__ out, const uint64_t* __restrict__ src,
+                             const __grid_constant__ GadgetFactors gf, const __grid_constant__ LimbPrimes lp,
+                             const PrimeInfo* __restrict__ primes, int L, long long N) {
+    const long long d = blockIdx.y;
+    const long long j = d / L;
+    const int i = (int)(d - j * L);
+    const PrimeInfo pi = primes[lp.p[i]];
+    uint64_t* b = out + (d * 2 + 1) * L * N + (long long)i * N;
+    const uint64_t* sr = src + (j * L + i) * N;
+    const uint64_t f = gf.f[i] % pi.q;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+         x += (long long)gridDim.x * blockDim.x)
+        b[x] = add_mod(b[x], mul_mod(sr[x], f, pi), pi.q);
+}
+
 __global__ void k_prng_blocks(uint32_t* __restrict__ out, uint64_t nblocks, const __grid_constant__ PrngKey key,
                               uint64_t counter0, uint64_t nonce) {
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nblocks;
@@ -653,9 +676,10 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
 
-int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, const uint32_t* limbs, uint32_t L,
-                 const uint64_t* sk, double sigma, cudaStream_t st) {
-    const char* where = "vfhe_cuda_rlwe_encrypt_batch";
+namespace {
+// ntt_out: leave both components in the NTT domain (msg must then be null).
+int rlwe_encrypt_impl(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, const uint32_t* limbs, uint32_t L,
+                      const uint64_t* sk, double sigma, bool ntt_out, const char* where, cudaStream_t st) {
     if (!t || !limbs || L == 0 || L > (uint32_t)kMaxLimbs || !out || !sk || B == 0 || B > 65535 / L ||
         !(sigma >= 0.0)) {
         set_error(where, "bad pool, limb list, buffers, batch (1 <= batch * nlimbs <= 65535) or sigma");
@@ -702,6 +726,8 @@ int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, cons
         default: k_encrypt_combine<16><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
     }
     if (!check_cuda(cudaGetLastError(), where)) return 1;
+    // a was drawn in the NTT domain: a key wants both components there already
+    if (ntt_out) return 0;
     // both components back to the coefficient domain
     if (!check_cuda(blocks_transform(t, out, 2 * B, limbs, nl, true, st), where)) return 1;
     if (msg) {
@@ -709,6 +735,34 @@ int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, cons
         if (!check_cuda(cudaGetLastError(), where)) return 1;
     }
     return 0;
+}
+
+}  // namespace
+
+int rlwe_encrypt(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, const uint32_t* limbs, uint32_t L,
+                 const uint64_t* sk, double sigma, cudaStream_t st) {
+    return rlwe_encrypt_impl(t, out, msg, B, limbs, L, sk, sigma, false, "vfhe_cuda_rlwe_encrypt_batch", st);
+}
+
+int rlwe_gen_ksk(IncNtt* t, uint64_t* out, const uint64_t* src, uint64_t nsrc, const uint32_t* limbs, uint32_t L,
+                 const uint64_t* factors, const uint64_t* sk, double sigma, cudaStream_t st) {
+    const char* where = "vfhe_cuda_gen_ksk_batch";
+    if (!src || !factors || nsrc == 0 || L == 0 || nsrc * L > 65535 / (L ? L : 1)) {
+        set_error(where, "need source polynomials, gadget factors and 1 <= nsrc * nlimbs^2 <= 65535");
+        return 1;
+    }
+    if (rlwe_encrypt_impl(t, out, nullptr, nsrc * L, limbs, L, sk, sigma, true, where, st)) return 1;
+    LimbPrimes lp;
+    memset(&lp, 0, sizeof lp);
+    GadgetFactors gf;
+    memset(&gf, 0, sizeof gf);
+    for (uint32_t i = 0; i < L; ++i) {
+        lp.p[i] = limbs[i];
+        gf.f[i] = factors[i];
+    }
+    const long long N = (long long)t->pub.N;
+    k_gadget_add<<<grid_xy(N, (long long)(nsrc * L)), 256, 0, st>>>(out, src, gf, lp, t->d_info, (int)L, N);
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
 
 int prng_blocks(uint32_t* out, uint64_t nblocks, const uint32_t* key8, uint64_t counter0, uint64_t nonce,
