@@ -6,6 +6,7 @@ difference in a residue is an engine difference.
 
 from __future__ import annotations
 
+import numpy as np
 import pytest
 
 from . import scenarios
@@ -60,3 +61,85 @@ def test_cggi_bootstrap_n1024(cuda, oracle_engine):
     b = scenarios.cggi_bootstrap(oracle_engine, N=1024, n_lwe=64, count=2)
     compare(a, b)
     assert all(a["ok"])
+
+
+def test_full_packing_keyswitch_matches_reference_library(cuda, ref_portable):
+    """mlwe_full_packing_keyswitch (mlwe.c:343-430, GP25's LWE repacking): the same
+    samples and packing key on the cuda engine and on the reference's own library
+    give the same MLWE, residue for residue."""
+    from tests.helpers import twin_rings
+    from vfhe_b200.arith import repr
+    from vfhe_b200.mlwe import LWE, MLWE, MLWE_Scheme, MLWE_Set
+
+    N, size = 256, 8
+    rng = np.random.default_rng(41)
+    outs = []
+    rings = twin_rings([cuda, ref_portable], N, [50, 50, 50], split=1)
+    rows_lwe = [(np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in rings[0].primes[:2]]),
+                 [int(rng.integers(0, q)) for q in rings[0].primes[:2]]) for _ in range(size)]
+    key_rows = [[np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in rings[0].primes])
+                           for _ in range(2)]) for _ in range(2)] for _ in range(N)]
+    for R in rings:
+        s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
+        lwes = []
+        for a, b in rows_lwe:
+            c = LWE(s.rings[0], n=N)
+            c.set_rows(a, b)
+            lwes.append(c)
+        comps = []
+        for i in range(N):
+            row = []
+            for d in range(2):
+                k = MLWE(s, ring=s.special_rings[0])
+                k.set_component_rows(0, key_rows[i][d][0])
+                k.set_component_rows(1, key_rows[i][d][1])
+                k.repr = repr.ntt
+                row.append(k)
+            comps.append(row)
+        ksk = MLWE_Set(comps)
+        res = MLWE(s, lvl=0)
+        arr = R.ffi.new("void*[]", [c.obj for c in lwes])
+        R.lib.mlwe_full_packing_keyswitch(res.obj, arr, size, ksk.obj, 0)
+        R.engine.check("mlwe_full_packing_keyswitch")
+        outs.append(np.stack([res.component_rows(0), res.component_rows(1)]))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_trace_matches_reference_library(cuda, ref_portable):
+    """mlwe_trace (mlwe.c:436-444 over mlwe_partial_trace, mlwe.c:328-341: log2 N automorphism key
+    switches and additions) on the cuda engine and on the reference's own library,
+    with the same (random) key material: the same MLWE, residue for residue."""
+    from tests.helpers import twin_rings
+    from vfhe_b200.arith import repr
+    from vfhe_b200.mlwe import MLWE, MLWE_Scheme, MLWE_Set
+
+    N = 256
+    logN = 8
+    rng = np.random.default_rng(43)
+    rings = twin_rings([cuda, ref_portable], N, [50, 50, 50], split=1)
+    ct_rows = [np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in rings[0].primes[:2]]) for _ in range(2)]
+    key_rows = [[np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in rings[0].primes])
+                           for _ in range(2)]) for _ in range(2)] for _ in range(logN)]
+    outs = []
+    for R in rings:
+        s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
+        c = MLWE(s, lvl=0)
+        c.set_component_rows(0, ct_rows[0])
+        c.set_component_rows(1, ct_rows[1])
+        c.repr = repr.coeff
+        sets = []
+        for g in range(logN):
+            digits = []
+            for d in range(2):
+                k = MLWE(s, ring=s.special_rings[0])
+                k.set_component_rows(0, key_rows[g][d][0])
+                k.set_component_rows(1, key_rows[g][d][1])
+                k.repr = repr.ntt
+                digits.append(k)
+            sets.append(MLWE_Set([digits]))
+        ksks = MLWE_Set.flatten_array(sets)
+        out = MLWE(s, lvl=0)
+        R.lib.mlwe_trace(out.obj, c.obj, ksks.obj, 0)
+        R.engine.check("mlwe_trace")
+        outs.append(np.stack([out.component_rows(0), out.component_rows(1)]))
+    assert np.array_equal(outs[0], outs[1])

@@ -875,10 +875,72 @@ void mgsw_NCMUX(void* out, void* in1, void* in2, void* mgsw, void* ksk, uint64_t
 }
 
 // ------------------------------------------------------------------ packing (composite)
+// Packing of `size` LWE samples into one MLWE (mlwe_full_packing_keyswitch, mlwe.c:343-430):
+// out = sum over mask coefficients i of -(the polynomial of the samples' i-th mask
+// entries, one coefficient per sample) lifted per limb and times ksk[i][limb], computed
+// over the extended limbs of the key, then divided down to the output's limbs, plus
+// the polynomial of the bodies.  The same sequence of engine operations as the
+// reference, each on the GPU.
 void mlwe_full_packing_keyswitch(void* out, void* in, uint64_t size, void* ksk, uint64_t lvl) {
     VC_ENTER("mlwe_full_packing_keyswitch");
-    (void)out; (void)in; (void)size; (void)ksk; (void)lvl;
-    set_error(vc_where_, "LWE-to-MLWE packing key switch is not part of the cuda engine");
+    (void)lvl;
+    RNS_MLWE o = as_mlwe(out);
+    LWE* lw = (LWE*)in;
+    RNS_MLWE** K = (RNS_MLWE**)ksk;
+    if (!o || !lw || !K || size == 0 || !lw[0]) {
+        set_error(vc_where_, "null output, samples or keys, or no samples");
+        return;
+    }
+    const uint64_t N = o->b->ntt->N, in_n = lw[0]->n, lwe_l = lw[0]->l;
+    if (size > N) {
+        set_error(vc_where_, "more samples than ring coefficients");
+        return;
+    }
+    const uint64_t target = o->b->rns_mask, extended = K[0][0]->b->rns_mask;
+    const uint64_t divide = extended & ~target;
+    // pool index of the limb-th active limb of the target mask
+    std::vector<uint64_t> active;
+    for (uint64_t j = 0; j < 64; ++j)
+        if ((target >> j) & 1) active.push_back(j);
+    if (active.size() < lwe_l) {
+        set_error(vc_where_, "the output has fewer limbs than the samples");
+        return;
+    }
+    for (uint64_t k = 0; k < o->r; ++k) o->a[k]->rns_mask = extended;
+    o->b->rns_mask = extended;
+    mlwe_RNS_trivial_sample_of_zero(out);
+    IncNtt* t = pool(o);
+    void* tmp = polynomial_new_RNS_polynomial(N, target, t);
+    void* tmp_red = polynomial_new_RNS_polynomial(N, extended, t);
+    void* tmp_rns = polynomial_new_RNS_polynomial(N, extended, t);
+    RNS_Polynomial tp = (RNS_Polynomial)tmp;
+    for (uint64_t i = 0; i < in_n; ++i) {
+        vc::sync(vc_where_);  // the rows are written from the host below
+        for (uint64_t j : active) memset(tp->coeffs[j], 0, N * sizeof(uint64_t));
+        for (uint64_t limb = 0; limb < lwe_l; ++limb)
+            for (uint64_t k = 0; k < size; ++k) tp->coeffs[active[limb]][k] = lw[k]->a[limb][i];
+        uint64_t idx = 0;
+        for (uint64_t j : active) {
+            polynomial_RNSc_mod_reduce_lifted(tmp_red, tmp, j);
+            polynomial_RNSc_to_RNS(tmp_rns, tmp_red);
+            mlwe_RNS_mul_subto_by_poly(out, K[i][idx++], tmp_rns);
+        }
+    }
+    vc::sync(vc_where_);
+    for (uint64_t j : active) memset(tp->coeffs[j], 0, N * sizeof(uint64_t));
+    for (uint64_t limb = 0; limb < lwe_l; ++limb)
+        for (uint64_t k = 0; k < size; ++k) tp->coeffs[active[limb]][k] = lw[k]->b[limb];
+    mlwe_RNS_to_RNSc(out, out);
+    if (divide) {
+        for (uint64_t j = 0; j < o->r; ++j) polynomial_round_division_RNSc_wo_free(o->a[j], divide);
+        polynomial_round_division_RNSc_wo_free(o->b, divide);
+    }
+    polynomial_add_RNSc_polynomial(o->b, o->b, tmp);
+    mlwe_RNSc_to_RNS(out, out);
+    free_RNS_polynomial(tmp);
+    free_RNS_polynomial(tmp_red);
+    free_RNS_polynomial(tmp_rns);
+    VC_FINISH();
 }
 
 static void packing_rec(RNS_MLWE* vec, uint64_t ell, RNS_MLWE*** ksks, uint64_t lvl) {
