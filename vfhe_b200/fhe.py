@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import math
 
-from .arith import Polynomial, Ring, repr
+from .arith import Polynomial, Ring, ntt_processor, repr
 from .complex import ComplexPolynomial, ComplexRing
 from .mlwe import CMUX, LWE, MGSW_Scheme, MLWE, MLWE_Key, MLWE_Scheme, MLWE_Set
 from .numbers import crt
@@ -93,11 +93,36 @@ class CKKS_Scheme(MLWE_Scheme):
         assert lvl + 1 < len(self.rings), "no lower level to rescale into"
         nxt = self.rings[lvl + 1]
         if not nxt.is_quotient_ring(ciphertext.ring):
-            raise NotImplementedError("non-nested level chains need rational rescaling")
+            return self.rational_rescale(ciphertext)
         dropped = math.prod(p for p in ciphertext.ring.primes if p not in nxt.primes)
         ciphertext.round_division(lvl=lvl + 1)
         ciphertext.delta = ciphertext.delta / dropped
         return ciphertext
+
+    def rational_rescale(self, ct):
+        """Rescale level lvl -> lvl + 1 when the next level is not a quotient of this one
+        (reference ckks.py:150-202): each component is scaled and lifted into the union
+        of both levels' primes (polynomial_RNSc_scaled_lift), then round-divided by the
+        primes the next level drops; delta changes by prod(new) / prod(dropped)."""
+        level = ct.lvl
+        assert level < len(self.rings) - 1, "cannot rescale a ciphertext at the last level"
+        start, end = ct.ring, self.rings[level + 1]
+        pmap = ntt_processor(self.ring.engine).prime_to_index[(self.ring.N, self.ring.split_degree)]
+        union = sorted(set(start.primes + end.primes), key=lambda p: pmap[p])
+        union_ring = Ring(self.ring.N, primes=union, prime_size=[math.ceil(math.log2(p)) for p in union],
+                          split_degree=self.ring.split_degree, engine=self.ring.engine)
+        res = CKKS_Ciphertext(self, lvl=level + 1)
+        for i in range(self.r):
+            a = ct.get_a_poly(i).scaled_lift(union_ring).round_division(end)
+            self.ring.lib.polynomial_copy_RNS_polynomial(res.obj_a_i(i), a.obj)
+        b = ct.get_b_poly().scaled_lift(union_ring).round_division(end)
+        self.ring.lib.polynomial_copy_RNS_polynomial(res.obj_b(), b.obj)
+        self.ring.engine.check("rational_rescale")
+        p_val = math.prod(p for p in end.primes if p not in start.primes)
+        q_val = math.prod(q for q in start.primes if q not in end.primes)
+        res.delta = ct.delta * p_val / q_val
+        res.repr = repr.coeff
+        return res
 
 
 class CKKS_Ciphertext(MLWE):
