@@ -143,3 +143,83 @@ def test_trace_matches_reference_library(cuda, ref_portable):
         R.engine.check("mlwe_trace")
         outs.append(np.stack([out.component_rows(0), out.component_rows(1)]))
     assert np.array_equal(outs[0], outs[1])
+
+
+def _mlwe_rows(rng, primes, N, count):
+    return [np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in primes]) for _ in range(2)])
+            for _ in range(count)]
+
+
+def _mlwe_array(s, ring, rows, rep):
+    """An engine-side RNS_MLWE* array (MGSW layout) from [2][limbs][N] row sets."""
+    from vfhe_b200.mlwe import MLWE
+
+    objs = []
+    for r in rows:
+        m = MLWE(s, ring=ring)
+        m.set_component_rows(0, r[0])
+        m.set_component_rows(1, r[1])
+        m.repr = rep
+        objs.append(m)
+    tmp = ring.ffi.new("void*[]", [m.obj for m in objs])
+    arr = ring.lib.mlwe_create_copy_array(tmp, len(objs))
+    return arr, objs
+
+
+def test_gp25_steps_match_reference_library(cuda, ref_portable):
+    """GP25's C steps (gp25.c:68-336): the RGSW monomial multiply (NCMUX/CMUX rounds
+    over the accumulators) and sub_a (rotate, external product with the sign key,
+    add) on the cuda engine and on the reference's own library, same inputs: the same
+    accumulators, residue for residue."""
+    from tests.helpers import twin_rings
+    from vfhe_b200.arith import repr
+    from vfhe_b200.mlwe import MLWE, MLWE_Scheme, MLWE_Set
+
+    N, in_N, r_prec, ell = 256, 4, 2, 2
+    rng = np.random.default_rng(47)
+    rings = twin_rings([cuda, ref_portable], N, [50, 50, 50], split=1)
+    primes = rings[0].primes
+    acc_rows = _mlwe_rows(rng, primes[:2], N, in_N)
+    e_rows = [_mlwe_rows(rng, primes, N, 2 * ell) for _ in range(r_prec)]
+    k_rows = _mlwe_rows(rng, primes, N, ell)
+    sign_rows = _mlwe_rows(rng, primes, N, 2 * ell)
+    rots = [int(v) for v in rng.integers(0, 2 * N, in_N)]
+    results = []
+    for R in rings:
+        s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
+        sr = s.special_rings[0]
+        outs = []
+        for step in ("monomial", "sub_a"):
+            accs = []
+            for rows in acc_rows:
+                m = MLWE(s, lvl=0)
+                m.set_component_rows(0, rows[0])
+                m.set_component_rows(1, rows[1])
+                m.repr = repr.coeff
+                accs.append(m)
+            p0 = R.ffi.new("void*[]", [m.obj for m in accs])
+            keep = []
+            if step == "monomial":
+                es = [_mlwe_array(s, sr, rows, repr.ntt) for rows in e_rows]
+                keep += es
+                e = R.ffi.new("void*[]", [a for a, _ in es])
+                digits = []
+                for rows in k_rows:
+                    k = MLWE(s, ring=sr)
+                    k.set_component_rows(0, rows[0])
+                    k.set_component_rows(1, rows[1])
+                    k.repr = repr.ntt
+                    digits.append(k)
+                ksk = MLWE_Set([digits])
+                keep.append(ksk)
+                R.lib.gp25_RGSW_monomial_mul(p0, in_N, e, r_prec, ksk.obj, ell, 1)
+                R.engine.check("gp25_RGSW_monomial_mul")
+            else:
+                sign, objs = _mlwe_array(s, sr, sign_rows, repr.ntt)
+                keep.append(objs)
+                R.lib.gp25_sub_a_mt(p0, in_N, R.ffi.new("uint64_t[]", rots), sign, ell, 1, N, 1)
+                R.engine.check("gp25_sub_a_mt")
+            outs.append(np.stack([np.stack([m.component_rows(0), m.component_rows(1)]) for m in accs]))
+        results.append(outs)
+    for got, want in zip(results[0], results[1]):
+        assert np.array_equal(got, want)

@@ -229,21 +229,4 @@ void field_base_conversion(uint64_t* out, const uint64_t* in, uint64_t source_co
 void ntt_free_proc(void* proc) { (void)proc; }
 uint64_t inverse_mod_eea(uint64_t a, uint64_t p) { return p ? host_inv_mod(a % p, p) : 0; }
 
-// ---- GP25
-void gp25_RGSW_monomial_mul(void* p0, uint64_t in_N, void* e, uint64_t r_prec, void* ksk, uint64_t ell,
-                            uint64_t special_primes) {
-    (void)p0; (void)in_N; (void)e; (void)r_prec; (void)ksk; (void)ell; (void)special_primes;
-    unsupported("gp25_RGSW_monomial_mul");
-}
-void gp25_RGSW_monomial_mul_mt(void* p0, uint64_t in_N, void* e, uint64_t r_prec, void* ksk, uint64_t ell,
-                               uint64_t special_primes, uint64_t num_threads) {
-    (void)p0; (void)in_N; (void)e; (void)r_prec; (void)ksk; (void)ell; (void)special_primes; (void)num_threads;
-    unsupported("gp25_RGSW_monomial_mul_mt");
-}
-void gp25_sub_a_mt(void* p0, uint64_t in_N, uint64_t* a, void* s_sign, uint64_t ell, uint64_t special_primes,
-                   uint64_t N, uint64_t num_threads) {
-    (void)p0; (void)in_N; (void)a; (void)s_sign; (void)ell; (void)special_primes; (void)N; (void)num_threads;
-    unsupported("gp25_sub_a_mt");
-}
-
 }  // extern "C"

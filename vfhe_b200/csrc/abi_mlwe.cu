@@ -976,4 +976,102 @@ void mlwe_full_packing_keyswitch_scaled(void* vec, uint64_t ell, void* ksks, uin
     VC_FINISH();
 }
 
+// ------------------------------------------------------------------ GP25 (composite)
+// GP25's sparse-amortised bootstrap steps (modules/fhe/c/src/gp25.c:68-336) as the same
+// sequence of engine operations, each on the GPU.  The reference's thread count is
+// a CPU work split and does not change results; the _mt entry points take it and run
+// the single sequence.
+
+// out = ExtProd(mgsw, in2 - in1) to the coefficient domain, + in1 (mgsw_CMUX_to_coeff,
+// modules/mlwe/c/src/mgsw.c:103-119: equal to CMUX followed by an inverse transform).
+static void cmux_to_coeff(void* out, void* in1, void* in2, void* mgsw, uint64_t ell, uint64_t sp) {
+    RNS_MLWE a = as_mlwe(in1);
+    RNS_MLWE diff = new_mlwe(a->b->ntt->N, a->r, a->b->rns_mask, pool(a));
+    mlwe_sub_RNSc_sample(diff, in2, in1);
+    mgsw_external_product(out, mgsw, diff, ell, sp);
+    mlwe_RNS_to_RNSc(out, out);
+    mlwe_add_RNSc_sample(out, out, in1);
+    del_mlwe(diff);
+}
+
+// CMUX with in2 first mapped by X -> X^(2N-1) (mgsw_NCMUX_to_coeff, mgsw.c:121-136).
+static void ncmux_to_coeff(void* out, void* in1, void* in2, void* mgsw, void* ksk, uint64_t ell, uint64_t sp) {
+    RNS_MLWE a = as_mlwe(in1);
+    const uint64_t N = a->b->ntt->N;
+    RNS_MLWE tmp = new_mlwe(N, a->r, a->b->rns_mask, pool(a));
+    mlwe_automorphism_RNSc_GHS(tmp, in2, 2 * N - 1, ksk, ell);
+    cmux_to_coeff(out, in1, tmp, mgsw, ell, sp);
+    del_mlwe(tmp);
+}
+
+// gp25_RGSW_monomial_mul (gp25.c:68-128): r_prec rounds of (N)CMUXes over the in_N
+// accumulators, ping-ponging between p0 and a scratch array.
+void gp25_RGSW_monomial_mul(void* p0v, uint64_t in_N, void* ev, uint64_t r_prec, void* ksk, uint64_t ell,
+                            uint64_t special_primes) {
+    VC_ENTER("gp25_RGSW_monomial_mul");
+    RNS_MLWE* p0 = (RNS_MLWE*)p0v;
+    RNS_MLWE* e = (RNS_MLWE*)ev;
+    if (!p0 || !e || in_N == 0) {
+        set_error(vc_where_, "null accumulators or keys");
+        return;
+    }
+    const uint64_t N = p0[0]->b->ntt->N, r = p0[0]->r, mask = p0[0]->b->rns_mask;
+    std::vector<RNS_MLWE> p1(in_N);
+    for (uint64_t i = 0; i < in_N; ++i) p1[i] = new_mlwe(N, r, mask, pool(p0[0]));
+    RNS_MLWE* p[2] = {p0, p1.data()};
+    for (uint64_t i = 0; i < r_prec; ++i) {
+        const uint64_t power = 1ULL << i;
+        const uint64_t out_idx = (i + 1) & 1, in_idx = out_idx ^ 1;
+        const void* ei = ((void* const*)e)[i];
+        for (uint64_t j = 0; j < power; ++j)
+            ncmux_to_coeff(p[out_idx][j], p[in_idx][j], p[in_idx][in_N - power + j], (void*)ei, ksk, ell,
+                           special_primes);
+        for (uint64_t j = 0; j + power < in_N; ++j)
+            cmux_to_coeff(p[out_idx][j + power], p[in_idx][j + power], p[in_idx][j], (void*)ei, ell,
+                          special_primes);
+    }
+    if (r_prec & 1)
+        for (uint64_t i = 0; i < in_N; ++i) mlwe_copy_RNS_sample(p0[i], p1[i]);
+    for (uint64_t i = 0; i < in_N; ++i) del_mlwe(p1[i]);
+    VC_FINISH();
+}
+
+void gp25_RGSW_monomial_mul_mt(void* p0, uint64_t in_N, void* e, uint64_t r_prec, void* ksk, uint64_t ell,
+                               uint64_t special_primes, uint64_t num_threads) {
+    (void)num_threads;
+    gp25_RGSW_monomial_mul(p0, in_N, e, r_prec, ksk, ell, special_primes);
+}
+
+// gp25_sub_a_mt (gp25.c:278-336): p[k] <- p[k] X^a_k + s_sign (x) (p[k] X^a_k (X^(-2 a_k) - 1)).
+void gp25_sub_a_mt(void* p0v, uint64_t in_N, uint64_t* a, void* s_sign, uint64_t ell, uint64_t special_primes,
+                   uint64_t N, uint64_t num_threads) {
+    VC_ENTER("gp25_sub_a_mt");
+    (void)num_threads;
+    RNS_MLWE* p0 = (RNS_MLWE*)p0v;
+    if (!p0 || !a || !s_sign || in_N == 0) {
+        set_error(vc_where_, "null accumulators, rotations or key");
+        return;
+    }
+    const uint64_t twoN = 2 * N, r = p0[0]->r, mask = p0[0]->b->rns_mask;
+    IncNtt* t = pool(p0[0]);
+    RNS_MLWE pax = new_mlwe(N, r, mask, t), tmp = new_mlwe(N, r, mask, t);
+    RNS_MLWE ext = new_mlwe(N, r, mask, t), pax_ntt = new_mlwe(N, r, mask, t);
+    for (uint64_t k = 0; k < in_N; ++k) {
+        mlwe_RNSc_mul_by_xai(pax, p0[k], a[k]);
+        const uint64_t m2a = (twoN - (2 * a[k]) % twoN) % twoN;
+        mlwe_RNSc_mul_by_xai_minus1(tmp, pax, m2a);
+        mgsw_external_product(ext, s_sign, tmp, ell, special_primes);
+        mlwe_copy_RNS_sample(pax_ntt, pax);
+        mlwe_RNSc_to_RNS(pax_ntt, pax_ntt);
+        for (uint64_t i = 0; i < r; ++i) polynomial_add_RNS_polynomial(ext->a[i], ext->a[i], pax_ntt->a[i]);
+        polynomial_add_RNS_polynomial(ext->b, ext->b, pax_ntt->b);
+        mlwe_RNS_to_RNSc(p0[k], ext);
+    }
+    del_mlwe(pax);
+    del_mlwe(tmp);
+    del_mlwe(ext);
+    del_mlwe(pax_ntt);
+    VC_FINISH();
+}
+
 }  // extern "C"
