@@ -500,7 +500,8 @@ def serving_leg(eng, requests: int, rates=(50.0, 200.0, 1000.0)) -> dict:
     budget = 160 * 10**9
     out = {"budget_bytes": budget, "resident_bytes": mix.resident, "requests_per_rate": requests,
            "mix": "90% CKKS (half mul+relin+rescale, half rotate) over (2^13,4),(2^14,9),(2^15,16),(2^16,24); "
-                  "10% CGGI16 batches of 1..1024 LWEs (log-uniform), n=630, N=1024",
+                  "10% CGGI16 programmable bootstraps, batches of 1..1024 LWEs (log-uniform), n=630, N=1024, "
+                  "gadget 2^7 x 3, key switch 2^2 x 8 (torus FP64-FFT path)",
            "rates": []}
     reqs = mix.requests(requests, seed=SEED + 6, ckks_share=0.9)
     p = mix.ckks[1]
@@ -511,8 +512,8 @@ def serving_leg(eng, requests: int, rates=(50.0, 200.0, 1000.0)) -> dict:
         srv = Server(budget, streams=streams, max_batch=mb, engine=eng)
         mix.register(srv)
         srv.reserve(16 * 10**9 if mb > 1 else 2 * 10**9)
-        # warm-up: every CGGI batch-size bucket once (captures its blind-rotation
-        # graph), a short mixed stream and a short multiply burst
+        # warm-up: every CGGI batch-size bucket once, a short mixed stream and a short
+        # multiply burst
         for k in range(11):
             run_stream(mix, srv, [("cggi", -1, 1 << k, 0)], np.zeros(1))
         run_stream(mix, srv, reqs[:24], np.zeros(24))

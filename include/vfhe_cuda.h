@@ -513,6 +513,16 @@ int64_t vfhe_cuda_server_submit_ckks_rotate(void *server, int cls, uint64_t *d_o
                                             uint64_t gen, const uint64_t *d_gk);
 int64_t vfhe_cuda_server_submit_cggi(void *server, int cls, uint64_t *d_out_a, uint64_t *d_out_b,
                                      const uint64_t *d_in_a, const uint64_t *d_in_b, uint64_t count);
+/* Torus CGGI classes (the FP64-FFT programmable bootstrap with the key switch back to
+ * the input key; vfhe_cuda_cggi_fft_bootstrap_batch + _keyswitch_batch): keys are
+ * device-resident (spectra, LUT test vector, key-switching key), requests carry
+ * `count` uint32 LWEs [count][n+1] in and out.  Class ids share the CGGI list. */
+int vfhe_cuda_server_torus_class(void *server, const double *d_bsk_f, const uint32_t *d_tv,
+                                 const uint32_t *d_ksk, uint32_t n, uint32_t N, uint32_t bs_base_log,
+                                 uint32_t bs_levels, uint32_t ks_base_log, uint32_t ks_levels,
+                                 uint32_t torus_base, uint32_t max_count);
+int64_t vfhe_cuda_server_submit_torus(void *server, int cls, uint32_t *d_out, const uint32_t *d_in,
+                                      uint64_t count);
 int vfhe_cuda_server_wait(void *server, int64_t id, double *latency_ms);
 int vfhe_cuda_server_stats(void *server, uint64_t *out5);
 

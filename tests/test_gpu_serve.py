@@ -10,18 +10,21 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _mix(cuda):
+def _mix(cuda, kind="rns"):
     from vfhe_b200.serve import ServingMix
 
-    return ServingMix(cuda, ckks=((2**12, 4), (2**13, 5)), cggi=(256, 16), cggi_max=16, pool=2, gens=2, seed=3)
+    cggi = (256, 16) if kind == "rns" else (512, 32)
+    return ServingMix(cuda, ckks=((2**12, 4), (2**13, 5)), cggi=cggi, cggi_max=16, pool=2, gens=2, seed=3,
+                      cggi_kind=kind)
 
 
-def test_results_identical_alone_and_in_mix(cuda):
+@pytest.mark.parametrize("kind", ["rns", "torus"])
+def test_results_identical_alone_and_in_mix(cuda, kind):
     import torch
 
     from vfhe_b200.serve import Server, poisson_arrivals, run_stream
 
-    mix = _mix(cuda)
+    mix = _mix(cuda, kind)
     reqs = mix.requests(48, seed=1, ckks_share=0.75, cggi_counts=(1, 16))
     assert {r[0] for r in reqs} == {"mul", "rot", "cggi"}
 
@@ -109,3 +112,26 @@ def test_budget_limits_admission(cuda):
         srv.wait(rid)
     cuda.lib.vfhe_cuda_clear_error()
     srv.close()
+
+
+def test_torus_requests_equal_direct_bootstraps_and_decrypt(cuda):
+    """Torus CGGI requests served in a mix equal the direct programmable bootstrap of
+    the same LWEs, and decrypt to the lookup table's values."""
+    import torch
+
+    from vfhe_b200.cggi_fft import to_host
+    from vfhe_b200.serve import Server, run_stream
+
+    mix = _mix(cuda, "torus")
+    reqs = [r for r in mix.requests(30, seed=9, ckks_share=0.5, cggi_counts=(1, 16)) if r[0] == "cggi"]
+    assert reqs
+    srv = Server(8 << 30, streams=2, max_batch=4, engine=cuda)
+    mix.register(srv)
+    res = run_stream(mix, srv, reqs, np.zeros(len(reqs)), keep_outputs=True)
+    srv.close()
+    cg = mix.cggi
+    for (kind, pi, x, y), outs in zip(reqs, res["outputs"]):
+        want = cg.dev.bootstrap(cg.lwe[y:y + x], cg.tv)
+        torch.cuda.synchronize()
+        assert torch.equal(outs[0], want)
+        assert np.array_equal(cg.keys.decrypt(to_host(outs[0])), cg.lut[cg.msgs[y:y + x]])

@@ -81,6 +81,16 @@ struct CggiClass {
     uint64_t* out_a = nullptr;  // [bmax][L0][N]
     uint64_t* out_b = nullptr;  // [bmax][L0]
     bool busy = false;
+    // torus classes (FP64-FFT programmable bootstrap, then key switch back to n):
+    // uint32 LWEs [bmax][n+1] in, extracted [bmax][N+1], [bmax][n+1] out; no padding
+    bool torus = false;
+    uint32_t N = 0, bs_base_log = 0, bs_levels = 0, ks_base_log = 0, ks_levels = 0;
+    const double* bsk_f = nullptr;
+    const uint32_t* tv32 = nullptr;
+    const uint32_t* ksk = nullptr;
+    uint32_t* t_in = nullptr;
+    uint32_t* t_mid = nullptr;
+    uint32_t* t_out = nullptr;
 };
 
 struct Request {
@@ -201,7 +211,29 @@ bool Server::launch(Batch* b) {
     cudaStream_t st = streams[b->stream];
     const uint64_t B = b->reqs.size();
     int err = 0;
-    if (b->kind == kCggi) {
+    if (b->kind == kCggi && cggi[b->cls].torus) {
+        CggiClass& g = cggi[b->cls];
+        const uint64_t n1 = g.n + 1;
+        uint64_t total = 0;
+        for (Request* r : b->reqs) {
+            err = err ? err : cudaMemcpyAsync(g.t_in + total * n1, r->in1, r->count * n1 * 4, cudaMemcpyDeviceToDevice,
+                                              st);
+            total += r->count;
+        }
+        if (!err && vfhe_cuda_cggi_fft_bootstrap_batch(g.t_mid, g.t_in, total, g.bsk_f, g.tv32, g.n, g.N,
+                                                       g.bs_base_log, g.bs_levels, (uint32_t)g.torus_base, st))
+            err = -1;
+        if (!err && vfhe_cuda_cggi_fft_keyswitch_batch(g.t_out, g.t_mid, total, g.ksk, g.N, g.n, g.ks_base_log,
+                                                       g.ks_levels, st))
+            err = -1;
+        total = 0;
+        for (Request* r : b->reqs) {
+            if (!err) err = cudaMemcpyAsync(r->out, g.t_out + total * n1, r->count * n1 * 4, cudaMemcpyDeviceToDevice,
+                                            st);
+            total += r->count;
+        }
+        g.busy = true;
+    } else if (b->kind == kCggi) {
         CggiClass& g = cggi[b->cls];
         const uint64_t N = g.t->pub.N, L0 = g.L0, n = g.n;
         uint64_t total = 0;
@@ -481,6 +513,9 @@ void vfhe_cuda_server_free(void* sv) {
         cudaFree(g.in_b);
         cudaFree(g.out_a);
         cudaFree(g.out_b);
+        cudaFree(g.t_in);
+        cudaFree(g.t_mid);
+        cudaFree(g.t_out);
     }
     for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
     if (s->pool) cudaMemPoolDestroy(s->pool);
@@ -558,6 +593,52 @@ int vfhe_cuda_server_cggi_class(void* sv, void* ntt, const uint32_t* limbs, uint
     g.out_b = (uint64_t*)p4;
     std::lock_guard<std::mutex> lk(s->mu);
     s->used += ws + io;
+    s->cggi.push_back(g);
+    return (int)s->cggi.size() - 1;
+}
+
+// Torus CGGI class: programmable bootstraps with the FP64-FFT kernel and the key
+// switch back to the input key (vfhe_cuda_cggi_fft_bootstrap_batch, _keyswitch_batch);
+// keys stay where the caller put them.  Class ids share the CGGI class list.
+int vfhe_cuda_server_torus_class(void* sv, const double* d_bsk_f, const uint32_t* d_tv, const uint32_t* d_ksk,
+                                 uint32_t n, uint32_t N, uint32_t bs_base_log, uint32_t bs_levels, uint32_t ks_base_log,
+                                 uint32_t ks_levels, uint32_t torus_base, uint32_t max_count) {
+    Server* s = (Server*)sv;
+    if (!s || !d_bsk_f || !d_tv || !d_ksk || n == 0 || N == 0 || max_count == 0 || max_count > (1u << 20) ||
+        torus_base == 0) {
+        vc::set_error("vfhe_cuda_server_torus_class", "bad keys, n, N, torus base or max_count (1..2^20)");
+        return -1;
+    }
+    vc::CggiClass g;
+    memset(g.limbs, 0, sizeof g.limbs);
+    g.t = nullptr;
+    g.torus = true;
+    g.n = n;
+    g.N = N;
+    g.bs_base_log = bs_base_log;
+    g.bs_levels = bs_levels;
+    g.ks_base_log = ks_base_log;
+    g.ks_levels = ks_levels;
+    g.torus_base = torus_base;
+    g.bsk_f = d_bsk_f;
+    g.tv32 = d_tv;
+    g.ksk = d_ksk;
+    g.bmax = max_count;
+    const uint64_t io = 4ULL * max_count * (2ULL * (n + 1) + N + 1);
+    void *p0 = nullptr, *p1 = nullptr, *p2 = nullptr;
+    if (cudaMalloc(&p0, 4ULL * max_count * (n + 1)) || cudaMalloc(&p1, 4ULL * max_count * (N + 1)) ||
+        cudaMalloc(&p2, 4ULL * max_count * (n + 1))) {
+        cudaFree(p0);
+        cudaFree(p1);
+        cudaFree(p2);
+        vc::set_error("vfhe_cuda_server_torus_class", "cudaMalloc of the class buffers failed");
+        return -1;
+    }
+    g.t_in = (uint32_t*)p0;
+    g.t_mid = (uint32_t*)p1;
+    g.t_out = (uint32_t*)p2;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->used += io;
     s->cggi.push_back(g);
     return (int)s->cggi.size() - 1;
 }
@@ -646,6 +727,22 @@ int64_t vfhe_cuda_server_submit_cggi(void* sv, int cls, uint64_t* d_out_a, uint6
     r->out_b = d_out_b;
     r->in1 = d_in_a;
     r->in2 = d_in_b;
+    r->count = count;
+    return submit(s, r);
+}
+
+// Torus bootstrap of `count` LWEs d_in [count][n+1] (uint32, mask then body) into
+// d_out [count][n+1] under the same key, through a torus class.
+int64_t vfhe_cuda_server_submit_torus(void* sv, int cls, uint32_t* d_out, const uint32_t* d_in, uint64_t count) {
+    Server* s = (Server*)sv;
+    if (!s || cls < 0 || cls >= (int)s->cggi.size() || !s->cggi[cls].torus || count == 0 ||
+        count > s->cggi[cls].bmax)
+        return -1;
+    vc::Request* r = new vc::Request();
+    r->kind = vc::kCggi;
+    r->cls = cls;
+    r->out = (uint64_t*)d_out;
+    r->in1 = (const uint64_t*)d_in;
     r->count = count;
     return submit(s, r);
 }

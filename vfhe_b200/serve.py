@@ -64,6 +64,25 @@ class Server:
         self._keep += [bk, tv]
         return c
 
+    def torus_class(self, dev, tv: torch.Tensor, max_count: int) -> int:
+        """A torus CGGI class over the device keys of a CggiFft (programmable bootstrap
+        through the test vector tv, key switch back to the LWE key)."""
+        p = dev.params
+        c = self.lib.vfhe_cuda_server_torus_class(
+            self.handle, self.ffi.cast("double*", dev.bsk_f.data_ptr()), self.ffi.cast("uint32_t*", tv.data_ptr()),
+            self.ffi.cast("uint32_t*", dev.ksk.data_ptr()), p.n, p.N, p.bs_base_log, p.bs_levels, p.ks_base_log,
+            p.ks_levels, p.t, max_count)
+        if c < 0:
+            self.engine.check("server_torus_class")
+            raise EngineError("server_torus_class")
+        self._keep += [dev, tv]
+        return c
+
+    def submit_torus(self, cls: int, out: torch.Tensor, lwe: torch.Tensor) -> int:
+        return self._ok(self.lib.vfhe_cuda_server_submit_torus(self.handle, cls, self.ffi.cast("uint32_t*", out.data_ptr()),
+                                                               self.ffi.cast("uint32_t*", lwe.data_ptr()),
+                                                               lwe.shape[0]))
+
     def submit_mul(self, cls: int, out: torch.Tensor, ct1: torch.Tensor, ct2: torch.Tensor) -> int:
         return self._ok(self.lib.vfhe_cuda_server_submit_ckks_mul(self.handle, cls, _p(self.ffi, out),
                                                                   _p(self.ffi, ct1), _p(self.ffi, ct2)))
@@ -147,13 +166,15 @@ class CggiParams:
 
 class ServingMix:
     """Synthetic serving setup: CKKS parameter classes (N, L) with a relinearisation key,
-    Galois keys and a pool of input ciphertexts each, and one CGGI class (RNS gadget,
-    N_cggi, LWE dimension n) with a bootstrapping key and a pool of LWE inputs; every
-    residue uniform from a seeded generator (keys are resident in HBM, not derived from
-    a secret: throughput and latency do not depend on key values)."""
+    Galois keys and a pool of input ciphertexts each (every residue uniform from a seeded
+    generator: throughput and latency do not depend on key values), and one CGGI class
+    with a pool of LWE inputs.  cggi_kind "torus" (the CGGI16 parameter set: n, N,
+    gadget 2^7 x 3, key switch 2^2 x 8) uses real keys and encryptions of random 4-bit
+    messages; "rns" uses the RNS-gadget CGGI16 with uniform key material."""
 
     def __init__(self, engine: Engine, ckks=((2**13, 4), (2**14, 9), (2**15, 16), (2**16, 24)),
-                 cggi=(1024, 630), cggi_max=1024, pool: int = 4, gens: int = 2, seed: int = 7, with_cggi=True):
+                 cggi=(1024, 630), cggi_max=1024, pool: int = 4, gens: int = 2, seed: int = 7, with_cggi=True,
+                 cggi_kind: str = "torus"):
         from .arith import Ring
 
         self.engine = engine
@@ -183,7 +204,25 @@ class ServingMix:
             p.special = R.prime_indices[L]
             self.ckks.append(p)
         self.cggi = None
-        if with_cggi:
+        self.cggi_kind = cggi_kind
+        if with_cggi and cggi_kind == "torus":
+            from .cggi_fft import CggiFft, TorusKeys, TorusParams, test_vector
+            from .cggi_fft import to_device as to_device32
+
+            N, n = cggi
+            tp = TorusParams(n=n, N=N)
+            keys = TorusKeys.generate(tp, self.rng)
+            cg = CggiParams(N, n)
+            cg.dev = CggiFft(keys, engine)
+            cg.lut = self.rng.integers(0, tp.t, tp.t)
+            cg.tv = to_device32(test_vector(cg.lut, tp))
+            cg.msgs = self.rng.integers(0, tp.t, cggi_max)
+            cg.lwe = to_device32(keys.encrypt(cg.msgs, self.rng))
+            cg.keys = keys
+            cg.max = cggi_max
+            self.resident += cg.dev.bsk_f.numel() * 8 + cg.dev.ksk.numel() * 4 + cg.lwe.numel() * 4
+            self.cggi = cg
+        elif with_cggi:
             N, n = cggi
             Rc = Ring(N, prime_size=[50, 50, 50], split_degree=1, engine=engine)
             q = Rc.primes
@@ -204,7 +243,10 @@ class ServingMix:
             _, ring_L, ring_R = p.ring
             p.mul_cls = server.ckks_class(ring_L, p.special, p.rlk)
             p.rot_cls = server.ckks_class(ring_R, p.special, None)
-        if self.cggi is not None:
+        if self.cggi is not None and self.cggi_kind == "torus":
+            cg = self.cggi
+            cg.cls = server.torus_class(cg.dev, cg.tv, cg.max)
+        elif self.cggi is not None:
             cg = self.cggi
             cg.cls = server.cggi_class(cg.ring, cg.special, cg.n, cg.bk, cg.tv, 16, cg.max)
 
@@ -236,6 +278,8 @@ class ServingMix:
             p = self.ckks[pi]
             return (torch.empty((2, p.L - 1, p.N), dtype=torch.int64, device="cuda"),)
         cg = self.cggi
+        if self.cggi_kind == "torus":
+            return (torch.empty((x, cg.n + 1), dtype=torch.int32, device="cuda"),)
         return (torch.empty((x, 2, cg.N), dtype=torch.int64, device="cuda"),
                 torch.empty((x, 2), dtype=torch.int64, device="cuda"))
 
@@ -248,6 +292,8 @@ class ServingMix:
             p = self.ckks[pi]
             return server.submit_rotate(p.rot_cls, outs[0], p.rcts[x], y, p.gks[y])
         cg = self.cggi
+        if self.cggi_kind == "torus":
+            return server.submit_torus(cg.cls, outs[0], cg.lwe[y:y + x])
         return server.submit_cggi(cg.cls, outs[0], outs[1], cg.a[y:y + x], cg.b[y:y + x])
 
 
