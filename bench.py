@@ -11,7 +11,9 @@ from fixed seeds.
 
 Prints one JSON line (rank 0).  ``value`` is pairs per second over all ranks with
 ciphertexts already in HBM; ``e2e`` adds the host->device copy of each step's input
-ciphertexts from pinned memory and the device->host copy of its results.  The
+ciphertexts from pinned memory and the device->host copy of its results, moved in the
+compact wire format (residues at their primes' bit lengths; plain uint64 rows timed
+beside it).  The
 reference arm runs the reference's own CPU library (built from its sources into
 oracle/_ref/) on the same workload, one process per host core.
 """
@@ -616,11 +618,24 @@ def run_cuda_arm(args) -> None:
     # ---- end to end: pinned host inputs in, host results out, every step.  Steps are
     # pipelined over two buffer sets and three streams (copy in, compute, copy out), as
     # a caller of the batched API would run them: step i's inputs travel while step i-1
-    # computes and step i-2's results travel back.
+    # computes and step i-2's results travel back.  The headline figure moves the
+    # ciphertexts in the compact wire format (WireFormat: each residue at its prime's
+    # bit length, unpacked and packed on the GPU inside the step); the plain uint64
+    # transport is timed beside it.
+    from vfhe_b200.batch import WireFormat
+
+    wf_in = WireFormat.for_ring(s.rings[0], engine=eng)
+    wf_out = WireFormat.for_ring(s.rings[1], engine=eng)
     h1 = torch.from_numpy(host1.view(np.int64)).pin_memory()
     h2 = torch.from_numpy(host2.view(np.int64)).pin_memory()
+    h1p = wf_in.pack(d1).cpu().pin_memory()
+    h2p = wf_in.pack(d2).cpu().pin_memory()
+    torch.cuda.synchronize()
     hout = [torch.empty(rot.shape, dtype=torch.int64).pin_memory() for _ in range(2)]
+    houtp = [torch.empty((PAIRS, wf_out.item_bytes), dtype=torch.uint8).pin_memory() for _ in range(2)]
     din = [(d1, d2), (torch.empty_like(d1), torch.empty_like(d2))]
+    dinp = [(torch.empty_like(h1p, device="cuda"), torch.empty_like(h2p, device="cuda")) for _ in range(2)]
+    doutp = [torch.empty_like(houtp[0], device="cuda") for _ in range(2)]
     dprod = [prod, torch.empty_like(prod)]
     drot = [rot, torch.empty_like(rot)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
@@ -629,36 +644,56 @@ def run_cuda_arm(args) -> None:
     ev_out = [torch.cuda.Event() for _ in range(2)]
     e2e_steps = max(4, min(args.steps, 10))
 
-    def e2e_run(count):
+    def e2e_run(count, packed):
         for i in range(count):
             b = i % 2
             a1, a2 = din[b]
+            src1, src2 = (dinp[b] if packed else din[b])
             with torch.cuda.stream(s_in):
                 if i >= 2:
                     s_in.wait_event(ev_comp[b])  # step i-2 has finished reading these inputs
-                a1.copy_(h1, non_blocking=True)
-                a2.copy_(h2, non_blocking=True)
+                src1.copy_(h1p if packed else h1, non_blocking=True)
+                src2.copy_(h2p if packed else h2, non_blocking=True)
                 ev_in[b].record(s_in)
             stream.wait_event(ev_in[b])
             if i >= 2:
-                stream.wait_event(ev_out[b])  # step i-2's results have left drot[b]
+                stream.wait_event(ev_out[b])  # step i-2's results have left drot[b] / doutp[b]
+            if packed:
+                wf_in.unpack(src1, a1.shape, out=a1, stream=stream)
+                wf_in.unpack(src2, a2.shape, out=a2, stream=stream)
             mul.mul_relin_rescale(a1, a2, rlk_t, out=dprod[b], stream=stream)
             rotb.rotate(dprod[b], gens, keys, out=drot[b], stream=stream)
+            if packed:
+                wf_out.pack(drot[b], out=doutp[b], stream=stream)
             ev_comp[b].record(stream)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_comp[b])
-                hout[b].copy_(drot[b], non_blocking=True)
+                if packed:
+                    houtp[b].copy_(doutp[b], non_blocking=True)
+                else:
+                    hout[b].copy_(drot[b], non_blocking=True)
                 ev_out[b].record(s_out)
         stream.wait_stream(s_out)
 
-    e2e_run(2)
-    barrier()
-    ev0.record(stream)
-    e2e_run(e2e_steps)
-    ev1.record(stream)
-    barrier()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, dist, "cuda")
+    def e2e_time(packed):
+        e2e_run(2, packed)
+        barrier()
+        ev0.record(stream)
+        e2e_run(e2e_steps, packed)
+        ev1.record(stream)
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps, dist, "cuda")
+
+    e2e_ms_plain = e2e_time(False)
+    e2e_value_plain = whole_job_rate(PAIRS, world, e2e_ms_plain)
+    e2e_ms = e2e_time(True)
     e2e_value = whole_job_rate(PAIRS, world, e2e_ms)
+    # the packed transport delivers the same results: compare the last step's output
+    hres = torch.empty_like(rot)
+    wf_out.unpack(houtp[(e2e_steps - 1) % 2].cuda(), rot.shape, out=hres)
+    torch.cuda.synchronize()
+    e2e_packed_ok = bool(torch.equal(hres, drot[(e2e_steps - 1) % 2]))
+    del hres, dinp, doutp
     del din, dprod, drot
 
     # ---- dominant kernel: the digit transforms (B x (L+1) rows of N = 2^14 per launch)
@@ -770,9 +805,14 @@ def run_cuda_arm(args) -> None:
         "dtype": "u64 (RNS residues < 2^50)",
         "data": "synthetic (seeded keys, noise and unit-disk slots)",
         "config": dict(CONFIG, pairs_per_step=PAIRS),
-        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
-                "d2h_bytes_per_step": int(hout[0].numel() * 8), "ms_per_step": e2e_ms,
-                "pipelining": "copy-in, compute and copy-out of consecutive steps overlap (two buffer sets)"},
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(h1p.numel() + h2p.numel()),
+                "d2h_bytes_per_step": int(houtp[0].numel()), "ms_per_step": e2e_ms,
+                "transport": "compact wire format (residues at their primes' bit lengths; unpack and pack on "
+                             "the GPU inside the step)", "packed_matches_plain": e2e_packed_ok,
+                "pipelining": "copy-in, compute and copy-out of consecutive steps overlap (two buffer sets)",
+                "plain_uint64": {"value": e2e_value_plain, "ms_per_step": e2e_ms_plain,
+                                 "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
+                                 "d2h_bytes_per_step": int(hout[0].numel() * 8)}},
         "roofline": {"bound": "hbm", "kernel": f"forward FP64 NTT, {kname} (digit transforms, {PAIRS * ne} rows x 2^14)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": MEASURED_TRAFFIC.get((kname, PAIRS * ne)), "launch_ms": ntt_ms,

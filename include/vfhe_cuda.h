@@ -379,6 +379,19 @@ int vfhe_cuda_gen_ksk_batch(void *ntt, uint64_t *d_out, const uint64_t *d_src, u
                             const uint32_t *limbs, uint32_t nlimbs, const uint64_t *factors,
                             const uint64_t *d_sk, double sigma, void *stream);
 
+/* Compact wire format for residue rows, for host <-> device copies of ciphertexts:
+ * each row of N residues of a b-bit prime (b = bits[r], residues < 2^b) is a
+ * little-endian bit stream of N b bits (N b a multiple of 64); an item (e.g. one
+ * ciphertext [2][L][N], rows_per_item = 2 L) is its rows in order, items follow each
+ * other.  pack: d_rows [items][rows_per_item][N] uint64 -> d_packed; unpack: back.
+ * packed_bytes: size of `items` packed items.  1 <= items * rows_per_item <= 65535,
+ * rows_per_item <= 128.  No counterpart in the reference (it has no serialisation). */
+uint64_t vfhe_cuda_packed_bytes(uint64_t N, const uint32_t *bits, uint32_t rows_per_item, uint64_t items);
+int vfhe_cuda_pack_rows(void *d_packed, const uint64_t *d_rows, uint64_t N, const uint32_t *bits,
+                        uint32_t rows_per_item, uint64_t items, void *stream);
+int vfhe_cuda_unpack_rows(uint64_t *d_rows, const void *d_packed, uint64_t N, const uint32_t *bits,
+                          uint32_t rows_per_item, uint64_t items, void *stream);
+
 /* ChaCha20 keystream blocks counter0 .. counter0 + nblocks - 1 for a 256-bit key
  * (8 little-endian words) and a 64-bit nonce, in the original layout (64-bit block
  * counter in state words 12-13, nonce in 14-15), into d_out[nblocks][16] words: the

@@ -193,6 +193,63 @@ def gen_galois_key_batch(scheme, key, gen: int, lvl: int = 0, **kw) -> torch.Ten
     return gen_ksk_batch(scheme, key, [p.automorphism(gen) for p in key.poly], lvl, **kw)
 
 
+class WireFormat:
+    """Compact host <-> device format of residue rows (vfhe_cuda_pack_rows): each row
+    of N residues of a b-bit prime is a bit stream of N b bits, so a ciphertext at the
+    CKKS benchmark's chain (one 50-bit and eight 40-bit primes) travels in 46.25 bytes per
+    coefficient instead of 72.  ``bits`` lists the width of each row of one item, e.g.
+    ``[b_0 .. b_{L-1}] * 2`` for a [2][L][N] ciphertext."""
+
+    def __init__(self, N: int, bits: list[int], engine: Engine | None = None):
+        self.engine = engine or cuda_engine()
+        self.ffi = self.engine.ffi
+        self.lib = self.engine.lib
+        self.N = int(N)
+        self.bits = [int(b) for b in bits]
+        self._bits = self.ffi.new("uint32_t[]", self.bits)
+        self.item_bytes = int(self.lib.vfhe_cuda_packed_bytes(self.N, self._bits, len(self.bits), 1))
+        if self.item_bytes == 0:
+            self.engine.check("packed_bytes")
+            raise EngineError("packed_bytes")
+
+    @classmethod
+    def for_ring(cls, ring: Ring, components: int = 2, engine: Engine | None = None) -> "WireFormat":
+        bits = [int(q).bit_length() for q in ring.primes]
+        return cls(ring.N, bits * components, engine)
+
+    def _stream(self, stream):
+        st = stream or torch.cuda.current_stream()
+        return self.ffi.cast("void*", st.cuda_stream)
+
+    def pack(self, rows: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """[B][rows...][N] int64 residues -> [B][item_bytes] uint8."""
+        B = rows.shape[0]
+        assert rows.numel() == B * len(self.bits) * self.N and rows.is_contiguous()
+        if out is None:
+            out = torch.empty((B, self.item_bytes), dtype=torch.uint8, device=rows.device)
+        rc = self.lib.vfhe_cuda_pack_rows(self.ffi.cast("void*", out.data_ptr()), _ptr(self.ffi, rows), self.N,
+                                          self._bits, len(self.bits), B, self._stream(stream))
+        if rc != 0:
+            self.engine.check("pack_rows")
+            raise EngineError("pack_rows")
+        return out
+
+    def unpack(self, packed: torch.Tensor, shape: tuple, out: torch.Tensor | None = None,
+               stream=None) -> torch.Tensor:
+        """[B][item_bytes] uint8 -> int64 residues of ``shape`` ([B][rows...][N])."""
+        B = packed.shape[0]
+        assert packed.numel() == B * self.item_bytes and packed.is_contiguous()
+        if out is None:
+            out = torch.empty(shape, dtype=torch.int64, device=packed.device)
+        assert out.numel() == B * len(self.bits) * self.N
+        rc = self.lib.vfhe_cuda_unpack_rows(_ptr(self.ffi, out), self.ffi.cast("void*", packed.data_ptr()), self.N,
+                                            self._bits, len(self.bits), B, self._stream(stream))
+        if rc != 0:
+            self.engine.check("unpack_rows")
+            raise EngineError("unpack_rows")
+        return out
+
+
 def bootstrap_key_tensor(bk) -> torch.Tensor:
     """Device copy of a CGGI16_Key: [n][2 L0][2][L0+1][N] (MGSW rows in encryption order)."""
     arr = np.stack([np.stack([np.stack([c.component_rows(0), c.component_rows(1)]) for c in m.obj]) for m in bk.bk])

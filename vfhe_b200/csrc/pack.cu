@@ -1,0 +1,155 @@
+// Compact wire format for residue rows (ciphertexts in transit between host and GPU).
+//
+// A row of N residues of a b-bit prime (b = bit length of q, residues < q < 2^b) is
+// stored as N b-bit fields in a little-endian bit stream: residue x occupies bits
+// [x b, x b + b) of the row, bit k of the stream being bit (k mod 64) of 64-bit word
+// k / 64.  N b must be a multiple of 64, so every row is whole words.  An item (one
+// ciphertext [2][L][N]) is its rows one after another; items follow each other.
+// For the CKKS benchmark's primes (one 50-bit, eight 40-bit) a ciphertext shrinks from
+// 72 to 46.25 bytes per coefficient: the host-device copies that bound the end-to-end
+// rate shrink with it.
+//
+// The reference has no serialisation (its ciphertexts live in host memory), so this
+// format has no counterpart there.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "abi_common.cuh"
+
+namespace vc {
+
+namespace {
+
+constexpr int kMaxPackRows = 128;
+
+struct PackLayout {
+    uint32_t bits[kMaxPackRows];
+    uint64_t word_off[kMaxPackRows];  // first 64-bit word of row r inside an item
+    uint64_t item_words;
+    int rows;
+};
+
+// one thread per residue: up to two words, shifted and masked
+__global__ void k_unpack(uint64_t* __restrict__ out, const uint64_t* __restrict__ in, long long N,
+                         const __grid_constant__ PackLayout lay) {
+    const long long item = blockIdx.y / lay.rows;
+    const int r = blockIdx.y - (int)(item * lay.rows);
+    const uint32_t b = lay.bits[r];
+    const uint64_t mask = b >= 64 ? ~0ULL : ((1ULL << b) - 1);
+    const uint64_t* row = in + item * lay.item_words + lay.word_off[r];
+    const uint64_t row_words = ((uint64_t)N * b) / 64;
+    uint64_t* o = out + ((uint64_t)item * lay.rows + r) * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
+         x += (long long)gridDim.x * blockDim.x) {
+        const uint64_t bit = (uint64_t)x * b;
+        const uint64_t w = bit >> 6;
+        const uint32_t s = (uint32_t)(bit & 63);
+        uint64_t v = row[w] >> s;
+        if (s + b > 64 && w + 1 < row_words) v |= row[w + 1] << (64 - s);
+        o[x] = v & mask;
+    }
+}
+
+// one thread per output word: the residues overlapping it, shifted into place
+__global__ void k_pack(uint64_t* __restrict__ out, const uint64_t* __restrict__ in, long long N,
+                       const __grid_constant__ PackLayout lay) {
+    const long long item = blockIdx.y / lay.rows;
+    const int r = blockIdx.y - (int)(item * lay.rows);
+    const uint32_t b = lay.bits[r];
+    const uint64_t mask = b >= 64 ? ~0ULL : ((1ULL << b) - 1);
+    uint64_t* row = out + item * lay.item_words + lay.word_off[r];
+    const uint64_t row_words = ((uint64_t)N * b) / 64;
+    const uint64_t* src = in + ((uint64_t)item * lay.rows + r) * N;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < row_words;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t lo = w * 64, hi = lo + 64;  // bit range of this word
+        uint64_t x = lo / b;
+        uint64_t acc = 0;
+        for (; x < (uint64_t)N && x * b < hi; ++x) {
+            const uint64_t v = src[x] & mask;
+            const uint64_t start = x * b;
+            if (start >= lo) acc |= v << (start - lo);
+            else acc |= v >> (lo - start);
+        }
+        row[w] = acc;
+    }
+}
+
+bool make_layout(PackLayout& lay, uint64_t N, const uint32_t* bits, uint32_t rows, const char* where) {
+    if (!bits || rows == 0 || rows > (uint32_t)kMaxPackRows || N == 0) {
+        set_error(where, "need 1..128 rows per item, their bit widths and N > 0");
+        return false;
+    }
+    memset(&lay, 0, sizeof lay);
+    uint64_t off = 0;
+    for (uint32_t r = 0; r < rows; ++r) {
+        if (bits[r] == 0 || bits[r] > 64 || (N * bits[r]) % 64 != 0) {
+            set_error(where, "bit widths must be 1..64 with N * bits a multiple of 64");
+            return false;
+        }
+        lay.bits[r] = bits[r];
+        lay.word_off[r] = off;
+        off += N * bits[r] / 64;
+    }
+    lay.item_words = off;
+    lay.rows = (int)rows;
+    return true;
+}
+
+dim3 pack_grid(uint64_t per_row, uint64_t rows_total) {
+    note_launch();
+    uint64_t blocks = (per_row + 255) / 256;
+    if (blocks > 64) blocks = 64;
+    if (blocks < 1) blocks = 1;
+    return dim3((unsigned)blocks, (unsigned)rows_total, 1);
+}
+
+}  // namespace
+
+}  // namespace vc
+
+using namespace vc;
+
+extern "C" {
+
+uint64_t vfhe_cuda_packed_bytes(uint64_t N, const uint32_t* bits, uint32_t rows_per_item, uint64_t items) {
+    PackLayout lay;
+    if (!make_layout(lay, N, bits, rows_per_item, "vfhe_cuda_packed_bytes")) return 0;
+    return 8 * lay.item_words * items;
+}
+
+int vfhe_cuda_pack_rows(void* d_packed, const uint64_t* d_rows, uint64_t N, const uint32_t* bits,
+                        uint32_t rows_per_item, uint64_t items, void* stream) {
+    if (!ensure_ready()) return 1;
+    const char* where = "vfhe_cuda_pack_rows";
+    PackLayout lay;
+    if (!make_layout(lay, N, bits, rows_per_item, where)) return 1;
+    if (!d_packed || !d_rows || items == 0 || items * rows_per_item > 65535) {
+        set_error(where, "null buffers or items * rows_per_item outside 1..65535");
+        return 1;
+    }
+    uint64_t maxw = 0;
+    for (uint32_t r = 0; r < rows_per_item; ++r) maxw = std::max<uint64_t>(maxw, N * bits[r] / 64);
+    k_pack<<<pack_grid(maxw, items * rows_per_item), 256, 0, (cudaStream_t)stream>>>(
+        (uint64_t*)d_packed, d_rows, (long long)N, lay);
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+int vfhe_cuda_unpack_rows(uint64_t* d_rows, const void* d_packed, uint64_t N, const uint32_t* bits,
+                          uint32_t rows_per_item, uint64_t items, void* stream) {
+    if (!ensure_ready()) return 1;
+    const char* where = "vfhe_cuda_unpack_rows";
+    PackLayout lay;
+    if (!make_layout(lay, N, bits, rows_per_item, where)) return 1;
+    if (!d_packed || !d_rows || items == 0 || items * rows_per_item > 65535) {
+        set_error(where, "null buffers or items * rows_per_item outside 1..65535");
+        return 1;
+    }
+    k_unpack<<<pack_grid(N, items * rows_per_item), 256, 0, (cudaStream_t)stream>>>(
+        d_rows, (const uint64_t*)d_packed, (long long)N, lay);
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+}  // extern "C"
