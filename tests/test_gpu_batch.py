@@ -68,6 +68,30 @@ def test_batched_ckks_matches_single_calls(cuda, N, n_mid, split):
     assert np.array_equal(to_host(rot), np.stack(ref_rot))
 
 
+def test_batched_rotate_ragged_key_groups(cuda):
+    """11 ciphertexts over 5 Galois keys, in an order that interleaves the keys: the
+    key-switch MAC takes ciphertexts in groups sharing a key, and groups that straddle
+    two keys or run past the batch end must not change a residue."""
+    import torch
+
+    from vfhe_b200.batch import CkksBatch, ciphertext_rows, key_tensor, to_device, to_host
+
+    steps = [1, 2, 4, 8, 16]
+    s, key, rlk, gks, cts = _setup(cuda, 2**12, 3, 11, steps, seed=7)
+    rot_steps = [steps[(3 * i) % len(steps)] for i in range(len(cts))]
+    for c in cts:
+        c.round_division(lvl=1)
+        c.to_coeff()
+    rows = np.stack([ciphertext_rows(c) for c in cts])
+    ref = [ciphertext_rows(s.automorphism(c, s.galois_gen(k), gks[k])) for c, k in zip(cts, rot_steps)]
+    t = to_device(rows)
+    keys = {k: key_tensor(v) for k, v in gks.items()}
+    special = s.special_rings[0].prime_indices[-1]
+    rot = CkksBatch(s.rings[1], special).rotate(t, [s.galois_gen(k) for k in rot_steps], [keys[k] for k in rot_steps])
+    torch.cuda.synchronize()
+    assert np.array_equal(to_host(rot), np.stack(ref))
+
+
 def test_batched_ntt_matches_single_calls(cuda):
     import torch
 

@@ -60,6 +60,36 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
     const uint64_t* a2 = c2 + b * cs + k * N;
     const uint64_t* b2 = a2 + LN;
     uint64_t* t0 = T + b * ts + k * N;
+    if (S == 1 && pi.fp64 && (N & 1) == 0 &&
+        ((reinterpret_cast<uintptr_t>(a1) | reinterpret_cast<uintptr_t>(a2) | reinterpret_cast<uintptr_t>(t0)) & 15) ==
+            0) {
+        // exact FP64 products (canonical operands below 2^50, uncentred multipliers),
+        // two coefficients per thread, inputs read once
+        const double q = pi.qd, qinv = pi.qinv;
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            const ulonglong2 ua1 = __ldcs(reinterpret_cast<const ulonglong2*>(a1 + x));
+            const ulonglong2 ub1 = __ldcs(reinterpret_cast<const ulonglong2*>(b1 + x));
+            const ulonglong2 ua2 = __ldcs(reinterpret_cast<const ulonglong2*>(a2 + x));
+            const ulonglong2 ub2 = __ldcs(reinterpret_cast<const ulonglong2*>(b2 + x));
+            ulonglong2 r0, r1, r2;
+            auto one = [&](uint64_t xa1, uint64_t xb1, uint64_t xa2, uint64_t xb2, unsigned long long& d0,
+                           unsigned long long& d1, unsigned long long& d2) {
+                const double fa1 = f_from_u64(xa1), fb1 = f_from_u64(xb1);
+                const double fa2 = f_from_u64(xa2), fb2 = f_from_u64(xb2);
+                const double qa1 = __dmul_rn(fa1, qinv), qb1 = __dmul_rn(fb1, qinv);
+                d0 = f_to_canonical(f_mulmod(fa2, fa1, qa1, q), q, qinv, pi.q);
+                d1 = f_to_canonical(__dadd_rn(f_mulmod(fb2, fa1, qa1, q), f_mulmod(fa2, fb1, qb1, q)), q, qinv, pi.q);
+                d2 = f_to_canonical(f_mulmod(fb2, fb1, qb1, q), q, qinv, pi.q);
+            };
+            one(ua1.x, ub1.x, ua2.x, ub2.x, r0.x, r1.x, r2.x);
+            one(ua1.y, ub1.y, ua2.y, ub2.y, r0.y, r1.y, r2.y);
+            *reinterpret_cast<ulonglong2*>(t0 + x) = r0;
+            *reinterpret_cast<ulonglong2*>(t0 + x + LN) = r1;
+            *reinterpret_cast<ulonglong2*>(t0 + x + 2 * LN) = r2;
+        }
+        return;
+    }
     if (S == 1) {
         for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
              x += (long long)gridDim.x * blockDim.x) {
@@ -104,45 +134,6 @@ __global__ void k_mac(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D
     const uint64_t* kb = ka + dstride;
     uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
     uint64_t* ob = oa + dstride;
-    if (S == 1 && pi.fp64 &&
-        (((reinterpret_cast<uintptr_t>(d) | reinterpret_cast<uintptr_t>(ka) | reinterpret_cast<uintptr_t>(oa)) & 15) ==
-         0)) {
-        // pointwise products, two residues per thread (16-byte accesses: the kernel streams
-        // the digits from HBM), partial sums reduced every four digits
-        const double q = pi.qd, qinv = pi.qinv;
-        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
-             x += 2 * (long long)gridDim.x * blockDim.x) {
-            double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
-#pragma unroll 2
-            for (int j = 0; j < nd; ++j) {
-                // digits are read once: streaming loads leave L2 to the keys
-                const ulonglong2 dv = __ldcs(reinterpret_cast<const ulonglong2*>(d + j * dstride + x));
-                const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(ka + j * kstride + x);
-                const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(kb + j * kstride + x);
-                const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
-                const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
-                const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
-                sa0 = __dadd_rn(sa0, f_mulmod(v0, wa0, __dmul_rn(wa0, qinv), q));
-                sa1 = __dadd_rn(sa1, f_mulmod(v1, wa1, __dmul_rn(wa1, qinv), q));
-                sb0 = __dadd_rn(sb0, f_mulmod(v0, wb0, __dmul_rn(wb0, qinv), q));
-                sb1 = __dadd_rn(sb1, f_mulmod(v1, wb1, __dmul_rn(wb1, qinv), q));
-                if ((j & 3) == 3) {
-                    sa0 = f_reduce(sa0, q, qinv);
-                    sa1 = f_reduce(sa1, q, qinv);
-                    sb0 = f_reduce(sb0, q, qinv);
-                    sb1 = f_reduce(sb1, q, qinv);
-                }
-            }
-            ulonglong2 ra, rb;
-            ra.x = f_to_canonical(-sa0, q, qinv, pi.q);
-            ra.y = f_to_canonical(-sa1, q, qinv, pi.q);
-            rb.x = f_to_canonical(-sb0, q, qinv, pi.q);
-            rb.y = f_to_canonical(-sb1, q, qinv, pi.q);
-            *reinterpret_cast<ulonglong2*>(oa + x) = ra;
-            *reinterpret_cast<ulonglong2*>(ob + x) = rb;
-        }
-        return;
-    }
     if (S == 1 && pi.fp64) {
         // pointwise products: the streaming loop, partial sums reduced every four digits
         const double q = pi.qd, qinv = pi.qinv;
@@ -215,8 +206,69 @@ __global__ void k_moddown(uint64_t* __restrict__ out, const uint64_t* __restrict
     const int use_pass = c == 0 ? use_pass_a : use_pass_b;
     const uint64_t* ps = use_pass ? pass + (long long)b * pass_stride + (c == 0 ? pass_off_a : pass_off_b) : nullptr;
     const PrimeInfo psp = primes[mc.special];
-    if (((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(o) |
-          reinterpret_cast<uintptr_t>(ps ? ps : a)) & 15) == 0) {
+    const bool aligned = ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(o) |
+                           reinterpret_cast<uintptr_t>(ps ? ps : a)) & 15) == 0;
+    if (mc.fp64 && aligned) {
+        // exact FP64 form of the branch below: every intermediate is an integer below
+        // 2^52, so no residue differs; two coefficients per thread, streaming loads
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            const ulonglong2 sp = __ldcs(reinterpret_cast<const ulonglong2*>(a + (long long)nl * N + x));
+            uint64_t t0 = sp.x + mc.half_p, t1 = sp.y + mc.half_p;
+            t0 -= t0 >= mc.p ? mc.p : 0;
+            t1 -= t1 >= mc.p ? mc.p : 0;
+            const double td0 = f_from_u64(t0), td1 = f_from_u64(t1);
+            // limb i after the special-prime division and the pass-through add, |v| < 7q/4
+            auto limb2 = [&](int i, double& v0, double& v1) {
+                const PrimeInfo& pi = primes[mc.prime[i]];
+                const ulonglong2 av = __ldcs(reinterpret_cast<const ulonglong2*>(a + (long long)i * N + x));
+                const double y0 = __dadd_rn(__dadd_rn(f_from_u64(av.x), mc.half_sp_d[i]), -td0);
+                const double y1 = __dadd_rn(__dadd_rn(f_from_u64(av.y), mc.half_sp_d[i]), -td1);
+                v0 = f_mulmod(y0, mc.inv_sp_d[i], mc.inv_sp_dq[i], pi.qd);
+                v1 = f_mulmod(y1, mc.inv_sp_d[i], mc.inv_sp_dq[i], pi.qd);
+                if (ps) {
+                    const ulonglong2 pv = __ldcs(reinterpret_cast<const ulonglong2*>(ps + (long long)i * N + x));
+                    v0 = __dadd_rn(v0, f_from_u64(pv.x));
+                    v1 = __dadd_rn(v1, f_from_u64(pv.y));
+                }
+            };
+            if (!rescale) {
+#pragma unroll 2
+                for (int i = 0; i < nl; ++i) {
+                    const PrimeInfo& pi = primes[mc.prime[i]];
+                    double v0, v1;
+                    limb2(i, v0, v1);
+                    ulonglong2 r;
+                    r.x = f_to_canonical(v0, pi.qd, pi.qinv, pi.q);
+                    r.y = f_to_canonical(v1, pi.qd, pi.qinv, pi.q);
+                    *reinterpret_cast<ulonglong2*>(o + (long long)i * N + x) = r;
+                }
+            } else {
+                const PrimeInfo& pt = primes[mc.prime[nl - 1]];
+                double u0, u1;
+                limb2(nl - 1, u0, u1);
+                uint64_t s0 = f_to_canonical(u0, pt.qd, pt.qinv, pt.q) + mc.half_top;
+                uint64_t s1 = f_to_canonical(u1, pt.qd, pt.qinv, pt.q) + mc.half_top;
+                s0 -= s0 >= mc.q_top ? mc.q_top : 0;
+                s1 -= s1 >= mc.q_top ? mc.q_top : 0;
+                const double sd0 = f_from_u64(s0), sd1 = f_from_u64(s1);
+#pragma unroll 2
+                for (int i = 0; i < nl - 1; ++i) {
+                    const PrimeInfo& pi = primes[mc.prime[i]];
+                    double v0, v1;
+                    limb2(i, v0, v1);
+                    const double y0 = __dadd_rn(__dadd_rn(v0, mc.half_r_d[i]), -sd0);
+                    const double y1 = __dadd_rn(__dadd_rn(v1, mc.half_r_d[i]), -sd1);
+                    ulonglong2 r;
+                    r.x = f_to_canonical(f_mulmod(y0, mc.inv_r_d[i], mc.inv_r_dq[i], pi.qd), pi.qd, pi.qinv, pi.q);
+                    r.y = f_to_canonical(f_mulmod(y1, mc.inv_r_d[i], mc.inv_r_dq[i], pi.qd), pi.qd, pi.qinv, pi.q);
+                    *reinterpret_cast<ulonglong2*>(o + (long long)i * N + x) = r;
+                }
+            }
+        }
+        return;
+    }
+    if (aligned) {
         // two coefficients per thread with 16-byte accesses; acc and the pass-through
         // rows are read once (streaming loads)
         for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
@@ -307,9 +359,10 @@ __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __re
     uint64_t* dst = out + ((long long)bc * L + k) * N;
     const uint64_t split = 1ULL << log_split;
     const uint64_t P = (uint64_t)N >> log_split;
+    const int log_p = 63 - __clzll((long long)P);  // N and the split degree are powers of two
     for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < N;
          pos += (long long)gridDim.x * blockDim.x) {
-        const uint64_t i = (uint64_t)pos / P, i2 = (uint64_t)pos % P;
+        const uint64_t i = (uint64_t)pos >> log_p, i2 = (uint64_t)pos & (P - 1);
         const uint64_t idx = (i + (i2 << log_split)) * gen;
         const uint64_t d = (idx & (split - 1)) * P + ((idx & ((uint64_t)N - 1)) >> log_split);
         const uint64_t v = src[pos];
@@ -317,10 +370,72 @@ __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __re
     }
 }
 
+// k_mac at split 1 for FP64 primes with every row 16-byte aligned and N even (the
+// launcher checks): pointwise products, two residues per thread (16-byte accesses: the
+// kernel streams the digits from HBM), partial sums reduced every four digits.  Its own
+// kernel so that its register count, not the general one's, sets the occupancy.
+__global__ void __launch_bounds__(256, 6) k_mac_pointwise(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
+                                                          const uint64_t* const* __restrict__ keys,
+                                                          const uint64_t* __restrict__ order,
+                                                          const __grid_constant__ LimbPrimes lp,
+                                                          const PrimeInfo* __restrict__ primes, int nd, int ne,
+                                                          long long N) {
+    const int by = blockIdx.y;
+    const int bo = by / ne, i = by - bo * ne;
+    const int b = order ? (int)order[bo] : bo;
+    const PrimeInfo& pi = primes[lp.p[i]];
+    const uint64_t* key = keys[b];
+    const long long dstride = (long long)ne * N;
+    const long long kstride = (long long)2 * ne * N;
+    const uint64_t* d = D + (long long)b * nd * dstride + (long long)i * N;
+    const uint64_t* ka = key + (long long)i * N;
+    const uint64_t* kb = ka + dstride;
+    uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
+    uint64_t* ob = oa + dstride;
+    // pointwise products, two residues per thread (16-byte accesses: the kernel streams
+    // the digits from HBM), partial sums reduced every four digits
+    const double q = pi.qd, qinv = pi.qinv;
+    for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+         x += 2 * (long long)gridDim.x * blockDim.x) {
+        double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
+#pragma unroll 1
+        for (int j = 0; j < nd; ++j) {
+            // digits are read once: streaming loads leave L2 to the keys
+            const ulonglong2 dv = __ldcs(reinterpret_cast<const ulonglong2*>(d + j * dstride + x));
+            const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(ka + j * kstride + x);
+            const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(kb + j * kstride + x);
+            // the digit is the multiplier of both key products (one quotient for
+            // two products; uncentred operands below 2^50, each term |t| <= 3q/4)
+            const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
+            const double vq0 = __dmul_rn(v0, qinv), vq1 = __dmul_rn(v1, qinv);
+            const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
+            const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
+            sa0 = __dadd_rn(sa0, f_mulmod(wa0, v0, vq0, q));
+            sa1 = __dadd_rn(sa1, f_mulmod(wa1, v1, vq1, q));
+            sb0 = __dadd_rn(sb0, f_mulmod(wb0, v0, vq0, q));
+            sb1 = __dadd_rn(sb1, f_mulmod(wb1, v1, vq1, q));
+            if ((j & 3) == 3) {
+                sa0 = f_reduce(sa0, q, qinv);
+                sa1 = f_reduce(sa1, q, qinv);
+                sb0 = f_reduce(sb0, q, qinv);
+                sb1 = f_reduce(sb1, q, qinv);
+            }
+        }
+        ulonglong2 ra, rb;
+        ra.x = f_to_canonical(-sa0, q, qinv, pi.q);
+        ra.y = f_to_canonical(-sa1, q, qinv, pi.q);
+        rb.x = f_to_canonical(-sb0, q, qinv, pi.q);
+        rb.y = f_to_canonical(-sb1, q, qinv, pi.q);
+        *reinterpret_cast<ulonglong2*>(oa + x) = ra;
+        *reinterpret_cast<ulonglong2*>(ob + x) = rb;
+    }
+}
+
 // One k_mac launch for the ring's split degree (each split degree is its own kernel,
 // so the pointwise one keeps its small register footprint).
+// keys_aligned: every key polynomial starts on a 16-byte boundary.
 void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
-                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st);
+                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned);
 
 // Grid for one launch of a per-coefficient kernel; every call site launches exactly
 // one kernel with it, so it also counts the launch.
@@ -333,9 +448,16 @@ dim3 grid_xy(long long n, long long y) {
 }
 
 void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
-                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st) {
-    // the pointwise kernel handles two residues per thread
-    const dim3 g = grid_xy(t->pub.split_degree == 1 ? (N + 1) / 2 : N, (long long)B * ne);
+                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned) {
+    bool pointwise = t->pub.split_degree == 1 && keys_aligned && (N & 1) == 0 &&
+                     ((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(D)) & 15) == 0;
+    for (int i = 0; i < ne && pointwise; ++i) pointwise = t->info[lpe.p[i]].fp64 != 0;
+    if (pointwise) {
+        k_mac_pointwise<<<grid_xy((N + 1) / 2, (long long)B * ne), 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info,
+                                                                               nd, ne, N);
+        return;
+    }
+    const dim3 g = grid_xy(N, (long long)B * ne);
     switch (t->pub.split_degree) {
         case 1: k_mac<1><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
         case 2: k_mac<2><<<g, 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N); break;
@@ -559,6 +681,18 @@ ModDownConsts moddown_consts(IncNtt* t, const uint32_t* limbs, int nl, uint32_t 
         mc.inv_r[i] = host_inv_mod(qt % q, q);
         mc.inv_r_sh[i] = host_shoup(mc.inv_r[i], q);
     }
+    mc.fp64 = p < (1ULL << 50);
+    for (int i = 0; i < nl; ++i) {
+        const uint64_t q = t->info[limbs[i]].q;
+        mc.fp64 = mc.fp64 && q < (1ULL << 50);
+        auto centred = [q](uint64_t w) { return w > q / 2 ? (double)w - (double)q : (double)w; };
+        mc.half_sp_d[i] = (double)mc.half_sp[i];
+        mc.inv_sp_d[i] = centred(mc.inv_sp[i]);
+        mc.inv_sp_dq[i] = mc.inv_sp_d[i] / (double)q;
+        mc.half_r_d[i] = (double)mc.half_r[i];
+        mc.inv_r_d[i] = centred(mc.inv_r[i]);
+        mc.inv_r_dq[i] = mc.inv_r_d[i] / (double)q;
+    }
     return mc;
 }
 
@@ -600,7 +734,9 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     std::vector<const uint64_t*> kp(B, rlk);
     if (!check_cuda(upload_small(keyptrs, (const uint64_t*)kp.data(), B, st), where)) return 1;
     switch (t->pub.split_degree) {
-        case 1: k_tensor<1><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
+        case 1:  // the FP64 path takes two coefficients per thread
+            k_tensor<1><<<grid_xy((N + 1) / 2, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N);
+            break;
         case 2: k_tensor<2><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
         case 4: k_tensor<4><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
         case 8: k_tensor<8><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
@@ -609,7 +745,8 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
     if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st);
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st,
+               (reinterpret_cast<uintptr_t>(rlk) & 15) == 0);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
@@ -667,7 +804,10 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
         src = Pm;
     }
     if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st);
+    bool keys_aligned = true;
+    for (uint64_t b = 0; b < B; ++b) keys_aligned = keys_aligned && (reinterpret_cast<uintptr_t>(gks[b]) & 15) == 0;
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st,
+               keys_aligned);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);

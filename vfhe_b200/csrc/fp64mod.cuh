@@ -21,6 +21,8 @@ namespace vc {
 constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
 
 // y * w mod q, centred, |result| <= 3q/4 (needs |y| < 2^52, |w| <= q/2, wq = fl(w/q)).
+// The same steps accept an uncentred 0 <= w < q when |y| < 2^50: then
+// |y w/q - n| <= 1/2 + |y| 2^-53 and |result| <= q/2 + q/8.
 __device__ __forceinline__ double f_mulmod(double y, double w, double wq, double q) {
     const double h = __dmul_rn(y, w);
     const double l = __fma_rn(y, w, -h);

@@ -17,6 +17,11 @@ struct ModDownConsts {
     uint32_t special;               // pool index of the special prime
     uint64_t p, half_p;             // special prime and floor(p/2)
     uint64_t q_top, half_top;       // top prime dropped by the rescale
+    // FP64 form (all primes below 2^50): multipliers centred in (-q/2, q/2] with
+    // their quotients fl(w/q), halves as exact doubles
+    int fp64;
+    double half_sp_d[kMaxLimbs], inv_sp_d[kMaxLimbs], inv_sp_dq[kMaxLimbs];
+    double half_r_d[kMaxLimbs], inv_r_d[kMaxLimbs], inv_r_dq[kMaxLimbs];
 };
 
 // Constants for dividing [nl + 1] limbs (limbs, then `special`) by the special prime,
