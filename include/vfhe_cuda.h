@@ -438,9 +438,9 @@ int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_b
                                int32_t ctas_per_sm);
 int vfhe_cuda_ntt_get_schedule(uint32_t logP, uint64_t rows, int32_t *out3);
 
-/* Nonzero when a persistent transform kernel's bounded wait for a bulk tile copy gave
- * up (its results are then wrong); -1 when the flag cannot be read.  Stays 0 in normal
- * operation. */
+/* Nonzero when a kernel's bounded wait for a bulk copy gave up (a persistent transform
+ * or the staged key-switch MAC; its results are then wrong); -1 when the flags cannot
+ * be read.  Stays 0 in normal operation. */
 int vfhe_cuda_device_faults(void);
 
 /* Work list: independent jobs of any mix of ring degree and limb count, run as ONE

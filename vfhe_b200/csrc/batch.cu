@@ -232,7 +232,9 @@ int vfhe_cuda_device_faults(void) {
     if (!vc::ensure_ready()) return -1;
     int f = 0;
     if (!check_cuda(read_tile_fault(&f), "vfhe_cuda_device_faults")) return -1;
-    return f;
+    int m = 0;
+    if (!check_cuda(read_mac_fault(&m), "vfhe_cuda_device_faults")) return -1;
+    return f | m;
 }
 
 int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_bits, int32_t tiles_per_cta,

@@ -17,9 +17,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "abi_common.cuh"
+#include "bulk.cuh"
 #include "fp64mod.cuh"
 #include "keyswitch.cuh"
 
@@ -431,6 +433,95 @@ __global__ void __launch_bounds__(256, 6) k_mac_pointwise(uint64_t* __restrict__
     }
 }
 
+// k_mac_pointwise with its operands staged through shared memory by bulk copies: block
+// (chunk, row) walks the digits of MAC_CHUNK residues of one extended limb, and thread 0
+// keeps MAC_STAGES digits (the digit chunk and both key chunks) in flight ahead of the
+// one being multiplied.  The digits stream from HBM; as plain loads only one digit per
+// thread was in flight and the kernel sat at half of DRAM bandwidth.  Needs N a multiple
+// of MAC_CHUNK and every row 16-byte aligned (checked by the launcher).
+constexpr int kMacChunk = 512;   // residues per block: two per thread
+constexpr int kMacStages = 4;    // digits in flight per block
+constexpr int kMacStageWords = 3 * kMacChunk;
+constexpr size_t kMacSmem = (size_t)kMacStages * kMacStageWords * 8;
+
+__device__ int vc_mac_fault;  // nonzero: a staged MAC copy wait gave up
+
+// Thread 0: request digit j's chunk and both key chunks into stage j mod kMacStages.
+__device__ __forceinline__ void mac_issue(uint64_t* msm, uint64_t* bars, const uint64_t* d, const uint64_t* ka, int j,
+                                          long long dstride, long long kstride) {
+    uint64_t* st = msm + (j % kMacStages) * kMacStageWords;
+    uint64_t* bar = &bars[j % kMacStages];
+    mbar_expect_tx(bar, kMacStageWords * 8);
+    bulk_load(st, d + j * dstride, kMacChunk * 8, bar);
+    bulk_load(st + kMacChunk, ka + j * kstride, kMacChunk * 8, bar);
+    bulk_load(st + 2 * kMacChunk, ka + j * kstride + dstride, kMacChunk * 8, bar);
+}
+
+__global__ void __launch_bounds__(256) k_mac_staged(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
+                                                    const uint64_t* const* __restrict__ keys,
+                                                    const uint64_t* __restrict__ order,
+                                                    const __grid_constant__ LimbPrimes lp,
+                                                    const PrimeInfo* __restrict__ primes, int nd, int ne,
+                                                    long long N) {
+    extern __shared__ __align__(128) uint64_t msm[];
+    __shared__ uint64_t bars[kMacStages];
+    const int by = blockIdx.y;
+    const int bo = by / ne, i = by - bo * ne;
+    const int b = order ? (int)order[bo] : bo;
+    const long long x0 = (long long)blockIdx.x * kMacChunk;
+    const long long dstride = (long long)ne * N;
+    const long long kstride = (long long)2 * ne * N;
+    const uint64_t* d = D + (long long)b * nd * dstride + (long long)i * N + x0;
+    const uint64_t* ka = keys[b] + (long long)i * N + x0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kMacStages; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+        for (int j = 0; j < nd && j < kMacStages; ++j) mac_issue(msm, bars, d, ka, j, dstride, kstride);
+    }
+    __syncthreads();
+    const PrimeInfo& pi = primes[lp.p[i]];
+    const double q = pi.qd, qinv = pi.qinv;
+    const int r = 2 * threadIdx.x;
+    double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
+    for (int j = 0; j < nd; ++j) {
+        const int s = j % kMacStages;
+        mbar_wait_bounded(&bars[s], (uint32_t)((j / kMacStages) & 1), &vc_mac_fault);
+        const uint64_t* st = msm + s * kMacStageWords;
+        const ulonglong2 dv = *reinterpret_cast<const ulonglong2*>(st + r);
+        const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(st + kMacChunk + r);
+        const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(st + 2 * kMacChunk + r);
+        // the digit is the multiplier of both key products (one quotient for two
+        // products; uncentred operands below 2^50, each term |t| <= 3q/4)
+        const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
+        const double vq0 = __dmul_rn(v0, qinv), vq1 = __dmul_rn(v1, qinv);
+        const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
+        const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
+        __syncthreads();  // every thread has read stage s: it may be refilled
+        if (threadIdx.x == 0 && j + kMacStages < nd) {
+            fence_proxy_async_smem();
+            mac_issue(msm, bars, d, ka, j + kMacStages, dstride, kstride);
+        }
+        sa0 = __dadd_rn(sa0, f_mulmod(wa0, v0, vq0, q));
+        sa1 = __dadd_rn(sa1, f_mulmod(wa1, v1, vq1, q));
+        sb0 = __dadd_rn(sb0, f_mulmod(wb0, v0, vq0, q));
+        sb1 = __dadd_rn(sb1, f_mulmod(wb1, v1, vq1, q));
+        if ((j & 3) == 3) {
+            sa0 = f_reduce(sa0, q, qinv);
+            sa1 = f_reduce(sa1, q, qinv);
+            sb0 = f_reduce(sb0, q, qinv);
+            sb1 = f_reduce(sb1, q, qinv);
+        }
+    }
+    uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N + x0 + r;
+    ulonglong2 ra, rb;
+    ra.x = f_to_canonical(-sa0, q, qinv, pi.q);
+    ra.y = f_to_canonical(-sa1, q, qinv, pi.q);
+    rb.x = f_to_canonical(-sb0, q, qinv, pi.q);
+    rb.y = f_to_canonical(-sb1, q, qinv, pi.q);
+    *reinterpret_cast<ulonglong2*>(oa) = ra;
+    *reinterpret_cast<ulonglong2*>(oa + dstride) = rb;
+}
+
 // One k_mac launch for the ring's split degree (each split degree is its own kernel,
 // so the pointwise one keeps its small register footprint).
 // keys_aligned: every key polynomial starts on a 16-byte boundary.
@@ -452,6 +543,12 @@ void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* con
     bool pointwise = t->pub.split_degree == 1 && keys_aligned && (N & 1) == 0 &&
                      ((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(D)) & 15) == 0;
     for (int i = 0; i < ne && pointwise; ++i) pointwise = t->info[lpe.p[i]].fp64 != 0;
+    if (pointwise && N % kMacChunk == 0 && prepare_ckks_kernels() == 0) {
+        note_launch();
+        const dim3 g((unsigned)(N / kMacChunk), (unsigned)(B * ne), 1);
+        k_mac_staged<<<g, kMacChunk / 2, kMacSmem, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N);
+        return;
+    }
     if (pointwise) {
         k_mac_pointwise<<<grid_xy((N + 1) / 2, (long long)B * ne), 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info,
                                                                                nd, ne, N);
@@ -660,6 +757,19 @@ __global__ void k_prng_blocks(uint32_t* __restrict__ out, uint64_t nblocks, cons
 
 
 }  // namespace
+
+int prepare_ckks_kernels() {
+    static std::once_flag once;
+    static int err = 0;
+    std::call_once(once, [] {
+        err = (int)cudaFuncSetAttribute(k_mac_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMacSmem);
+    });
+    return err;
+}
+
+int read_mac_fault(int* out) {
+    return (int)cudaMemcpyFromSymbol(out, vc_mac_fault, sizeof(int));
+}
 
 ModDownConsts moddown_consts(IncNtt* t, const uint32_t* limbs, int nl, uint32_t special) {
     ModDownConsts mc;

@@ -104,4 +104,12 @@ int prepare_ntt_kernels();
 // for a tile copy gave up (0 = never).
 int read_tile_fault(int* out);
 
+// Kernel attributes of the batched CKKS kernels (the staged key-switch MAC's shared
+// memory), set once; prepare_ntt_kernels calls it too.
+int prepare_ckks_kernels();
+
+// Copy the device flag that the staged key-switch MAC raises when a bounded wait for
+// a bulk copy gave up (0 = never).
+int read_mac_fault(int* out);
+
 }  // namespace vc

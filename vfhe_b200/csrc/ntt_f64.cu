@@ -17,6 +17,7 @@
 #include <mutex>
 #include <vector>
 
+#include "bulk.cuh"
 #include "fp64mod.cuh"
 #include "ntt.cuh"
 
@@ -283,52 +284,13 @@ __device__ __forceinline__ double load_in(const uint64_t* p, bool in_double, boo
 // ---- bulk asynchronous tile loads (persistent kernels)
 //
 // A persistent CTA keeps two tile buffers: while it transforms the tiles in one, the
-// bulk-copy engine fills the other with its next group's input (cp.async.bulk from
-// global to shared memory, completion counted in bytes on an mbarrier).  Every wait
-// is bounded: if a copy has not landed after the limit, the kernel records the fault
-// in vc_tile_fault, waits once more, and carries on (results are then wrong, but the
-// kernel ends and the host can read the flag).
+// bulk-copy engine fills the other with its next group's input (bulk.cuh).  A wait
+// that gives up records the fault in vc_tile_fault.
 
 __device__ int vc_tile_fault;  // nonzero: a tile copy wait gave up
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// global -> shared, `bytes` (multiple of 16, both addresses 16-byte aligned)
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
 __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (int round = 0; round < 2; ++round) {
-        for (int i = 0; i < (1 << 18); ++i)
-            if (mbar_try_wait(bar, parity)) return;
-        if (round == 0) atomicExch(&vc_tile_fault, 1);
-    }
+    vc::mbar_wait_bounded(bar, parity, &vc_tile_fault);
 }
 
 // Thread 0: request the input of tile group `grp` into buf (tiles at buf + l * padded).
@@ -1077,7 +1039,8 @@ int read_tile_fault(int* out) {
 }
 
 int prepare_ntt_kernels() {
-    int e = prepare_k<8>();
+    int e = prepare_ckks_kernels();
+    if (!e) e = prepare_k<8>();
     if (!e) e = prepare_k<9>();
     if (!e) e = prepare_k<10>();
     if (!e) e = prepare_k<11>();
