@@ -347,28 +347,40 @@ __global__ void k_moddown(uint64_t* __restrict__ out, const uint64_t* __restrict
     (void)psp;
 }
 
-// Galois permutation of both components, per-ciphertext generator (rns_polynomial.c:996-1035).
+// Galois permutation of both components, per-ciphertext generator (rns_polynomial.c:996-1035:
+// coefficient c moves to c gen mod 2N, negated when that is >= N; position k of block i
+// holds coefficient i + k S at split degree S).  Written as a gather: output coefficient
+// c' takes source coefficient p = c' gen^-1 mod 2N when p < N, and minus coefficient
+// p - N otherwise (gen odd, so N gen = N mod 2N).  Stores are coalesced 16-byte pairs;
+// the scattered 8-byte reads hit the source row in L2.  Index arithmetic is 32-bit
+// (2N <= 2^31, so products wrap correctly modulo 2N).
 __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __restrict__ in,
-                                const uint64_t* __restrict__ gens, const __grid_constant__ LimbPrimes lp,
+                                const uint64_t* __restrict__ ginvs, const __grid_constant__ LimbPrimes lp,
                                 const PrimeInfo* __restrict__ primes, int L, long long N, int log_split) {
     const int by = blockIdx.y;  // (b, c, k)
     const int k = by % L;
     const int bc = by / L;
     const int b = bc >> 1;
     const uint64_t q = primes[lp.p[k]].q;
-    const uint64_t gen = gens[b];
+    const uint32_t ginv = (uint32_t)ginvs[b];
     const uint64_t* src = in + ((long long)bc * L + k) * N;
     uint64_t* dst = out + ((long long)bc * L + k) * N;
-    const uint64_t split = 1ULL << log_split;
-    const uint64_t P = (uint64_t)N >> log_split;
-    const int log_p = 63 - __clzll((long long)P);  // N and the split degree are powers of two
-    for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < N;
-         pos += (long long)gridDim.x * blockDim.x) {
-        const uint64_t i = (uint64_t)pos >> log_p, i2 = (uint64_t)pos & (P - 1);
-        const uint64_t idx = (i + (i2 << log_split)) * gen;
-        const uint64_t d = (idx & (split - 1)) * P + ((idx & ((uint64_t)N - 1)) >> log_split);
-        const uint64_t v = src[pos];
-        dst[d] = (idx & (uint64_t)N) ? neg_mod(v, q) : v;
+    const uint32_t n = (uint32_t)N, mask2n = 2 * n - 1;
+    const uint32_t split = 1u << log_split;
+    const int log_p = 31 - __clz((int)(n >> log_split));
+    const uint32_t pmask = (n >> log_split) - 1;
+    auto gather = [&](uint32_t d) -> uint64_t {
+        const uint32_t cd = (d >> log_p) + ((d & pmask) << log_split);  // output coefficient
+        const uint32_t p = (cd * ginv) & mask2n;
+        const uint32_t c = p & (n - 1);
+        const uint64_t v = src[((c & (split - 1)) << log_p) + (c >> log_split)];
+        return p >= n ? neg_mod(v, q) : v;
+    };
+    for (uint32_t d = 2 * (blockIdx.x * blockDim.x + threadIdx.x); d < n; d += 2 * gridDim.x * blockDim.x) {
+        ulonglong2 r;
+        r.x = gather(d);
+        r.y = gather(d + 1);
+        *reinterpret_cast<ulonglong2*>(dst + d) = r;
     }
 }
 
@@ -872,6 +884,10 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     const char* where = gens ? "vfhe_cuda_ckks_rotate_batch" : "vfhe_cuda_keyswitch_batch";
     if (!check_shape(t, limbs, L, special, where)) return 1;
     const long long N = (long long)t->pub.N;
+    if (gens && N > (1LL << 30)) {
+        set_error(where, "rotation needs N <= 2^30");
+        return 1;
+    }
     if (gens)
         for (uint64_t b = 0; b < B; ++b)
             if ((gens[b] & 1) == 0 || gens[b] >= 2 * (uint64_t)N) {
@@ -908,8 +924,16 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     if (!identity && !check_cuda(upload_small(d_order, order.data(), B, st), where)) return 1;
     const uint64_t* src = ct;
     if (gens) {
-        if (!check_cuda(upload_small(d_gens, gens, B, st), where)) return 1;
-        k_permute_batch<<<grid_xy(N, (long long)B * 2 * nl), 256, 0, st>>>(Pm, ct, d_gens, lp, t->d_info, nl, N, ls);
+        // the gather needs gen^-1 mod 2N (Newton's iteration doubles the correct low bits)
+        std::vector<uint64_t> ginv(B);
+        for (uint64_t b = 0; b < B; ++b) {
+            uint64_t x = gens[b];
+            for (int it = 0; it < 6; ++it) x *= 2 - gens[b] * x;
+            ginv[b] = x & (2 * (uint64_t)N - 1);
+        }
+        if (!check_cuda(upload_small(d_gens, ginv.data(), B, st), where)) return 1;
+        k_permute_batch<<<grid_xy((N + 1) / 2, (long long)B * 2 * nl), 256, 0, st>>>(Pm, ct, d_gens, lp, t->d_info, nl,
+                                                                                N, ls);
         if (!check_cuda(cudaGetLastError(), where)) return 1;
         src = Pm;
     }
