@@ -36,7 +36,14 @@ struct FCtx {
     double q, qinv;
     const double2* tw;
     const double2* lt;  // lane-major twiddles of bits 0..3 (PrimeInfo::fwd_lane / inv_lane)
+    bool lazy = false;  // forward: skip the reductions between passes (fwd_lazy)
 };
+
+// A forward transform of a prime q < 2^47 needs no reduction between its load and its
+// final canonical store: each stage adds at most |t| <= q/2 + q|y| 2^-54 <= 0.69q to a
+// value (centred twiddles, |y| < 2^52), so after at most 20 stages every value stays
+// below 0.5q + 20 * 0.69q < 14.3q < 2^51 and every step stays exact.
+__device__ __forceinline__ bool fwd_lazy(const PrimeInfo& pi) { return pi.q < (1ULL << 47); }
 
 // Position of slot (bit b, h) of 16-residue block g in a lane-major twiddle table.
 __device__ __forceinline__ int lane_tw_index(int g, int b, int h) {
@@ -156,8 +163,10 @@ __device__ __forceinline__ void f_fwd_bits(double (&x)[16], const PassTw<LO, BHI
     // The pass at bit 0 is the transform's last and is followed by f_to_canonical, whose
     // own reduction takes its outputs (|x| < 4q < 2^52) directly.
     if constexpr (LO != 0) {
+        if (!c.lazy) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = f_reduce(x[m], c.q, c.qinv);
+            for (int m = 0; m < 16; ++m) x[m] = f_reduce(x[m], c.q, c.qinv);
+        }
     }
 }
 
@@ -356,6 +365,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value, TileMinBlocks<K>::value
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
     c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
+    c.lazy = fwd_lazy(pi);
     const int logP = rows.logP, hi = r.hi;
     double x[16];
 
@@ -561,6 +571,7 @@ __global__ void __launch_bounds__(256, (K1 >= 5 ? 2 : 4)) k_col_f(const __grid_c
     double x[R];
     if (!INV) {
         const double2* tw = reinterpret_cast<const double2*>(pi.fwd_d);
+        const bool lazy = fwd_lazy(pi);
 #pragma unroll
         for (int m = 0; m < R; ++m) {
             double v = f_from_u64(src[(long long)m << KT]);
@@ -579,14 +590,14 @@ __global__ void __launch_bounds__(256, (K1 >= 5 ? 2 : 4)) k_col_f(const __grid_c
                 x[m | (1 << bb)] = __dsub_rn(u, v);
             }
             // at most four stages between reductions (|x| < 4q)
-            if (bb == K1 - 4 && bb > 0) {
+            if (bb == K1 - 4 && bb > 0 && !lazy) {
 #pragma unroll
                 for (int m = 0; m < R; ++m) x[m] = f_reduce(x[m], q, qinv);
             }
         }
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            dst[(long long)m << KT] = (uint64_t)__double_as_longlong(f_reduce(x[m], q, qinv));
+            dst[(long long)m << KT] = (uint64_t)__double_as_longlong(lazy ? x[m] : f_reduce(x[m], q, qinv));
     } else {
         const double2* tw = reinterpret_cast<const double2*>(pi.inv_d);
 #pragma unroll
@@ -650,6 +661,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
     c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
+    c.lazy = fwd_lazy(pi);
     const int logP = rows.logP;
     const bool red = rows.reduce_input != 0;
     // phase 1: this CTA's block, natural order, as residues in doubles
