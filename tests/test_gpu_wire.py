@@ -80,10 +80,22 @@ def test_round_trip_ckks_ring(cuda):
 
 
 def test_size_checks(cuda):
+    """Bad shapes are refused with a recorded error (read and cleared here, so no later
+    call sees it)."""
+    from vfhe_b200.native import EngineError
+
     ffi, lib = cuda.ffi, cuda.lib
     bits = ffi.new("uint32_t[]", [40, 33])
     assert lib.vfhe_cuda_packed_bytes(64, bits, 2, 3) == 3 * 64 * 73 // 8
+    cuda.check("valid shape")
     assert lib.vfhe_cuda_packed_bytes(32, bits, 2, 1) == 0  # 32 * 33 bits is not whole words
+    with pytest.raises(EngineError, match="multiple of 64"):
+        cuda.check()
     bad = ffi.new("uint32_t[]", [65])
     assert lib.vfhe_cuda_packed_bytes(64, bad, 1, 1) == 0
+    with pytest.raises(EngineError, match="1..64"):
+        cuda.check()
     assert lib.vfhe_cuda_pack_rows(ffi.NULL, ffi.NULL, 64, bits, 2, 1, ffi.NULL) != 0
+    with pytest.raises(EngineError, match="null buffers"):
+        cuda.check()
+    assert lib.vfhe_cuda_status() == 0
