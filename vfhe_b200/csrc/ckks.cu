@@ -384,73 +384,12 @@ __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __re
     }
 }
 
-// k_mac at split 1 for FP64 primes with every row 16-byte aligned and N even (the
-// launcher checks): pointwise products, two residues per thread (16-byte accesses: the
-// kernel streams the digits from HBM), partial sums reduced every four digits.  Its own
-// kernel so that its register count, not the general one's, sets the occupancy.
-__global__ void __launch_bounds__(256, 6) k_mac_pointwise(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
-                                                          const uint64_t* const* __restrict__ keys,
-                                                          const uint64_t* __restrict__ order,
-                                                          const __grid_constant__ LimbPrimes lp,
-                                                          const PrimeInfo* __restrict__ primes, int nd, int ne,
-                                                          long long N) {
-    const int by = blockIdx.y;
-    const int bo = by / ne, i = by - bo * ne;
-    const int b = order ? (int)order[bo] : bo;
-    const PrimeInfo& pi = primes[lp.p[i]];
-    const uint64_t* key = keys[b];
-    const long long dstride = (long long)ne * N;
-    const long long kstride = (long long)2 * ne * N;
-    const uint64_t* d = D + (long long)b * nd * dstride + (long long)i * N;
-    const uint64_t* ka = key + (long long)i * N;
-    const uint64_t* kb = ka + dstride;
-    uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N;
-    uint64_t* ob = oa + dstride;
-    // pointwise products, two residues per thread (16-byte accesses: the kernel streams
-    // the digits from HBM), partial sums reduced every four digits
-    const double q = pi.qd, qinv = pi.qinv;
-    for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
-         x += 2 * (long long)gridDim.x * blockDim.x) {
-        double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
-#pragma unroll 1
-        for (int j = 0; j < nd; ++j) {
-            // digits are read once: streaming loads leave L2 to the keys
-            const ulonglong2 dv = __ldcs(reinterpret_cast<const ulonglong2*>(d + j * dstride + x));
-            const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(ka + j * kstride + x);
-            const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(kb + j * kstride + x);
-            // the digit is the multiplier of both key products (one quotient for
-            // two products; uncentred operands below 2^50, each term |t| <= 3q/4)
-            const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
-            const double vq0 = __dmul_rn(v0, qinv), vq1 = __dmul_rn(v1, qinv);
-            const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
-            const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
-            sa0 = __dadd_rn(sa0, f_mulmod(wa0, v0, vq0, q));
-            sa1 = __dadd_rn(sa1, f_mulmod(wa1, v1, vq1, q));
-            sb0 = __dadd_rn(sb0, f_mulmod(wb0, v0, vq0, q));
-            sb1 = __dadd_rn(sb1, f_mulmod(wb1, v1, vq1, q));
-            if ((j & 3) == 3) {
-                sa0 = f_reduce(sa0, q, qinv);
-                sa1 = f_reduce(sa1, q, qinv);
-                sb0 = f_reduce(sb0, q, qinv);
-                sb1 = f_reduce(sb1, q, qinv);
-            }
-        }
-        ulonglong2 ra, rb;
-        ra.x = f_to_canonical(-sa0, q, qinv, pi.q);
-        ra.y = f_to_canonical(-sa1, q, qinv, pi.q);
-        rb.x = f_to_canonical(-sb0, q, qinv, pi.q);
-        rb.y = f_to_canonical(-sb1, q, qinv, pi.q);
-        *reinterpret_cast<ulonglong2*>(oa + x) = ra;
-        *reinterpret_cast<ulonglong2*>(ob + x) = rb;
-    }
-}
-
-// k_mac_pointwise with its operands staged through shared memory by bulk copies: block
-// (chunk, row) walks the digits of MAC_CHUNK residues of one extended limb, and thread 0
-// keeps MAC_STAGES digits (the digit chunk and both key chunks) in flight ahead of the
-// one being multiplied.  The digits stream from HBM; as plain loads only one digit per
-// thread was in flight and the kernel sat at half of DRAM bandwidth.  Needs N a multiple
-// of MAC_CHUNK and every row 16-byte aligned (checked by the launcher).
+// k_mac at split 1 for FP64 primes, its operands staged through shared memory by bulk
+// copies: block (chunk, row) walks the digits of kMacChunk residues of one extended
+// limb, and thread 0 keeps kMacStages digits (the digit chunk and both key chunks) in
+// flight ahead of the one being multiplied; the digits stream from HBM, the keys mostly
+// from L2.  Same result as k_mac<1>, which takes the shapes this kernel does not: N a
+// multiple of kMacChunk and every row 16-byte aligned (checked by the launcher).
 constexpr int kMacChunk = 512;   // residues per block: two per thread
 constexpr int kMacStages = 4;    // digits in flight per block
 constexpr int kMacStageWords = 3 * kMacChunk;
@@ -559,11 +498,6 @@ void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* con
         note_launch();
         const dim3 g((unsigned)(N / kMacChunk), (unsigned)(B * ne), 1);
         k_mac_staged<<<g, kMacChunk / 2, kMacSmem, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N);
-        return;
-    }
-    if (pointwise) {
-        k_mac_pointwise<<<grid_xy((N + 1) / 2, (long long)B * ne), 256, 0, st>>>(acc, D, keys, order, lpe, t->d_info,
-                                                                               nd, ne, N);
         return;
     }
     const dim3 g = grid_xy(N, (long long)B * ne);
