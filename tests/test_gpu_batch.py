@@ -32,7 +32,8 @@ def _setup(cuda, N, n_mid, pairs, steps, seed, split=1):
         return s, key, rlk, gks, cts
 
 
-@pytest.mark.parametrize("N,n_mid,split", [(2**12, 3, 1), (2**14, 8, 1), (2**12, 3, None), (2**13, 2, 2)])
+@pytest.mark.parametrize("N,n_mid,split", [(2**12, 3, 1), (2**14, 8, 1), (2**12, 3, None), (2**13, 2, 2),
+                                           (2**8, 2, 1)])
 def test_batched_ckks_matches_single_calls(cuda, N, n_mid, split):
     import torch
 
