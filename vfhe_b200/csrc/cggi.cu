@@ -133,6 +133,41 @@ __global__ void k_mac_shared(uint64_t* __restrict__ ext, const uint64_t* __restr
     const uint64_t* gb = ga + dstr;
     uint64_t* oa = ext + b * 2 * dstr + (long long)e * N;
     uint64_t* ob = oa + dstr;
+    if ((N & 1) == 0 &&
+        ((reinterpret_cast<uintptr_t>(d) | reinterpret_cast<uintptr_t>(ga) | reinterpret_cast<uintptr_t>(oa)) & 15) ==
+            0) {
+        // two residues per thread with 16-byte accesses; the digit is the multiplier of
+        // both key products (one quotient; uncentred operands below 2^50, |t| <= 3q/4)
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
+            for (int j = 0; j < nd; ++j) {
+                const ulonglong2 dv = __ldcs(reinterpret_cast<const ulonglong2*>(d + j * dstr + x));
+                const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(ga + j * gstr + x);
+                const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(gb + j * gstr + x);
+                const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
+                const double vq0 = __dmul_rn(v0, qinv), vq1 = __dmul_rn(v1, qinv);
+                sa0 = __dadd_rn(sa0, f_mulmod(f_from_u64(av.x), v0, vq0, q));
+                sa1 = __dadd_rn(sa1, f_mulmod(f_from_u64(av.y), v1, vq1, q));
+                sb0 = __dadd_rn(sb0, f_mulmod(f_from_u64(bv.x), v0, vq0, q));
+                sb1 = __dadd_rn(sb1, f_mulmod(f_from_u64(bv.y), v1, vq1, q));
+                if ((j & 3) == 3) {
+                    sa0 = f_reduce(sa0, q, qinv);
+                    sa1 = f_reduce(sa1, q, qinv);
+                    sb0 = f_reduce(sb0, q, qinv);
+                    sb1 = f_reduce(sb1, q, qinv);
+                }
+            }
+            ulonglong2 ra, rb;
+            ra.x = f_to_canonical(sa0, q, qinv, pi.q);
+            ra.y = f_to_canonical(sa1, q, qinv, pi.q);
+            rb.x = f_to_canonical(sb0, q, qinv, pi.q);
+            rb.y = f_to_canonical(sb1, q, qinv, pi.q);
+            *reinterpret_cast<ulonglong2*>(oa + x) = ra;
+            *reinterpret_cast<ulonglong2*>(ob + x) = rb;
+        }
+        return;
+    }
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x) {
         double sa = 0.0, sb = 0.0;
         for (int j = 0; j < nd; ++j) {
@@ -154,6 +189,9 @@ __global__ void k_mac_shared(uint64_t* __restrict__ ext, const uint64_t* __restr
 struct DivConsts {
     uint64_t half_sp[4], inv_sp[4], inv_sp_sh[4];
     uint64_t p, half_p;
+    // FP64 form (every prime below 2^50): p^-1 centred with its quotient fl(w/q)
+    int fp64;
+    double half_sp_d[4], inv_sp_d[4], inv_sp_dq[4];
 };
 
 // acc[b][c][l] += round(ext[b][c] / p) limb l   (round division by the special prime,
@@ -167,6 +205,33 @@ __global__ void k_moddown_acc(uint64_t* __restrict__ acc, const uint64_t* __rest
     const int c = blockIdx.y & 1;
     const uint64_t* ex = ext + (b * 2 + c) * ne * N;
     uint64_t* ac = acc + (b * 2 + c) * L0 * N;
+    if (dc.fp64 && (N & 1) == 0 && ((reinterpret_cast<uintptr_t>(ex) | reinterpret_cast<uintptr_t>(ac)) & 15) == 0) {
+        // exact FP64 form of the loop below (every intermediate an integer below 2^52),
+        // two coefficients per thread
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            const ulonglong2 sp = __ldcs(reinterpret_cast<const ulonglong2*>(ex + (long long)L0 * N + x));
+            uint64_t t0 = sp.x + dc.half_p, t1 = sp.y + dc.half_p;
+            t0 -= t0 >= dc.p ? dc.p : 0;
+            t1 -= t1 >= dc.p ? dc.p : 0;
+            const double td0 = f_from_u64(t0), td1 = f_from_u64(t1);
+            for (int l = 0; l < L0; ++l) {
+                const PrimeInfo& pi = primes[sh.lwe_prime[l]];
+                const ulonglong2 ev = __ldcs(reinterpret_cast<const ulonglong2*>(ex + (long long)l * N + x));
+                ulonglong2* ap = reinterpret_cast<ulonglong2*>(ac + (long long)l * N + x);
+                const ulonglong2 av = *ap;
+                const double y0 = __dadd_rn(__dadd_rn(f_from_u64(ev.x), dc.half_sp_d[l]), -td0);
+                const double y1 = __dadd_rn(__dadd_rn(f_from_u64(ev.y), dc.half_sp_d[l]), -td1);
+                const double v0 = __dadd_rn(f_mulmod(y0, dc.inv_sp_d[l], dc.inv_sp_dq[l], pi.qd), f_from_u64(av.x));
+                const double v1 = __dadd_rn(f_mulmod(y1, dc.inv_sp_d[l], dc.inv_sp_dq[l], pi.qd), f_from_u64(av.y));
+                ulonglong2 r;
+                r.x = f_to_canonical(v0, pi.qd, pi.qinv, pi.q);
+                r.y = f_to_canonical(v1, pi.qd, pi.qinv, pi.q);
+                *ap = r;
+            }
+        }
+        return;
+    }
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x) {
         const uint64_t t = add_mod(ex[(long long)L0 * N + x], dc.half_p, dc.p);
         for (int l = 0; l < L0; ++l) {
@@ -278,6 +343,15 @@ int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* 
         dc.inv_sp[l] = host_inv_mod(p % q, q);
         dc.inv_sp_sh[l] = host_shoup(dc.inv_sp[l], q);
     }
+    dc.fp64 = p < (1ULL << 50);
+    for (uint32_t l = 0; l < L0; ++l) {
+        const uint64_t q = t->info[limbs[l]].q;
+        dc.fp64 = dc.fp64 && q < (1ULL << 50);
+        const uint64_t w = dc.inv_sp[l];
+        dc.half_sp_d[l] = (double)dc.half_sp[l];
+        dc.inv_sp_d[l] = w > q / 2 ? (double)w - (double)q : (double)w;
+        dc.inv_sp_dq[l] = dc.inv_sp_d[l] / (double)q;
+    }
     const PrimeInfo* dp = t->d_info;
 
     // digit transforms: slot k = d * ne + e, d = c * L0 + l: diff row (b, c, l) lifted to ext limb e
@@ -348,13 +422,15 @@ int cggi_bootstrap(IncNtt* t, uint64_t* out_a, uint64_t* out_b, const uint64_t* 
         const uint64_t bk_stride = (uint64_t)nd * 2 * ne * N;
         int err = 0;
         for (uint32_t i = 0; i < n && !err; ++i) {
-            k_rot_diff<<<cg_grid(N, B * 2 * L0), 256, 0, cs>>>(diff, acc, rots + (uint64_t)i * B, sh, dp);
+            // four coefficients per thread: at N = 1024 one block per row, so the launch is
+            // not bound by the block rate
+            k_rot_diff<<<cg_grid((N + 3) / 4, B * 2 * L0), 256, 0, cs>>>(diff, acc, rots + (uint64_t)i * B, sh, dp);
             err = launch_ntt(dig, dp, false, cs);
             if (err) break;
-            k_mac_shared<<<cg_grid(N, B * ne), 256, 0, cs>>>(ext, D, bk + i * bk_stride, sh, dp, nd);
+            k_mac_shared<<<cg_grid((N + 1) / 2, B * ne), 256, 0, cs>>>(ext, D, bk + i * bk_stride, sh, dp, nd);
             err = launch_ntt(inv, dp, true, cs);
             if (err) break;
-            k_moddown_acc<<<cg_grid(N, B * 2), 256, 0, cs>>>(acc, ext, sh, dc, dp);
+            k_moddown_acc<<<cg_grid((N + 1) / 2, B * 2), 256, 0, cs>>>(acc, ext, sh, dc, dp);
         }
         cudaGraph_t graph = nullptr;
         const cudaError_t e1 = cudaStreamEndCapture(cs, &graph);
