@@ -82,6 +82,12 @@ __global__ void __launch_bounds__(kWlThreads) k_wl_product(const ProdDesc* __res
         av[j] = d.a[j * P + x];
         bv[j] = d.b[j * P + x];
     }
+    if (S == 1 && pi.fp64) {
+        // exact FP64 product of canonical operands (uncentred, below 2^50: |t| <= 3q/4)
+        const double fa = f_from_u64(av[0]), fb = f_from_u64(bv[0]);
+        d.out[x] = f_to_canonical(f_mulmod(fa, fb, __dmul_rn(fb, pi.qinv), pi.qd), pi.qd, pi.qinv, q);
+        return;
+    }
     const ulonglong2 w = S > 1 ? reinterpret_cast<const ulonglong2*>(pi.twist)[x] : make_ulonglong2(0, 0);
 #pragma unroll
     for (int o = 0; o < S; ++o) {
@@ -128,6 +134,20 @@ __global__ void __launch_bounds__(kWlThreads) k_wl_moddown(const DownDesc* __res
     const long long x = chunk * kWlThreads + threadIdx.x;
     if (x >= N) return;
     const ModDownConsts& mc = *d.mc;
+    if (mc.fp64) {
+        // exact FP64 form of the loop below (every intermediate an integer below 2^52)
+        uint64_t t = d.acc[(long long)d.nl * N + x] + mc.half_p;
+        t -= t >= mc.p ? mc.p : 0;
+        const double td = f_from_u64(t);
+        for (int i = 0; i < d.nl; ++i) {
+            const PrimeInfo& pi = primes[mc.prime[i]];
+            const double y = __dadd_rn(__dadd_rn(f_from_u64(d.acc[(long long)i * N + x]), mc.half_sp_d[i]), -td);
+            double v = f_mulmod(y, mc.inv_sp_d[i], mc.inv_sp_dq[i], pi.qd);
+            if (d.pass) v = __dadd_rn(v, f_from_u64(d.pass[(long long)i * N + x]));
+            d.out[(long long)i * N + x] = f_to_canonical(v, pi.qd, pi.qinv, pi.q);
+        }
+        return;
+    }
     const uint64_t t = add_mod(d.acc[(long long)d.nl * N + x], mc.half_p, mc.p);
     for (int i = 0; i < d.nl; ++i) {
         const PrimeInfo& pi = primes[mc.prime[i]];
