@@ -37,7 +37,7 @@ def candidates(logP: int) -> list[tuple[int, int, int]]:
     out = []
     for k in sorted(tiles):
         tpt = 1 << (k - 4)
-        tpcs = [0] + [t for t in (1, 2, 4, 8) if tpt * t <= max(256, tpt) and tpt * t >= 128]
+        tpcs = [0] + [t for t in (1, 2, 4, 8) if tpt * t <= max(256, tpt) and tpt * t >= 64]
         for tpc in sorted(set(tpcs)):
             for cps in (0, 2, 4):
                 out.append((k, tpc, cps))
