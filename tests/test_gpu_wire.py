@@ -7,25 +7,9 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+from tests.wire_helpers import pack_rows_host
+
 pytestmark = pytest.mark.gpu
-
-
-def pack_rows_host(rows: np.ndarray, bits: list[int]) -> np.ndarray:
-    """[B][R][N] uint64 -> [B][bytes] uint8: row r as N fields of bits[r] bits, least
-    significant bit first, rows of an item one after another."""
-    B, R, N = rows.shape
-    assert R == len(bits)
-    out = []
-    for i in range(B):
-        parts = []
-        for r, b in enumerate(bits):
-            v = rows[i, r].astype(np.uint64)
-            if b < 64:
-                v = v & np.uint64((1 << b) - 1)
-            bitarr = ((v[:, None] >> np.arange(b, dtype=np.uint64)[None, :]) & np.uint64(1)).astype(np.uint8)
-            parts.append(np.packbits(bitarr.reshape(-1), bitorder="little"))
-        out.append(np.concatenate(parts))
-    return np.stack(out)
 
 
 def _rows(rng, B, bits, N):

@@ -1,0 +1,53 @@
+"""The compact wire format's host side, without a GPU: the size the library reports
+for a layout, its refusal of layouts that are not whole 64-bit words, and the numpy
+restatement that the GPU tests check the kernels against (a round trip here)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.wire_helpers import pack_rows_host, unpack_rows_host
+
+
+@pytest.fixture(scope="module")
+def lib_engine():
+    from vfhe_b200 import build
+    from vfhe_b200.native import Engine
+
+    if not build.LIB.exists():
+        build.build()
+    return Engine(build.LIB)
+
+
+def test_packed_bytes(lib_engine):
+    ffi, lib = lib_engine.ffi, lib_engine.lib
+    bits = ffi.new("uint32_t[]", ([50] + [40] * 8) * 2)
+    assert lib.vfhe_cuda_packed_bytes(1 << 14, bits, 18, 256) == 256 * (1 << 14) * 740 // 8
+    lib_engine.check("valid layout")
+    odd = ffi.new("uint32_t[]", [33])
+    assert lib.vfhe_cuda_packed_bytes(32, odd, 1, 1) == 0
+    assert lib.vfhe_cuda_status() != 0
+    lib.vfhe_cuda_clear_error()
+    assert lib.vfhe_cuda_packed_bytes(64, ffi.new("uint32_t[]", [0]), 1, 1) == 0
+    lib.vfhe_cuda_clear_error()
+    assert lib.vfhe_cuda_packed_bytes(64, bits, 129, 1) == 0
+    lib.vfhe_cuda_clear_error()
+
+
+@pytest.mark.parametrize("bits,N", [([50, 40, 40], 64), ([1, 7, 13, 31, 33, 63, 64, 8], 64), ([37, 41], 128)])
+def test_host_packer_round_trip(bits, N):
+    rng = np.random.default_rng(N + len(bits))
+    rows = np.stack([np.stack([rng.integers(0, 1 << b, N, dtype=np.uint64) if b < 64
+                               else rng.integers(0, 2**64, N, dtype=np.uint64) for b in bits]) for _ in range(3)])
+    packed = pack_rows_host(rows, bits)
+    assert packed.shape == (3, N * sum(bits) // 8)
+    assert np.array_equal(unpack_rows_host(packed, bits, N), rows)
+
+
+def test_host_packer_bit_order():
+    """Residue x of a row occupies bits [x b, x b + b), least significant bit first."""
+    rows = np.array([[[1, 2, 3, 4, 5, 6, 7, 8]]], dtype=np.uint64)
+    assert pack_rows_host(rows, [8]).tolist() == [[1, 2, 3, 4, 5, 6, 7, 8]]
+    rows = np.array([[[0b101] + [0] * 63]], dtype=np.uint64)
+    assert pack_rows_host(rows, [3])[0, 0] == 0b101
