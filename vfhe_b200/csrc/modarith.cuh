@@ -46,6 +46,11 @@ struct PrimeInfo {
     // consecutive blocks reads 32 consecutive (w, fl(w/q)) pairs per slot.
     const double* fwd_lane;
     const double* inv_lane;
+    // The stages at index bits 2..5 the same way, by group G of 64 residues (P >= 64,
+    // else null): slot s = 2^(3-b') - 1 + h for bit b' + 2, at ((G >> 5) * 15 + s) * 32
+    // + (G & 31); a radix-16 pass over bits 2..5 gives a warp 8 consecutive groups.
+    const double* fwd_mid;
+    const double* inv_mid;
 };
 
 VC_HD uint64_t umulhi(uint64_t a, uint64_t b) {

@@ -36,6 +36,7 @@ struct FCtx {
     double q, qinv;
     const double2* tw;
     const double2* lt;  // lane-major twiddles of bits 0..3 (PrimeInfo::fwd_lane / inv_lane)
+    const double2* mt;  // the same for bits 2..5 by 64-residue group (fwd_mid / inv_mid)
     bool lazy = false;  // forward: skip the reductions between passes (fwd_lazy)
 };
 
@@ -135,6 +136,12 @@ __device__ __forceinline__ void f_fwd_tw(PassTw<LO, BHI, BLO>& T, int t, int hi,
 #pragma unroll
             for (int h = 0; h < (1 << (3 - bb)); ++h)
                 T.w[PassTw<LO, BHI, BLO>::offset(b) + h] = __ldg(&c.lt[lane_tw_index(g, b, h)]);
+        } else if constexpr (LO == 2 && K >= 6) {
+            // four threads per 64-residue group: a warp's loads are 8 consecutive pairs
+            const int g = (hi << (K - 6)) + (t >> 2);
+#pragma unroll
+            for (int h = 0; h < (1 << (3 - bb)); ++h)
+                T.w[PassTw<LO, BHI, BLO>::offset(b) + h] = __ldg(&c.mt[lane_tw_index(g, bb, h)]);
         } else {
             const int base = (1 << (logP - 1 - b)) + (hi << (K - b - 1));
 #pragma unroll
@@ -183,6 +190,11 @@ __device__ __forceinline__ void f_inv_tw(PassTw<LO, BLO, BHI>& T, int t, int hi,
 #pragma unroll
             for (int h = 0; h < (1 << (3 - bb)); ++h)
                 T.w[PassTw<LO, BLO, BHI>::offset(b) + h] = __ldg(&c.lt[lane_tw_index(g, b, h)]);
+        } else if constexpr (LO == 2 && K >= 6) {
+            const int g = (hi << (K - 6)) + (t >> 2);
+#pragma unroll
+            for (int h = 0; h < (1 << (3 - bb)); ++h)
+                T.w[PassTw<LO, BLO, BHI>::offset(b) + h] = __ldg(&c.mt[lane_tw_index(g, bb, h)]);
         } else {
             const int base = ((1 << logP) >> (b + 1)) + (hi << (K - b - 1));
 #pragma unroll
@@ -365,6 +377,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value, TileMinBlocks<K>::value
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
     c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
+    c.mt = reinterpret_cast<const double2*>(pi.fwd_mid);
     c.lazy = fwd_lazy(pi);
     const int logP = rows.logP, hi = r.hi;
     double x[16];
@@ -461,6 +474,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value, TileMinBlocks<K>::value
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.inv_d);
     c.lt = reinterpret_cast<const double2*>(pi.inv_lane);
+    c.mt = reinterpret_cast<const double2*>(pi.inv_mid);
     const int logP = rows.logP, hi = r.hi;
     double x[16];
 
@@ -661,6 +675,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
     c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
+    c.mt = reinterpret_cast<const double2*>(pi.fwd_mid);
     c.lazy = fwd_lazy(pi);
     const int logP = rows.logP;
     const bool red = rows.reduce_input != 0;
@@ -756,6 +771,7 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_inv_f(const __g
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.inv_d);
     c.lt = reinterpret_cast<const double2*>(pi.inv_lane);
+    c.mt = reinterpret_cast<const double2*>(pi.inv_mid);
     const int logP = rows.logP, hi = rank;
     // phase 1: inverse tile passes over the low K bits of this block
     double x[16];

@@ -341,8 +341,22 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
                 inv_l[2 * dst] = inv_d[2 * src];
                 inv_l[2 * dst + 1] = inv_d[2 * src + 1];
             }
+    // the same for the stages at bits 2..5, by 64-residue group G (layout described
+    // with PrimeInfo)
+    const uint64_t ngrp = P / 64, mid_pairs = ((ngrp + 31) / 32) * 15 * 32;
+    std::vector<double> fwd_m(2 * mid_pairs, 0.0), inv_m(2 * mid_pairs, 0.0);
+    for (uint64_t g = 0; g < ngrp && fp64; ++g)
+        for (int bb = 0; bb < 4; ++bb)
+            for (uint64_t h = 0; h < (1u << (3 - bb)); ++h) {
+                const uint64_t src = (P >> (bb + 3)) + (g << (3 - bb)) + h;
+                const uint64_t dst = (((g >> 5) * 15 + ((1u << (3 - bb)) - 1) + h) << 5) + (g & 31);
+                fwd_m[2 * dst] = fwd_d[2 * src];
+                fwd_m[2 * dst + 1] = fwd_d[2 * src + 1];
+                inv_m[2 * dst] = inv_d[2 * src];
+                inv_m[2 * dst + 1] = inv_d[2 * src + 1];
+            }
     void* blk = nullptr;
-    const size_t bytes = sizeof(uint64_t) * (10 * P + 4 * lane_pairs);
+    const size_t bytes = sizeof(uint64_t) * (10 * P + 4 * lane_pairs + 4 * mid_pairs);
     if (!check_cuda(cudaMalloc(&blk, bytes), "table alloc")) return false;
     uint64_t* d = (uint64_t*)blk;
     if (!check_cuda(cudaMemcpy(d, fwd.data(), 16 * P, cudaMemcpyHostToDevice), "table upload") ||
@@ -353,6 +367,11 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
         !check_cuda(cudaMemcpy(d + 10 * P, fwd_l.data(), 16 * lane_pairs, cudaMemcpyHostToDevice), "table upload") ||
         !check_cuda(cudaMemcpy(d + 10 * P + 2 * lane_pairs, inv_l.data(), 16 * lane_pairs, cudaMemcpyHostToDevice),
                     "table upload"))
+        return false;
+    uint64_t* dm = d + 10 * P + 4 * lane_pairs;
+    if (mid_pairs && (!check_cuda(cudaMemcpy(dm, fwd_m.data(), 16 * mid_pairs, cudaMemcpyHostToDevice), "table upload") ||
+                      !check_cuda(cudaMemcpy(dm + 2 * mid_pairs, inv_m.data(), 16 * mid_pairs, cudaMemcpyHostToDevice),
+                                  "table upload")))
         return false;
     t->dev_blocks.push_back(blk);
 
@@ -376,6 +395,8 @@ bool build_prime(IncNtt* t, uint64_t q, PrimeInfo* out, _NTT_proc* proc,
     o.inv_d = reinterpret_cast<const double*>(d + 8 * P);
     o.fwd_lane = reinterpret_cast<const double*>(d + 10 * P);
     o.inv_lane = reinterpret_cast<const double*>(d + 10 * P + 2 * lane_pairs);
+    o.fwd_mid = mid_pairs ? reinterpret_cast<const double*>(dm) : nullptr;
+    o.inv_mid = mid_pairs ? reinterpret_cast<const double*>(dm + 2 * mid_pairs) : nullptr;
     o.fp64 = fp64 ? 1 : 0;
     o.qd = (double)q;
     o.qinv = 1.0 / (double)q;
