@@ -13,7 +13,7 @@ import pytest
 
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "ntt_kats.json").read_text())
 
-SURVEY_KAT = [  # (N, split, fwd[0:4] of limb 0, w[0][0:2])
+REFERENCE_KAT = [  # (N, split, fwd[0:4] of limb 0, w[0][0:2])
     (4096, 4, [822099881308752, 886061694057521, 82400588911197, 891213608007162], [220465343233214, 905434563586883]),
     (4096, 1, [476757054511894, 540532001433779, 445267771961344, 397498397173953], [371347710277771, 754552196147062]),
     (2**14, 1, [1083056184672557, 455098839724364, 67796770342872, 673087944409817],
@@ -64,7 +64,7 @@ def check_engine(engine):
 
 
 def test_fixture_agrees_with_the_survey_table():
-    for (N, split, fwd4, w2), case in zip(SURVEY_KAT, GOLDEN["forward"]):
+    for (N, split, fwd4, w2), case in zip(REFERENCE_KAT, GOLDEN["forward"]):
         assert (case["N"], case["split"]) == (N, split)
         assert case["head"][0][:4] == fwd4
         assert case["w0"][:2] == w2
