@@ -337,7 +337,11 @@ int vfhe_cuda_ntt_mul_intt_batch_noalloc(void *ntt, uint64_t *d_out, const uint6
  * `batch` entries (Galois elements, device key pointers).
  *
  * Scratch comes from `workspace` (device memory of at least the size returned by the
- * matching *_workspace_bytes call); pass NULL to let the engine allocate it. */
+ * matching *_workspace_bytes call); pass NULL to let the engine allocate it.  Engine-
+ * owned scratch is one buffer per stream, shared by every NULL-workspace call and every
+ * vfhe_cuda_ntt_mul_intt_batch call on that stream (stream order keeps them apart);
+ * calls on different streams use different buffers.  Growing a stream's buffer
+ * synchronises that stream. */
 uint64_t vfhe_cuda_ckks_mul_workspace_bytes(void *ntt, uint64_t batch, uint32_t nlimbs);
 int vfhe_cuda_ckks_mul_relin_rescale_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct1,
                                            const uint64_t *d_ct2, uint64_t batch,
@@ -442,6 +446,16 @@ int vfhe_cuda_ntt_get_schedule(uint32_t logP, uint64_t rows, int32_t *out3);
  * or the staged key-switch MAC; its results are then wrong); -1 when the flags cannot
  * be read.  Stays 0 in normal operation. */
 int vfhe_cuda_device_faults(void);
+
+/* Reset the flags vfhe_cuda_device_faults reads.  0 on success. */
+int vfhe_cuda_clear_device_faults(void);
+
+/* Self-check of the bounded-wait machinery (no reference counterpart): runs a one-thread
+ * kernel that waits, at most `tries` attempts, on an mbarrier that no copy completes.
+ * The wait must give up, raise the flag vfhe_cuda_device_faults reads, and return with
+ * the context usable.  Returns 1 when it gave up as designed, 0 if it did not, -1 on a
+ * CUDA error.  Clear the flag afterwards with vfhe_cuda_clear_device_faults. */
+int vfhe_cuda_selfcheck_bounded_wait(int32_t tries);
 
 /* Work list: independent jobs of any mix of ring degree and limb count, run as ONE
  * CUDA-graph launch (grouped per transform pool; each stage of a group is one launch

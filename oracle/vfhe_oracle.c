@@ -12,7 +12,7 @@
  * exact modular arithmetic on canonical residues; there is no random sampling here
  * (tests inject seeded inputs).
  *
- * Parity pins: tests/test_oracle.py checks this oracle against the golden vectors in
+ * Parity pins: tests/test_golden.py and tests/test_oracle_arith.py check this oracle against the golden vectors in
  * tests/golden/ (made by running the reference built from its own sources) and
  * against the reference library itself when it is present.
  */

@@ -102,6 +102,21 @@ def _fresh_prime_pools():
     reset_registries()
 
 
+@pytest.fixture(autouse=True)
+def _no_device_faults(request):
+    """After every GPU test: no kernel's bounded wait for a bulk copy gave up (a wait
+    that gives up raises a device flag and leaves wrong results behind)."""
+    yield
+    if request.node.get_closest_marker("gpu") is None:
+        return
+    from vfhe_b200 import native
+
+    eng = native._CUDA
+    if eng is None:
+        return
+    assert eng.lib.vfhe_cuda_device_faults() == 0, "a bounded device wait gave up during this test"
+
+
 def has_ifma() -> bool:
     try:
         return "avx512ifma" in Path("/proc/cpuinfo").read_text()

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "abi_common.cuh"
@@ -57,23 +59,35 @@ bool batch_rowset(IncNtt* t, uint64_t* d_out, const uint64_t* d_in, uint64_t bat
     return true;
 }
 
-// Scratch owned by the engine when the caller passes no workspace: grown on demand,
-// recycled only after the stream that used it has drained.
+// Scratch owned by the engine when the caller passes no workspace: one buffer per
+// stream, grown on demand.  Calls on one stream are ordered by that stream, so they
+// may share its buffer; calls on different streams get different buffers and never
+// race on scratch contents.  A buffer is freed only after its own stream has drained.
+// The map is guarded by a mutex, so host threads may call concurrently.
 uint64_t* engine_workspace(size_t bytes, cudaStream_t st) {
-    static void* buf = nullptr;
-    static size_t cap = 0;
-    if (bytes > cap) {
-        cudaStreamSynchronize(st);
-        if (buf) cudaFree(buf);
-        buf = nullptr;
-        cap = 0;
-        if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+    struct Buf {
+        void* p;
+        size_t cap;
+    };
+    static std::mutex mu;
+    static std::unordered_map<cudaStream_t, Buf> bufs;
+    std::lock_guard<std::mutex> lk(mu);
+    Buf& b = bufs[st];
+    if (bytes > b.cap) {
+        if (b.p) {
+            cudaStreamSynchronize(st);
+            cudaFree(b.p);
+        }
+        b.p = nullptr;
+        b.cap = 0;
+        if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+            b.p = nullptr;
             set_error("workspace", "cudaMalloc failed");
             return nullptr;
         }
-        cap = bytes;
+        b.cap = bytes;
     }
-    return (uint64_t*)buf;
+    return (uint64_t*)b.p;
 }
 
 }  // namespace
@@ -235,6 +249,24 @@ int vfhe_cuda_device_faults(void) {
     int m = 0;
     if (!check_cuda(read_mac_fault(&m), "vfhe_cuda_device_faults")) return -1;
     return f | m;
+}
+
+int vfhe_cuda_clear_device_faults(void) {
+    if (!vc::ensure_ready()) return 1;
+    if (!check_cuda(clear_tile_fault(), "vfhe_cuda_clear_device_faults")) return 1;
+    if (!check_cuda(clear_mac_fault(), "vfhe_cuda_clear_device_faults")) return 1;
+    return 0;
+}
+
+int vfhe_cuda_selfcheck_bounded_wait(int32_t tries) {
+    if (!vc::ensure_ready()) return -1;
+    if (tries <= 0) {
+        set_error("vfhe_cuda_selfcheck_bounded_wait", "tries must be positive");
+        return -1;
+    }
+    int gave_up = 0;
+    if (!check_cuda(bounded_wait_selfcheck((int)tries, &gave_up), "vfhe_cuda_selfcheck_bounded_wait")) return -1;
+    return gave_up;
 }
 
 int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_bits, int32_t tiles_per_cta,

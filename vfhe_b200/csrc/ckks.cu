@@ -717,6 +717,44 @@ int read_mac_fault(int* out) {
     return (int)cudaMemcpyFromSymbol(out, vc_mac_fault, sizeof(int));
 }
 
+int clear_mac_fault() {
+    const int zero = 0;
+    return (int)cudaMemcpyToSymbol(vc_mac_fault, &zero, sizeof(int));
+}
+
+namespace {
+// Self-check of the bounded wait: one thread arms an mbarrier for 16 bytes that no copy
+// will ever deliver and waits on it with the same bounded retry loop the staged kernels
+// use, so the wait must give up, set vc_mac_fault and return.  No copy is issued, so
+// nothing can land in shared memory after the block exits.
+__global__ void k_bounded_wait_selfcheck(int tries, int* gave_up) {
+    __shared__ uint64_t bar;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(&bar, 16);
+    int i = 0;
+    while (i < tries && !mbar_try_wait(&bar, 0)) ++i;
+    if (i == tries) {
+        atomicExch(&vc_mac_fault, 1);
+        *gave_up = 1;
+    }
+}
+}  // namespace
+
+int bounded_wait_selfcheck(int tries, int* gave_up_host) {
+    int* d = nullptr;
+    int e = (int)cudaMalloc(&d, sizeof(int));
+    if (e) return e;
+    e = (int)cudaMemset(d, 0, sizeof(int));
+    if (!e) {
+        k_bounded_wait_selfcheck<<<1, 1>>>(tries, d);
+        e = (int)cudaGetLastError();
+    }
+    if (!e) e = (int)cudaMemcpy(gave_up_host, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e;
+}
+
 ModDownConsts moddown_consts(IncNtt* t, const uint32_t* limbs, int nl, uint32_t special) {
     ModDownConsts mc;
     memset(&mc, 0, sizeof mc);

@@ -57,6 +57,9 @@ int vfhe_cuda_ntt_mul_intt_batch_noalloc(void* ntt, uint64_t* d_out, const uint6
                                          uint64_t batch, const uint32_t* limbs, uint32_t nlimbs, void* stream_) {
     static const char* const where = "vfhe_cuda_ntt_mul_intt_batch_noalloc";
     using namespace vc;
+    // ensure_ready only selects the device and creates the engine's stream; it
+    // allocates no device memory
+    if (!ensure_ready()) return 1;
     IncNtt* t = as_ntt(ntt);
     if (!t || !limbs || !d_out || !d_a || !d_b || nlimbs == 0 || nlimbs > (uint32_t)kMaxLimbs || batch == 0) {
         set_error(where, "bad pool, buffers or limb list");
@@ -73,10 +76,9 @@ int vfhe_cuda_ntt_mul_intt_batch_noalloc(void* ntt, uint64_t* d_out, const uint6
             set_error(where, "limb index outside the pool");
             return 1;
         }
-    if (ctx().ready) {
+    {
         int dev = -1;
-        cudaGetDevice(&dev);
-        if (dev != ctx().device) {
+        if (cudaGetDevice(&dev) != cudaSuccess || dev != ctx().device) {
             set_error(where, "call with the engine's device current (its tables live there)");
             return 1;
         }

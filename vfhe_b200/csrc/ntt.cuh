@@ -103,6 +103,7 @@ int prepare_ntt_kernels();
 // Copy the device flag that persistent transform kernels raise when a bounded wait
 // for a tile copy gave up (0 = never).
 int read_tile_fault(int* out);
+int clear_tile_fault();
 
 // Kernel attributes of the batched CKKS kernels (the staged key-switch MAC's shared
 // memory), set once; prepare_ntt_kernels calls it too.
@@ -111,5 +112,11 @@ int prepare_ckks_kernels();
 // Copy the device flag that the staged key-switch MAC raises when a bounded wait for
 // a bulk copy gave up (0 = never).
 int read_mac_fault(int* out);
+int clear_mac_fault();
+
+// Launch a one-thread kernel whose bounded mbarrier wait can never be satisfied (a
+// transaction count no copy delivers) with a limit of `tries` attempts; on return
+// *gave_up is 1 when the wait gave up and raised the staged-MAC fault flag.
+int bounded_wait_selfcheck(int tries, int* gave_up);
 
 }  // namespace vc

@@ -1066,6 +1066,11 @@ int read_tile_fault(int* out) {
     return (int)cudaMemcpyFromSymbol(out, vc_tile_fault, sizeof(int));
 }
 
+int clear_tile_fault() {
+    const int zero = 0;
+    return (int)cudaMemcpyToSymbol(vc_tile_fault, &zero, sizeof(int));
+}
+
 int prepare_ntt_kernels() {
     int e = prepare_ckks_kernels();
     if (!e) e = prepare_k<8>();
