@@ -11,9 +11,9 @@ from fixed seeds.
 
 Prints one JSON line (rank 0).  ``value`` is pairs per second over all ranks with
 ciphertexts already in HBM; ``e2e`` adds the host->device copy of each step's input
-ciphertexts from pinned memory and the device->host copy of its results, moved in the
-compact wire format (residues at their primes' bit lengths; plain uint64 rows timed
-beside it).  The
+ciphertexts (uint64 residue rows) from pinned memory and the device->host copy of its
+results; the same step moving ciphertexts in the compact wire format (residues at their
+primes' bit lengths, as a sender would ship them) is timed beside it.  The
 reference arm runs the reference's own CPU library (built from its sources into
 oracle/_ref/) on the same workload, one process per host core.
 """
@@ -300,6 +300,69 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
     return res
 
 
+def _balanced_digits(c: np.ndarray, base_log: int, levels: int) -> np.ndarray:
+    """Signed gadget digits of 32-bit torus values: round to base_log * levels bits, then
+    digits in [-B/2, B/2) from the least significant up with a carry (the decomposition
+    the FFT external product applies).  Returns [levels][...] int64, most significant
+    digit first."""
+    total = base_log * levels
+    r = ((c.astype(np.uint64) + (1 << (31 - total))) >> (32 - total)) & ((1 << total) - 1)
+    r = r.astype(np.int64)
+    half, full = 1 << (base_log - 1), 1 << base_log
+    out = np.zeros((levels,) + c.shape, dtype=np.int64)
+    for lvl in range(levels - 1, -1, -1):
+        d = r & (full - 1)
+        r >>= base_log
+        carry = d >= half
+        d = np.where(carry, d - full, d)
+        r = r + carry
+        out[lvl] = d
+    return out
+
+
+def fft_product_error(eng, keys, dev, p, count: int = 8) -> dict:
+    """Max absolute error of the GPU's FP64-FFT external product (GLWE x GGSW(s_0)) against
+    the exact integer negacyclic product, computed here in int64 (every partial sum of
+    digit x 32-bit key coefficient products stays below 2^52), over `count` random GLWE
+    ciphertexts; errors are distances on the 2^32 torus."""
+    import torch
+
+    from vfhe_b200.cggi_fft import to_device, to_host
+
+    N, lv, bl = p.N, p.bs_levels, p.bs_base_log
+    rng = np.random.default_rng(SEED + 31)
+    c = rng.integers(0, 1 << 32, (count, 2 * N), dtype=np.uint64).astype(np.uint32)
+    out = torch.empty((count, 2 * N), dtype=torch.int32, device="cuda")
+    frac = torch.empty(count, dtype=torch.float64, device="cuda")
+    ffi = eng.ffi
+    dc = to_device(c)
+    rc = eng.lib.vfhe_cuda_cggi_fft_external_product(
+        ffi.cast("uint32_t*", out.data_ptr()), ffi.cast("uint32_t*", dc.data_ptr()), count,
+        ffi.cast("double*", dev.bsk_f[: 2 * lv * 2].data_ptr()), N, bl, lv, ffi.cast("double*", frac.data_ptr()),
+        ffi.cast("void*", torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    got = to_host(out).astype(np.uint32).astype(np.int64)
+    ggsw = np.asarray(keys.bsk[0], dtype=np.uint32).astype(np.int64).reshape(2 * lv, 2, N)
+    worst = 0
+    for b in range(count):
+        dig = _balanced_digits(c[b].reshape(2, N), bl, lv)  # [lv][comp][N]
+        exact = np.zeros((2, N), dtype=np.int64)
+        for comp in range(2):
+            for lvl in range(lv):
+                row = comp * lv + lvl
+                for oc in range(2):
+                    full = np.convolve(dig[lvl, comp], ggsw[row, oc])
+                    exact[oc] += full[:N]
+                    exact[oc, : N - 1] -= full[N:]
+        diff = (got[b].reshape(2, N) - exact) & 0xFFFFFFFF
+        dist = np.minimum(diff, (1 << 32) - diff)
+        worst = max(worst, int(dist.max()))
+    return {"max_abs_error": worst, "unit": "torus units (2^-32)", "products": count,
+            "max_rounding_fraction": float(frac.max()),
+            "reference": "exact integer negacyclic product (int64), same signed digits"}
+
+
 def cggi_fft_leg(eng, count: int, reps: int, million: bool = False) -> dict:
     """Torus CGGI programmable bootstrap (n = 630, N = 1024, base 2^7 x 3, key switch
     2^2 x 8): `count` LWEs of random 4-bit messages through one seeded 16-entry table
@@ -348,19 +411,24 @@ def cggi_fft_leg(eng, count: int, reps: int, million: bool = False) -> dict:
         "mismatches": int((keys.decrypt(res_host) != lut[m]).sum()),
         "phase_error_mean": float(err.mean()), "phase_error_max": float(err.max()),
     }
+    res["fft_external_product"] = fft_product_error(eng, keys, dev, p)
     if million:
         total, bad, bad_ext, worst, worst_ext = 0, 0, 0, 0.0, 0.0
+        mc = 16384  # LWEs per batch of the 10^6 run
         while total < 1_000_000:
-            mm = rng.integers(0, p.t, count)
+            mm = rng.integers(0, p.t, mc)
             e = dev.blind_rotate(to_device(keys.encrypt(mm, rng)), tv)
             o, eh = to_host(dev.keyswitch(e)), to_host(e)
             bad += int((keys.decrypt(o) != lut[mm]).sum())
             bad_ext += int((keys.decrypt(eh, keys.S) != lut[mm]).sum())
             worst = max(worst, float((np.abs(keys.phases(o) - lut[mm] * p.delta) / 2.0**32).max()))
             worst_ext = max(worst_ext, float((np.abs(keys.phases(eh, keys.S) - lut[mm] * p.delta) / 2.0**32).max()))
-            total += count
+            total += mc
         res["million"] = {"bootstraps": total, "mismatches_extracted": bad_ext, "phase_error_extracted_max": worst_ext,
-                          "mismatches": bad, "phase_error_max": worst}
+                          "mismatches": bad, "phase_error_max": worst,
+                          "note": "mismatches_extracted counts the bootstrapped LWEs (blind rotation + sample "
+                                  "extraction, the reference's functional_bootstrap); mismatches adds the LWE key "
+                                  "switch back to n = 630, whose key carries the LWE noise sigma 2^-15"}
     del dev
     torch.cuda.empty_cache()
     return res
@@ -421,26 +489,133 @@ def rns_cggi_leg(eng, count: int = 1024, cpu_bootstraps: int = 2) -> dict:
     profile_range(None, "cggi_rns", False)
     ms = e0.elapsed_time(e1)
     ha, hb = to_host(oa), to_host(ob)
-    bad = 0
+    def phase_error(ph: int, want: int, q: int) -> float:
+        """Distance of a phase from want * q / 32 on the ring Z_q, as a fraction of q."""
+        d = (ph - round(want * q / 32)) % q
+        return min(d, q - d) / q
+
+    bad, errs = 0, []
     for i in range(min(count, 64)):
         o = LWE(ring=in_ring, n=1024)
         o.set_rows(ha[i], hb[i])
         ph = o.phase(key2, recompose=True)
         bad += int(round(ph * 32 / in_ring.q_l) % 32 != lut[msgs[i]])
+        errs.append(phase_error(ph, lut[msgs[i]], in_ring.q_l))
     res = {"workload": f"{count} LWEs, n=630, N=1024, RNS gadget over 2 x 50-bit primes + 1 special, 16-entry LUT",
            "gpu_bootstraps_per_s": count / (ms * 1e-3), "gpu_ms": ms, "checked": min(count, 64),
-           "mismatches": bad}
+           "mismatches": bad, "phase_error_mean": float(np.mean(errs)), "phase_error_max": float(np.max(errs)),
+           "phase_error_unit": "fraction of Q (half box = 1/64)"}
     lib, name = _ref_library()
     if lib.exists() and cpu_bootstraps > 0:
         from vfhe_b200.native import Engine
 
         ref = Engine(lib)
-        rs, rcg, rbk, rtv, rlwes, _, _, rin, _ = _rns_cggi_setup(ref, 630, cpu_bootstraps, SEED + 12)
+        rs, rcg, rbk, rtv, rlwes, rmsgs, rlut, rin, rkey2 = _rns_cggi_setup(ref, 630, cpu_bootstraps, SEED + 12)
+        routs = [LWE(ring=rin) for _ in rlwes]
         t0 = time.perf_counter()
-        for x in rlwes:
-            rcg.functional_bootstrap(LWE(ring=rin), rtv, x, rbk, torus_base=16)
+        for x, o in zip(rlwes, routs):
+            rcg.functional_bootstrap(o, rtv, x, rbk, torus_base=16)
         res["cpu_reference_ms_per_bootstrap"] = 1e3 * (time.perf_counter() - t0) / cpu_bootstraps
+        rerr = [phase_error(o.phase(rkey2, recompose=True), rlut[m], rin.q_l) for o, m in zip(routs, rmsgs)]
+        res["cpu_reference_phase_error_max"] = float(np.max(rerr))
         res["cpu_reference"] = f"reference's {name} engine, one core, {cpu_bootstraps} bootstraps"
+    return res
+
+
+def ntt_round_trip_leg(eng, reps: int = 20, cpu_budget: float = 3.0) -> dict:
+    """The plain RNS NTT round trip: 64 pairs (a, b) in Z_q[X]/(X^4096 + 1), L = 3 (the
+    three largest 50-bit NTT primes of the reference's generator for the split), uniform
+    residues; forward NTT of both, the incomplete product with the split twist, inverse
+    NTT -- one vfhe_cuda_ntt_mul_intt_batch call per step.  Reported at the reference's
+    default split (4, P = 1024) and at split 1.  Device-resident steps flush L2 first
+    (the working set, 18.9 MB, would otherwise stay in the 126 MB L2); the e2e figure
+    copies the pinned host inputs in and the products out inside every step.  The
+    reference's own library times the same chain (polynomial_RNSc_to_RNS x 2,
+    polynomial_mul_RNS_polynomial, polynomial_RNS_to_RNSc; rns_polynomial.c:311-356,
+    582-614) on one host core."""
+    import torch
+
+    from vfhe_b200.arith import Ring
+    from vfhe_b200.batch import to_device
+    from vfhe_b200.native import Engine
+
+    pairs, N, L = 64, 4096, 3
+    ffi = eng.ffi
+    stream = torch.cuda.current_stream()
+    sp = ffi.cast("void*", stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peak, _ = measured_peaks()
+    alg_bytes = pairs * L * N * 8 * 3
+    res = {"workload": "64 pairs, N=4096, L=3 (50-bit primes), NTT -> product -> INTT per pair",
+           "algorithmic_bytes_per_step": alg_bytes}
+    lib, name = _ref_library()
+    ref = Engine(lib) if lib.exists() else None
+    for split in (None, 1):
+        R = Ring(N, prime_size=[50] * L, split_degree=split, engine=eng)
+        rng = np.random.default_rng(SEED + 21)
+        ha = np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in R.primes]) for _ in range(pairs)])
+        hb = np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in R.primes]) for _ in range(pairs)])
+        a, b = to_device(ha), to_device(hb)
+        out = torch.empty_like(a)
+        limbs = ffi.new("uint32_t[]", R.prime_indices)
+        pa, pb, po = (ffi.cast("uint64_t*", t.data_ptr()) for t in (a, b, out))
+
+        def call():
+            if eng.lib.vfhe_cuda_ntt_mul_intt_batch(R.NTT, po, pa, pb, pairs, limbs, L, sp) != 0:
+                eng.check("ntt_mul_intt_batch")
+
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for e0, e1 in evs:
+            flush.zero_()
+            e0.record(stream)
+            call()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
+        # end to end from pinned host buffers
+        hA = torch.from_numpy(ha.view(np.int64)).pin_memory()
+        hB = torch.from_numpy(hb.view(np.int64)).pin_memory()
+        hO = torch.empty(out.shape, dtype=torch.int64).pin_memory()
+        for e0, e1 in evs:
+            e0.record(stream)
+            a.copy_(hA, non_blocking=True)
+            b.copy_(hB, non_blocking=True)
+            call()
+            hO.copy_(out, non_blocking=True)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
+        key = f"split{R.split_degree}"
+        res[key] = {"pairs_per_s": pairs / (ms * 1e-3), "ms_per_step": ms,
+                    "frac_hbm": alg_bytes / (ms * 1e-3) / 1e9 / peak, "l2": "flushed before every step",
+                    "e2e": {"pairs_per_s": pairs / (e2e_ms * 1e-3), "ms_per_step": e2e_ms,
+                            "h2d_bytes_per_step": int(ha.nbytes + hb.nbytes), "d2h_bytes_per_step": int(ha.nbytes)}}
+        if ref is not None:
+            Rr = Ring(N, prime_size=[50] * L, split_degree=split, engine=ref)
+            assert Rr.primes == R.primes
+            from vfhe_b200.arith import Polynomial
+
+            P = [Polynomial(Rr) for _ in range(5)]
+            P[0].set_rows(ha[0])
+            P[1].set_rows(hb[0])
+            for x in P[:2]:
+                x.rns_mask = Rr.mask
+            rl = ref.lib
+            done, t0 = 0, time.perf_counter()
+            while time.perf_counter() - t0 < cpu_budget:
+                rl.polynomial_RNSc_to_RNS(P[2].obj, P[0].obj)
+                rl.polynomial_RNSc_to_RNS(P[3].obj, P[1].obj)
+                rl.polynomial_mul_RNS_polynomial(P[4].obj, P[2].obj, P[3].obj)
+                rl.polynomial_RNS_to_RNSc(P[4].obj, P[4].obj)
+                done += 1
+            el = time.perf_counter() - t0
+            res[key]["cpu_reference"] = {"pairs_per_s": done / el, "cores": 1, "kind": "reference",
+                                         "sample": f"{done} pairs on the reference's {name} engine, one thread"}
+        del a, b, out
+    del flush
     return res
 
 
@@ -764,10 +939,11 @@ def run_cuda_arm(args) -> None:
     ms16s4, limbs16s4 = ntt16_rate(4, False)
     eng.check("bench")
     encrypt = encrypt_leg(eng, s, key, d1[:, 1].contiguous(), reps=5)
+    round_trip = ntt_round_trip_leg(eng)
 
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
     serving = None if args.no_serving else serving_leg(eng, args.serving_requests)
-    cggi_fft = None if args.no_cggi else cggi_fft_leg(eng, 4096, reps=3, million=args.cggi_million)
+    cggi_fft = None if args.no_cggi else cggi_fft_leg(eng, 4096, reps=3, million=not args.no_cggi_million)
     rns_cggi = None if args.no_cggi else rns_cggi_leg(eng)
 
     if rank != 0:
@@ -805,14 +981,17 @@ def run_cuda_arm(args) -> None:
         "dtype": "u64 (RNS residues < 2^50)",
         "data": "synthetic (seeded keys, noise and unit-disk slots)",
         "config": dict(CONFIG, pairs_per_step=PAIRS),
-        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(h1p.numel() + h2p.numel()),
-                "d2h_bytes_per_step": int(houtp[0].numel()), "ms_per_step": e2e_ms,
-                "transport": "compact wire format (residues at their primes' bit lengths; unpack and pack on "
-                             "the GPU inside the step)", "packed_matches_plain": e2e_packed_ok,
+        "e2e": {"value": e2e_value_plain, "unit": "pairs/s", "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
+                "d2h_bytes_per_step": int(hout[0].numel() * 8), "ms_per_step": e2e_ms_plain,
+                "transport": "uint64 residue rows, the layout the cdef hands callers",
                 "pipelining": "copy-in, compute and copy-out of consecutive steps overlap (two buffer sets)",
-                "plain_uint64": {"value": e2e_value_plain, "ms_per_step": e2e_ms_plain,
-                                 "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
-                                 "d2h_bytes_per_step": int(hout[0].numel() * 8)}},
+                "wire_format": {"value": e2e_value, "ms_per_step": e2e_ms,
+                                "h2d_bytes_per_step": int(h1p.numel() + h2p.numel()),
+                                "d2h_bytes_per_step": int(houtp[0].numel()),
+                                "transport": "compact wire format (residues at their primes' bit lengths) as a "
+                                             "client would send it: packed by the sender before the timed region, "
+                                             "unpacked and packed on the GPU inside the step",
+                                "packed_matches_plain": e2e_packed_ok}},
         "roofline": {"bound": "hbm", "kernel": f"forward FP64 NTT, {kname} (digit transforms, {PAIRS * ne} rows x 2^14)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": MEASURED_TRAFFIC.get((kname, PAIRS * ne)), "launch_ms": ntt_ms,
@@ -832,6 +1011,7 @@ def run_cuda_arm(args) -> None:
     if cggi_fft is not None:
         line["cggi_fft_bootstrap"] = cggi_fft
     line["ckks_encrypt"] = encrypt
+    line["ntt_round_trip_n4096_L3"] = round_trip
     if rns_cggi is not None:
         line["cggi16_rns_bootstrap"] = rns_cggi
     if world == 1 and not args.no_cpu_baseline:
@@ -855,8 +1035,8 @@ def main() -> None:
     ap.add_argument("--worklist-jobs", type=int, default=512, help="jobs in the uneven work-list leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--no-cggi", action="store_true", help="skip the torus CGGI bootstrap leg")
-    ap.add_argument("--cggi-million", action="store_true",
-                    help="also bootstrap 10^6 LWEs and count lookup mismatches (about a minute)")
+    ap.add_argument("--no-cggi-million", action="store_true",
+                    help="skip bootstrapping 10^6 LWEs to count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
     ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
