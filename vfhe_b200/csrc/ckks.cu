@@ -14,7 +14,6 @@
 //     inverse transform at the start of its rescale are both skipped: they are
 //     inverse bijections on canonical residues, so skipping them changes no bit.
 #include <cuda_runtime.h>
-#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -528,37 +527,6 @@ bool check_shape(IncNtt* t, const uint32_t* limbs, uint32_t L, uint32_t special,
     return true;
 }
 
-// The key switch's digit transforms and key multiply-accumulate as one fused cluster
-// kernel (launch_ks_fused) when the ring takes it: split 1, every extended prime below
-// 2^50 (FP64 butterflies), 2^13 or 2^14 points, rows 16-byte aligned.  The accumulator
-// leaves in the coefficient domain.  Returns -1 when the caller must use the unfused
-// path (digits_forward + launch_mac, then the inverse transform of the accumulator).
-int keyswitch_fused(IncNtt* t, uint64_t* acc, const uint64_t* src, long long src_stride,
-                    const uint64_t* const* d_keys, const uint64_t* d_order, const uint32_t* ext, int nd, int ne,
-                    uint64_t B, bool keys_aligned, cudaStream_t st) {
-    static const int disabled = [] {
-        const char* e = getenv("VFHE_CUDA_NO_KS_FUSION");
-        return e && atoi(e) != 0 ? 1 : 0;
-    }();
-    if (disabled || t->pub.split_degree != 1 || !keys_aligned || ne > kMaxLimbs) return -1;
-    if (((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(src)) & 15) != 0) return -1;
-    for (int i = 0; i < ne; ++i)
-        if (!t->info[ext[i]].fp64) return -1;
-    if (prepare_ntt_kernels() != 0) return -1;
-    KsFusedArgs a;
-    memset(&a, 0, sizeof a);
-    a.src = src;
-    a.src_stride = src_stride;
-    a.keys = d_keys;
-    a.order = d_order;
-    a.acc = acc;
-    for (int i = 0; i < ne; ++i) a.prime[i] = ext[i];
-    a.nd = nd;
-    a.ne = ne;
-    a.N = (long long)t->pub.N;
-    return launch_ks_fused(a, t->d_info, t->logP, (long long)B, true, st);
-}
-
 // Forward transforms of every digit: D[b][j][i] = NTT(d_j mod q_i), reading digit
 // rows from src (limb j at src + j N, polynomials src_stride apart).
 int digits_forward(IncNtt* t, uint64_t* D, const uint64_t* src, long long src_stride, uint64_t B,
@@ -870,16 +838,11 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     }
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
-    const bool rlk_aligned = (reinterpret_cast<uintptr_t>(rlk) & 15) == 0;
-    const int fe = keyswitch_fused(t, acc, T, 3LL * nl * N, (const uint64_t* const*)keyptrs, nullptr, ext, nl, ne, B,
-                                   rlk_aligned, st);
-    if (fe > 0) return check_cuda(fe, where) ? 0 : 1;
-    if (fe < 0) {
-        if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-        launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st, rlk_aligned);
-        if (!check_cuda(cudaGetLastError(), where)) return 1;
-        if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
-    }
+    if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st,
+               (reinterpret_cast<uintptr_t>(rlk) & 15) == 0);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
     k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, T, 3LL * nl * N, (long long)nl * N,
                                                             2LL * nl * N, 1, 1, mc, t->d_info, nl, 1, N);
@@ -946,18 +909,13 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
         if (!check_cuda(cudaGetLastError(), where)) return 1;
         src = Pm;
     }
+    if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
     bool keys_aligned = true;
     for (uint64_t b = 0; b < B; ++b) keys_aligned = keys_aligned && (reinterpret_cast<uintptr_t>(gks[b]) & 15) == 0;
-    const int fe = keyswitch_fused(t, acc, src, 2LL * nl * N, (const uint64_t* const*)keyptrs,
-                                   identity ? nullptr : d_order, ext, nl, ne, B, keys_aligned, st);
-    if (fe > 0) return check_cuda(fe, where) ? 0 : 1;
-    if (fe < 0) {
-        if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-        launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st,
-                   keys_aligned);
-        if (!check_cuda(cudaGetLastError(), where)) return 1;
-        if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
-    }
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st,
+               keys_aligned);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
     k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
                                                             mc, t->d_info, nl, 0, N);

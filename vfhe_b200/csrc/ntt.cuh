@@ -89,26 +89,6 @@ int sm_count();
 // Work is enqueued on `stream`; returns a cudaError_t code (0 on success).
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
 
-// Key switch with the digit transforms fused into the key multiply-accumulate, for
-// split-1 rings of 2^13 or 2^14 points whose extended primes are all below 2^50:
-//   acc[b][c][i] = -sum_j NTT(src_b limb j mod q_i) * keys[b][j][c][i]
-// (gadget.c:22-36 over rns_polynomial.c:824-843; NTT domain out).  Returns -1 when
-// the shape is not one this kernel takes (the caller uses the unfused path), else a
-// cudaError_t code.  coeff_out: the accumulator rows leave in the coefficient domain
-// (inverse transforms of both rows run inside the same kernel).
-struct KsFusedArgs {
-    const uint64_t* src;          // limb j of ciphertext b at src + b src_stride + j N (coefficient domain)
-    long long src_stride;
-    const uint64_t* const* keys;  // device array: ciphertext b's key, [digits][2][ne][N]
-    const uint64_t* order;        // device array or null: the ciphertext of cluster row bo
-    uint64_t* acc;                // [B][2][ne][N]
-    uint32_t prime[kMaxLimbs];    // extended primes (pool indices), ne of them
-    int nd, ne;
-    long long N;
-};
-int launch_ks_fused(const KsFusedArgs& a, const PrimeInfo* d_primes, int logP, long long B, bool coeff_out,
-                    cudaStream_t st);
-
 // Count of kernels this engine has launched (vfhe_cuda_launch_count).  Kernels
 // recorded into a CUDA graph are counted at capture; the capturing code takes that
 // count back (forget_launches) and notes it again at every replay.

@@ -79,25 +79,6 @@ __device__ __forceinline__ void load16_u64(double (&x)[16], const uint64_t* p) {
     }
 }
 
-// 16 consecutive read-only residues (key rows): 32-byte loads when aligned.
-__device__ __forceinline__ void load16_raw(uint64_t (&v)[16], const uint64_t* p) {
-    if ((reinterpret_cast<uintptr_t>(p) & 31) == 0) {
-#pragma unroll
-        for (int m = 0; m < 16; m += 4)
-            asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
-                : "=l"(v[m]), "=l"(v[m + 1]), "=l"(v[m + 2]), "=l"(v[m + 3])
-                : "l"(p + m));
-    } else {
-        const ulonglong2* in = reinterpret_cast<const ulonglong2*>(p);
-#pragma unroll
-        for (int m = 0; m < 16; m += 2) {
-            const ulonglong2 w = __ldg(in + m / 2);
-            v[m] = w.x;
-            v[m + 1] = w.y;
-        }
-    }
-}
-
 // Canonical residues of x[0..15] to p[0..15] (same access widths as load16_u64).
 __device__ __forceinline__ void store16_canonical(uint64_t* p, const double (&x)[16], double q, double qinv,
                                                   uint64_t qi) {
@@ -678,51 +659,66 @@ constexpr size_t kTileSmemMax = 200 * 1024;
 // the column kernel + tile kernel pair, and it is one launch.
 namespace cgx = cooperative_groups;
 
-// Column stages of a forward cluster transform: index bits K .. K+K1-1 of the row
-// held across the cluster (natural order, centred doubles in each CTA's fsm); this CTA
-// takes positions [rank TILE/C, (rank + 1) TILE/C) of every block.  Callers sync the
-// cluster before (inputs written) and after (outputs visible).
-template <int K, int K1>
-__device__ __forceinline__ void fused_col_fwd(cgx::cluster_group& cluster, double* fsm, int rank, int t, int logP,
-                                              const FCtx& c) {
+template <int K, int K1, bool TABLE>
+__global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __grid_constant__ RowSet rows,
+                                                                      const PrimeInfo* __restrict__ primes) {
     constexpr int TPT = 1 << (K - 4), TILE = 1 << K, C = 1 << K1;
-    double* blk[C];
+    extern __shared__ __align__(128) double fsm[];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const long long row = blockIdx.x / C;
+    const int t = threadIdx.x;
+    const Tile r = locate<TABLE>(rows, primes, K, row * C + rank, C);
+    const PrimeInfo& pi = *r.pi;
+    FCtx c;
+    c.q = pi.qd;
+    c.qinv = pi.qinv;
+    c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
+    c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
+    c.mt = reinterpret_cast<const double2*>(pi.fwd_mid);
+    c.lazy = fwd_lazy(pi);
+    const int logP = rows.logP;
+    const bool red = rows.reduce_input != 0;
+    // phase 1: this CTA's block, natural order, as residues in doubles
 #pragma unroll
-    for (int m = 0; m < C; ++m) blk[m] = cluster.map_shared_rank(fsm, m);
-    double2 w[K1 * C / 2];  // stage bb's twiddles (at most C/2) do not depend on the position
+    for (int m = 0; m < 16; ++m) fsm[t + TPT * m] = load_in(r.src + t + TPT * m, false, red, c);
+    cluster.sync();
+    // phase 2: column stages on positions [rank TILE/C, (rank + 1) TILE/C)
+    {
+        double* blk[C];
 #pragma unroll
-    for (int bb = K1 - 1; bb >= 0; --bb)
+        for (int m = 0; m < C; ++m) blk[m] = cluster.map_shared_rank(fsm, m);
+        double2 w[K1 * C / 2];  // stage bb's twiddles (at most C/2) do not depend on the position
 #pragma unroll
-        for (int m = 0; m < C; ++m)
-            if (!(m & (1 << bb))) w[(K1 - 1 - bb) * (C / 2) + (m >> (bb + 1))] =
-                __ldg(&c.tw[(1 << (logP - K - 1 - bb)) + (m >> (bb + 1))]);
-    for (int j = rank * (TILE / C) + t; j < (rank + 1) * (TILE / C); j += TPT) {
-        double x[C];
+        for (int bb = K1 - 1; bb >= 0; --bb)
 #pragma unroll
-        for (int m = 0; m < C; ++m) x[m] = blk[m][j];
+            for (int m = 0; m < C; ++m)
+                if (!(m & (1 << bb))) w[(K1 - 1 - bb) * (C / 2) + (m >> (bb + 1))] =
+                    __ldg(&c.tw[(1 << (logP - K - 1 - bb)) + (m >> (bb + 1))]);
+        for (int j = rank * (TILE / C) + t; j < (rank + 1) * (TILE / C); j += TPT) {
+            double x[C];
 #pragma unroll
-        for (int bb = K1 - 1; bb >= 0; --bb) {
+            for (int m = 0; m < C; ++m) x[m] = blk[m][j];
 #pragma unroll
-            for (int m = 0; m < C; ++m) {
-                if (m & (1 << bb)) continue;
-                const double2 ww = w[(K1 - 1 - bb) * (C / 2) + (m >> (bb + 1))];
-                const double v = f_mulmod(x[m | (1 << bb)], ww.x, ww.y, c.q);
-                const double u = x[m];
-                x[m] = __dadd_rn(u, v);
-                x[m | (1 << bb)] = __dsub_rn(u, v);
+            for (int bb = K1 - 1; bb >= 0; --bb) {
+#pragma unroll
+                for (int m = 0; m < C; ++m) {
+                    if (m & (1 << bb)) continue;
+                    const double2 ww = w[(K1 - 1 - bb) * (C / 2) + (m >> (bb + 1))];
+                    const double v = f_mulmod(x[m | (1 << bb)], ww.x, ww.y, c.q);
+                    const double u = x[m];
+                    x[m] = __dadd_rn(u, v);
+                    x[m | (1 << bb)] = __dsub_rn(u, v);
+                }
             }
-        }
 #pragma unroll
-        for (int m = 0; m < C; ++m) blk[m][j] = f_reduce(x[m], c.q, c.qinv);
+            for (int m = 0; m < C; ++m) blk[m][j] = f_reduce(x[m], c.q, c.qinv);
+        }
     }
-}
-
-// Tile passes over the low K bits of block `hi` held in fsm (natural positions after
-// the column stages); leaves the thread's 16 outputs (positions 16 t .. 16 t + 15 of
-// the block, bit-reversed order) in x, below 4q in magnitude, not yet reduced.
-template <int K>
-__device__ __forceinline__ void fused_tiles_fwd(double (&x)[16], double* fsm, int t, int hi, int logP,
-                                                const FCtx& c) {
+    cluster.sync();
+    // phase 3: the tile passes over the low K bits of this block
+    const int hi = rank;
+    double x[16];
     constexpr int L1 = K - 4;
     constexpr int L2 = (K - 8) > 0 ? (K - 8) : 0;
     constexpr int L3 = (K - 12) > 0 ? (K - 12) : 0;
@@ -756,23 +752,13 @@ __device__ __forceinline__ void fused_tiles_fwd(double (&x)[16], double* fsm, in
             f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
         }
     }
-}
-
-__device__ __forceinline__ FCtx fwd_ctx(const PrimeInfo& pi) {
-    FCtx c;
-    c.q = pi.qd;
-    c.qinv = pi.qinv;
-    c.tw = reinterpret_cast<const double2*>(pi.fwd_d);
-    c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
-    c.mt = reinterpret_cast<const double2*>(pi.fwd_mid);
-    c.lazy = fwd_lazy(pi);
-    return c;
+    store16_canonical(r.dst + 16 * t, x, c.q, c.qinv, pi.q);
 }
 
 template <int K, int K1, bool TABLE>
-__global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __grid_constant__ RowSet rows,
+__global__ void __launch_bounds__(TileThreads<K>::value) k_fused_inv_f(const __grid_constant__ RowSet rows,
                                                                       const PrimeInfo* __restrict__ primes) {
-    constexpr int TPT = 1 << (K - 4), C = 1 << K1;
+    constexpr int TPT = 1 << (K - 4), TILE = 1 << K, C = 1 << K1;
     extern __shared__ __align__(128) double fsm[];
     cgx::cluster_group cluster = cgx::this_cluster();
     const int rank = (int)cluster.block_rank();
@@ -780,42 +766,19 @@ __global__ void __launch_bounds__(TileThreads<K>::value) k_fused_fwd_f(const __g
     const int t = threadIdx.x;
     const Tile r = locate<TABLE>(rows, primes, K, row * C + rank, C);
     const PrimeInfo& pi = *r.pi;
-    const FCtx c = fwd_ctx(pi);
-    const int logP = rows.logP;
-    const bool red = rows.reduce_input != 0;
-    // phase 1: this CTA's block, natural order, as residues in doubles
-#pragma unroll
-    for (int m = 0; m < 16; ++m) fsm[t + TPT * m] = load_in(r.src + t + TPT * m, false, red, c);
-    cluster.sync();
-    // phase 2: column stages on positions [rank TILE/C, (rank + 1) TILE/C)
-    fused_col_fwd<K, K1>(cluster, fsm, rank, t, logP, c);
-    cluster.sync();
-    // phase 3: the tile passes over the low K bits of this block
-    double x[16];
-    fused_tiles_fwd<K>(x, fsm, t, rank, logP, c);
-    store16_canonical(r.dst + 16 * t, x, c.q, c.qinv, pi.q);
-}
-
-__device__ __forceinline__ FCtx inv_ctx(const PrimeInfo& pi) {
     FCtx c;
     c.q = pi.qd;
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.inv_d);
     c.lt = reinterpret_cast<const double2*>(pi.inv_lane);
     c.mt = reinterpret_cast<const double2*>(pi.inv_mid);
-    return c;
-}
-
-// Inverse tile passes over the low K bits of block `hi`: x holds the thread's 16
-// inputs (positions 16 t .. 16 t + 15 of the block, bit-reversed order, |x| <= q);
-// on return the block is in fsm in natural order (centred doubles).  Starts with a
-// register pass, so callers sync before it when fsm may still be read.
-template <int K>
-__device__ __forceinline__ void fused_tiles_inv(double (&x)[16], double* fsm, int t, int hi, int logP, const FCtx& c,
-                                                const PrimeInfo& pi) {
+    const int logP = rows.logP, hi = rank;
+    // phase 1: inverse tile passes over the low K bits of this block
+    double x[16];
     constexpr int F1 = 4 < (K - 4) ? 4 : (K - 4);
     constexpr int F2 = 8 < (K - 4) ? 8 : (K - 4);
     constexpr int F3 = 12 < (K - 4) ? 12 : (K - 4);
+    load16_u64(x, r.src + 16 * t);
     PassTw<0, 0, 3> tw1;
     f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c);
     f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
@@ -862,184 +825,49 @@ __device__ __forceinline__ void fused_tiles_inv(double (&x)[16], double* fsm, in
     __syncthreads();  // the exchanges are over: the block goes back in natural order
 #pragma unroll
     for (int m = 0; m < 16; ++m) fsm[own<LAST>(t, m)] = x[m];
-}
-
-// Inverse column stages (index bits K .. K+K1-1, P^-1 folded into the last) over the
-// cluster, on positions [rank TILE/C, (rank + 1) TILE/C) of every block; every CTA's
-// fsm ends up holding its block as canonical uint64 residues.  Callers sync the
-// cluster before and after.
-template <int K, int K1>
-__device__ __forceinline__ void fused_col_inv(cgx::cluster_group& cluster, double* fsm, int rank, int t, int logP,
-                                              const FCtx& c, const PrimeInfo& pi) {
-    constexpr int TPT = 1 << (K - 4), TILE = 1 << K, C = 1 << K1;
-    double* blk[C];
-#pragma unroll
-    for (int m = 0; m < C; ++m) blk[m] = cluster.map_shared_rank(fsm, m);
-    for (int j = rank * (TILE / C) + t; j < (rank + 1) * (TILE / C); j += TPT) {
-        double y[C];
-#pragma unroll
-        for (int m = 0; m < C; ++m) y[m] = blk[m][j];
-#pragma unroll
-        for (int bb = 0; bb < K1; ++bb) {
-            const int base = (1 << logP) >> (bb + K + 1);
-            const bool last = bb == K1 - 1;
-#pragma unroll
-            for (int m = 0; m < C; ++m) {
-                if (m & (1 << bb)) continue;
-                const double u = y[m], v = y[m | (1 << bb)];
-                if (last) {
-                    y[m] = f_mulmod(__dadd_rn(u, v), pi.pinv_d, pi.pinv_q, c.q);
-                    y[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), pi.ilast_d, pi.ilast_q, c.q);
-                } else {
-                    const double2 w = __ldg(&c.tw[base + (m >> (bb + 1))]);
-                    y[m] = __dadd_rn(u, v);
-                    y[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), w.x, w.y, c.q);
-                }
-            }
-            if (!last && (bb & 1)) {
-#pragma unroll
-                for (int m = 0; m < C; ++m)
-                    if (!(m & (1 << bb))) y[m] = f_reduce(y[m], c.q, c.qinv);
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < C; ++m) reinterpret_cast<uint64_t*>(blk[m])[j] = f_to_canonical(y[m], c.q, c.qinv, pi.q);
-    }
-}
-
-template <int K, int K1, bool TABLE>
-__global__ void __launch_bounds__(TileThreads<K>::value) k_fused_inv_f(const __grid_constant__ RowSet rows,
-                                                                      const PrimeInfo* __restrict__ primes) {
-    constexpr int TPT = 1 << (K - 4), C = 1 << K1;
-    extern __shared__ __align__(128) double fsm[];
-    cgx::cluster_group cluster = cgx::this_cluster();
-    const int rank = (int)cluster.block_rank();
-    const long long row = blockIdx.x / C;
-    const int t = threadIdx.x;
-    const Tile r = locate<TABLE>(rows, primes, K, row * C + rank, C);
-    const PrimeInfo& pi = *r.pi;
-    const FCtx c = inv_ctx(pi);
-    const int logP = rows.logP;
-    // phase 1: inverse tile passes over the low K bits of this block
-    double x[16];
-    load16_u64(x, r.src + 16 * t);
-    fused_tiles_inv<K>(x, fsm, t, rank, logP, c, pi);
     cluster.sync();
     // phase 2: inverse column stages (P^-1 folded into the last), canonical results
-    fused_col_inv<K, K1>(cluster, fsm, rank, t, logP, c, pi);
+    {
+        double* blk[C];
+#pragma unroll
+        for (int m = 0; m < C; ++m) blk[m] = cluster.map_shared_rank(fsm, m);
+        for (int j = rank * (TILE / C) + t; j < (rank + 1) * (TILE / C); j += TPT) {
+            double y[C];
+#pragma unroll
+            for (int m = 0; m < C; ++m) y[m] = blk[m][j];
+#pragma unroll
+            for (int bb = 0; bb < K1; ++bb) {
+                const int base = (1 << logP) >> (bb + K + 1);
+                const bool last = bb == K1 - 1;
+#pragma unroll
+                for (int m = 0; m < C; ++m) {
+                    if (m & (1 << bb)) continue;
+                    const double u = y[m], v = y[m | (1 << bb)];
+                    if (last) {
+                        y[m] = f_mulmod(__dadd_rn(u, v), pi.pinv_d, pi.pinv_q, c.q);
+                        y[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), pi.ilast_d, pi.ilast_q, c.q);
+                    } else {
+                        const double2 w = __ldg(&c.tw[base + (m >> (bb + 1))]);
+                        y[m] = __dadd_rn(u, v);
+                        y[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), w.x, w.y, c.q);
+                    }
+                }
+                if (!last && (bb & 1)) {
+#pragma unroll
+                    for (int m = 0; m < C; ++m)
+                        if (!(m & (1 << bb))) y[m] = f_reduce(y[m], c.q, c.qinv);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < C; ++m)
+                reinterpret_cast<uint64_t*>(blk[m])[j] = f_to_canonical(y[m], c.q, c.qinv, pi.q);
+        }
+    }
     cluster.sync();
     // phase 3: this CTA's block to global memory
     const uint64_t* done = reinterpret_cast<const uint64_t*>(fsm);
 #pragma unroll
     for (int m = 0; m < 16; ++m) r.dst[t + TPT * m] = done[t + TPT * m];
-}
-
-// ---- key switch: digit transforms fused with the key multiply-accumulate
-//
-// acc[b][c][i] = -sum_j NTT(d_j mod q_i) (*) K_b[j][c][i] at split 1
-// (gadget_mul_subto_polynomial, gadget.c:22-36, over the digit broadcast of
-// polynomial_RNSc_mod_reduce_lifted, rns_polynomial.c:824-843).  One cluster of C CTAs
-// owns one (ciphertext, extended prime i).  For every digit j it transforms the row
-// d_j mod q_i as k_fused_fwd_f does (the source limb crosses HBM as uint64 residues
-// and is reduced on load; the column stages run over distributed shared memory), and
-// each thread multiplies the 16 residues the last tile pass leaves in its registers by
-// the key residues of both components, adding them into partial sums that stay in
-// shared memory between digits.  The digit spectra never reach global memory; only
-// the two accumulator rows are written, once.
-template <int K, int K1, bool INV>
-__global__ void __launch_bounds__(1 << (K - 4), 2) k_ks_fused(const __grid_constant__ KsFusedArgs a,
-                                                              const PrimeInfo* __restrict__ primes) {
-    constexpr int TPT = 1 << (K - 4), TILE = 1 << K, C = 1 << K1;
-    extern __shared__ __align__(128) double fsm[];
-    double* accs = fsm + TILE + (TILE >> 4);  // partial sums [2][16][TPT]: thread t's slot m at m TPT + t
-    cgx::cluster_group cluster = cgx::this_cluster();
-    const int rank = (int)cluster.block_rank();
-    const long long cl = blockIdx.x / C;
-    const int bo = (int)(cl / a.ne), i = (int)(cl - (long long)bo * a.ne);
-    const long long b = a.order ? (long long)a.order[bo] : (long long)bo;
-    const int t = threadIdx.x;
-    const PrimeInfo& pi = primes[a.prime[i]];
-    const FCtx c = fwd_ctx(pi);
-    const double q = c.q, qinv = c.qinv;
-    constexpr int logP = K + K1;
-    const long long N = a.N;
-    const uint64_t* src = a.src + b * a.src_stride + (long long)rank * TILE;
-    const long long kstride = 2LL * a.ne * N;
-    const uint64_t* ka = a.keys[b] + (long long)i * N + (long long)rank * TILE + 16 * t;
-    const uint64_t* kb = ka + (long long)a.ne * N;
-    uint64_t* oa = a.acc + (b * 2 * a.ne + i) * N + (long long)rank * TILE + (INV ? 0 : 16 * t);
-    uint64_t* ob = oa + (long long)a.ne * N;
-    for (int j = 0; j < a.nd; ++j) {
-        if (j) __syncthreads();  // every thread has read the previous digit's last exchange
-        const uint64_t* sj = src + (long long)j * N;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) fsm[t + TPT * m] = load_in(sj + t + TPT * m, false, true, c);
-        cluster.sync();
-        fused_col_fwd<K, K1>(cluster, fsm, rank, t, logP, c);
-        cluster.sync();
-        double x[16];
-        fused_tiles_fwd<K>(x, fsm, t, rank, logP, c);
-        // x[m] is residue 16 t + m of this block of NTT(d_j mod q_i), |x| < 2^51
-        uint64_t kav[16], kbv[16];
-        load16_raw(kav, ka + (long long)j * kstride);
-        load16_raw(kbv, kb + (long long)j * kstride);
-        const bool last = j + 1 == a.nd;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            // the digit residue in [0, q) multiplies both key residues (one quotient for
-            // two products; operands below 2^50, each term |t| <= 3q/4)
-            double v = f_reduce(x[m], q, qinv);
-            v = v < 0.0 ? __dadd_rn(v, q) : v;
-            const double vq = __dmul_rn(v, qinv);
-            double sa = f_mulmod(f_from_u64(kav[m]), v, vq, q);
-            double sb = f_mulmod(f_from_u64(kbv[m]), v, vq, q);
-            if (j) {
-                sa = __dadd_rn(sa, accs[m * TPT + t]);
-                sb = __dadd_rn(sb, accs[(16 + m) * TPT + t]);
-            }
-            if ((j & 3) == 3) {
-                sa = f_reduce(sa, q, qinv);
-                sb = f_reduce(sb, q, qinv);
-            }
-            if (last) {
-                x[m] = -sa;
-                kav[m] = (uint64_t)__double_as_longlong(-sb);
-            } else {
-                accs[m * TPT + t] = sa;
-                accs[(16 + m) * TPT + t] = sb;
-            }
-        }
-        if (last) {
-            if constexpr (!INV) {
-                store16_canonical(oa, x, q, qinv, pi.q);
-#pragma unroll
-                for (int m = 0; m < 16; ++m) x[m] = __longlong_as_double((long long)kav[m]);
-                store16_canonical(ob, x, q, qinv, pi.q);
-            } else {
-                // both accumulator rows back to the coefficient domain inside the cluster
-                // (the k_fused_inv_f stages), natural order out
-                const FCtx ci = inv_ctx(pi);
-#pragma unroll
-                for (int comp = 0; comp < 2; ++comp) {
-                    if (comp) {
-#pragma unroll
-                        for (int m = 0; m < 16; ++m) x[m] = __longlong_as_double((long long)kav[m]);
-                    }
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) x[m] = f_reduce(x[m], q, qinv);
-                    __syncthreads();  // fsm is free: every thread is past its last read of it
-                    fused_tiles_inv<K>(x, fsm, t, rank, logP, ci, pi);
-                    cluster.sync();
-                    fused_col_inv<K, K1>(cluster, fsm, rank, t, logP, ci, pi);
-                    cluster.sync();
-                    const uint64_t* done = reinterpret_cast<const uint64_t*>(fsm);
-                    uint64_t* o = comp ? ob : oa;
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) o[t + TPT * m] = done[t + TPT * m];
-                }
-            }
-        }
-    }
 }
 
 template <typename KernelT>
@@ -1174,39 +1002,6 @@ int fused_dispatch(int K, int K1, const RowSet& rows, const PrimeInfo* d, bool i
     }
 }
 
-template <int K>
-size_t ks_fused_smem() {
-    return sizeof(double) * (size_t)((1 << K) + (1 << (K - 4)) + 32 * (1 << (K - 4)));
-}
-
-template <int K, int K1, bool INV>
-int ks_fused_launch(const KsFusedArgs& a, const PrimeInfo* d_primes, long long B, cudaStream_t st) {
-    constexpr int TPT = 1 << (K - 4), C = 1 << K1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(B * a.ne * C), 1, 1);
-    cfg.blockDim = dim3(TPT, 1, 1);
-    cfg.dynamicSmemBytes = ks_fused_smem<K>();
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const int e = (int)cudaLaunchKernelEx(&cfg, k_ks_fused<K, K1, INV>, a, d_primes);
-    if (e) return e;
-    note_launch();
-    return (int)cudaGetLastError();
-}
-
-template <int K, int K1>
-int prepare_ks_fused() {
-    int e = set_smem(k_ks_fused<K, K1, false>, ks_fused_smem<K>());
-    if (!e) e = set_smem(k_ks_fused<K, K1, true>, ks_fused_smem<K>());
-    return e;
-}
-
 int tile_dispatch(int K, const RowSet& rows, const PrimeInfo* d, int mode, int tpr, const NttSchedule& sc,
                   cudaStream_t st) {
     switch (K) {
@@ -1284,21 +1079,7 @@ int prepare_ntt_kernels() {
     if (!e) e = prepare_k<11>();
     if (!e) e = prepare_k<12>();
     if (!e) e = prepare_k<13>();
-    if (!e) e = prepare_ks_fused<11, 2>();
-    if (!e) e = prepare_ks_fused<12, 2>();
     return e;
-}
-
-int launch_ks_fused(const KsFusedArgs& a, const PrimeInfo* d_primes, int logP, long long B, bool coeff_out,
-                    cudaStream_t st) {
-    if (B <= 0 || a.ne <= 0 || a.nd <= 0 || a.N != (1LL << logP)) return -1;
-    switch (logP * 2 + (coeff_out ? 1 : 0)) {
-        case 26: return ks_fused_launch<11, 2, false>(a, d_primes, B, st);
-        case 27: return ks_fused_launch<11, 2, true>(a, d_primes, B, st);
-        case 28: return ks_fused_launch<12, 2, false>(a, d_primes, B, st);
-        case 29: return ks_fused_launch<12, 2, true>(a, d_primes, B, st);
-        default: return -1;
-    }
 }
 
 bool set_ntt_schedule(int logP, int rows_log2, const NttSchedule& s) {
