@@ -552,6 +552,26 @@ int64_t vfhe_cuda_server_submit_torus(void *server, int cls, uint32_t *d_out, co
                                       uint64_t count);
 int vfhe_cuda_server_wait(void *server, int64_t id, double *latency_ms);
 int vfhe_cuda_server_stats(void *server, uint64_t *out5);
+/* Failure handling (no counterpart in the reference).
+ * wait_for: wait at most timeout_ms (< 0: no limit); 0 done, 1 failed or unknown id,
+ *   2 time ran out (the request is kept), 3 cancelled.  wait = wait_for without limit.
+ * cancel: drop a request no batch has taken yet; 0 cancelled, 1 already running or
+ *   finished (it completes normally), -1 unknown id.
+ * pause: hold (1) or resume (0) admission of queued requests into batches.
+ * set_batch_timeout: the requests of a batch still running after timeout_ms fail; the
+ *   batch's stream and scratch are released once its device work has finished.
+ * inject_fault (tests; host-side only, no GPU fault): kind 1 the next `count` batch
+ *   launches fail, kind 2 the next `count` scratch allocations fail (the batch is
+ *   re-queued and retried), kind 3 the next `count` batches' completions go unobserved
+ *   until the batch deadline.
+ * fault_stats: out[0] batches failed by the deadline, out[1] allocation retries,
+ *   out[2] cancelled requests, out[3] injected faults not yet consumed. */
+int vfhe_cuda_server_wait_for(void *server, int64_t id, double timeout_ms, double *latency_ms);
+int vfhe_cuda_server_cancel(void *server, int64_t id);
+int vfhe_cuda_server_pause(void *server, int paused);
+int vfhe_cuda_server_set_batch_timeout(void *server, double timeout_ms);
+int vfhe_cuda_server_inject_fault(void *server, int kind, uint32_t count);
+int vfhe_cuda_server_fault_stats(void *server, uint64_t *out4);
 
 #ifdef __cplusplus
 }

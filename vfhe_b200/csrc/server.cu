@@ -105,7 +105,8 @@ struct Request {
     const uint64_t* key;
     uint64_t count;
     Clock::time_point t_submit, t_done;
-    int status = 0;  // 0 queued/running, 1 done, -1 failed
+    int status = 0;  // 0 queued/running, 1 done, -1 failed, -2 cancelled
+    bool started = false;  // taken into a batch (no longer cancellable)
 };
 
 struct Batch {
@@ -115,7 +116,13 @@ struct Batch {
     int stream;
     cudaEvent_t done = nullptr;
     uint64_t bytes = 0;  // budget held until completion
+    Clock::time_point t_start;
+    bool stalled = false;  // injected: completion not observed until the deadline
+    bool expired = false;  // its requests were failed by the batch deadline
 };
+
+// launch() outcome
+enum LaunchResult { kLaunched = 0, kLaunchFailed = 1, kOutOfMemory = 2 };
 
 }  // namespace
 
@@ -140,6 +147,12 @@ struct Server {
     uint64_t batches = 0;
     uint64_t batched_requests = 0;
     bool stop = false;
+    bool paused = false;         // admission held (requests stay queued)
+    double batch_timeout_ms = 0;  // > 0: fail the requests of a batch not done by then
+    // host-side fault injection (tests): the next n batch launches fail, the next n
+    // scratch allocations fail, the next n batches' completions go unobserved
+    int inject_launch = 0, inject_alloc = 0, inject_stall = 0;
+    uint64_t expired_batches = 0, oom_retries = 0, cancelled = 0;
     std::thread worker;
     int device = 0;
     // the server's own stream-ordered pool: batch scratch comes and goes every batch,
@@ -148,7 +161,8 @@ struct Server {
     cudaMemPool_t pool = nullptr;
 
     void run();
-    bool launch(Batch* b);
+    int launch(Batch* b);
+    void fail_request(Request* r, int status);
     uint64_t batch_bytes(int kind, int cls, const std::vector<Request*>& rs) const;
 };
 
@@ -206,11 +220,16 @@ unsigned copy_grid(uint64_t elems) {
 
 }  // namespace
 
-bool Server::launch(Batch* b) {
+int Server::launch(Batch* b) {
     const char* where = "vfhe_cuda_server";
     cudaStream_t st = streams[b->stream];
     const uint64_t B = b->reqs.size();
     int err = 0;
+    if (inject_launch > 0) {  // an injected launch error: nothing is enqueued
+        --inject_launch;
+        set_error(where, "batch launch failed (injected fault)");
+        return kLaunchFailed;
+    }
     if (b->kind == kCggi && cggi[b->cls].torus) {
         CggiClass& g = cggi[b->cls];
         const uint64_t n1 = g.n + 1;
@@ -265,7 +284,15 @@ bool Server::launch(Batch* b) {
         const CkksClass& c = ckks[b->cls];
         const uint64_t cte = ckks_ct_elems(c, c.L), octe = ckks_ct_elems(c, c.L - 1);
         void* mem = nullptr;
+        if (inject_alloc > 0) {  // an injected scratch-allocation failure
+            --inject_alloc;
+            return kOutOfMemory;
+        }
         err = cudaMallocFromPoolAsync(&mem, b->bytes, pool, st);
+        if (err == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return kOutOfMemory;
+        }
         if (!err) {
             // [in1 | in2 or out | out (mul) | workspace | pointer tables (3 B)]
             uint64_t* in1 = (uint64_t*)mem;
@@ -317,9 +344,21 @@ bool Server::launch(Batch* b) {
     if (!err) err = cudaEventRecord(b->done, st);
     if (err) {
         if (err != -1) check_cuda(err, where);
-        return false;
+        return kLaunchFailed;
     }
-    return true;
+    b->t_start = Clock::now();
+    if (inject_stall > 0) {
+        --inject_stall;
+        b->stalled = true;
+    }
+    return kLaunched;
+}
+
+void Server::fail_request(Request* r, int status) {
+    r->status = status;
+    r->t_done = Clock::now();
+    if (status == -2) ++cancelled;
+    else ++failed;
 }
 
 void Server::run() {
@@ -335,17 +374,30 @@ void Server::run() {
         // completions
         for (size_t i = 0; i < inflight.size();) {
             Batch* b = inflight[i];
-            const cudaError_t q = cudaEventQuery(b->done);
+            const Clock::time_point now = Clock::now();
+            // a batch past its deadline: its requests fail now; the batch itself is
+            // released only once its work has really finished on the device
+            if (batch_timeout_ms > 0 && !b->expired &&
+                std::chrono::duration<double, std::milli>(now - b->t_start).count() > batch_timeout_ms) {
+                b->expired = true;
+                ++expired_batches;
+                for (Request* r : b->reqs) fail_request(r, -1);
+                set_error("vfhe_cuda_server", "batch deadline exceeded");
+                progress = true;
+            }
+            cudaError_t q = cudaEventQuery(b->done);
+            if (b->stalled && !b->expired && q != cudaErrorNotReady) q = cudaErrorNotReady;  // injected
             if (q == cudaErrorNotReady) {
                 ++i;
                 continue;
             }
-            const Clock::time_point now = Clock::now();
-            for (Request* r : b->reqs) {
-                r->t_done = now;
-                r->status = q == cudaSuccess ? 1 : -1;
-                if (q == cudaSuccess) ++completed;
-                else ++failed;
+            if (!b->expired) {
+                for (Request* r : b->reqs) {
+                    r->t_done = now;
+                    r->status = q == cudaSuccess ? 1 : -1;
+                    if (q == cudaSuccess) ++completed;
+                    else ++failed;
+                }
             }
             if (q != cudaSuccess) check_cuda(q, "vfhe_cuda_server: batch");
             used -= b->bytes;
@@ -359,7 +411,7 @@ void Server::run() {
         }
         if (progress) cv_done.notify_all();
         // admissions: oldest waiting class first
-        for (;;) {
+        for (; !paused;) {
             int free_stream = -1;
             for (size_t s = 0; s < streams.size(); ++s)
                 if (!stream_busy[s]) {
@@ -408,9 +460,7 @@ void Server::run() {
                     if (inflight.empty()) {  // can never fit: fail the oldest request
                         Request* r = best->front();
                         best->pop_front();
-                        r->status = -1;
-                        r->t_done = Clock::now();
-                        ++failed;
+                        fail_request(r, -1);
                         set_error("vfhe_cuda_server", "request scratch exceeds the HBM budget");
                         cv_done.notify_all();
                     }
@@ -421,12 +471,34 @@ void Server::run() {
                 delete b;
                 break;
             }
-            if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess || !launch(b)) {
-                for (Request* r : b->reqs) {
-                    r->status = -1;
-                    r->t_done = Clock::now();
-                    ++failed;
+            for (Request* r : b->reqs) r->started = true;
+            int lr = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess ? launch(b)
+                                                                                               : kLaunchFailed;
+            if (lr == kOutOfMemory && inflight.empty()) {
+                ++oom_retries;  // nothing in flight will free memory: one more attempt now
+                lr = launch(b);
+            }
+            if (lr == kOutOfMemory) {
+                // scratch did not fit (or an injected allocation failure): back to the
+                // front of the queue, retried when a running batch has freed memory
+                ++oom_retries;
+                for (auto it = b->reqs.rbegin(); it != b->reqs.rend(); ++it) {
+                    (*it)->started = false;
+                    best->push_front(*it);
                 }
+                cudaEventDestroy(b->done);
+                delete b;
+                if (inflight.empty()) {
+                    Request* r = best->front();
+                    best->pop_front();
+                    fail_request(r, -1);
+                    set_error("vfhe_cuda_server", "batch scratch allocation failed");
+                    cv_done.notify_all();
+                }
+                break;
+            }
+            if (lr != kLaunched) {
+                for (Request* r : b->reqs) fail_request(r, -1);
                 if (b->done) cudaEventDestroy(b->done);
                 delete b;
                 cv_done.notify_all();
@@ -503,6 +575,7 @@ void vfhe_cuda_server_free(void* sv) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
+        s->paused = false;  // everything queued still runs
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
@@ -747,22 +820,110 @@ int64_t vfhe_cuda_server_submit_torus(void* sv, int cls, uint32_t* d_out, const 
     return submit(s, r);
 }
 
-// Block until request `id` finished, then forget it (one wait per request); writes its
-// latency (ms).  Returns 0 when it succeeded, 1 when it failed or is unknown.
-int vfhe_cuda_server_wait(void* sv, int64_t id, double* latency_ms) {
+// Wait for request `id` at most timeout_ms (< 0: no limit).  When it has finished,
+// forget it (one successful wait per request) and write its latency (ms).  Returns 0
+// when it succeeded, 1 when it failed or the id is unknown, 2 when the time ran out
+// (the request is kept: wait again or cancel it), 3 when it was cancelled.
+int vfhe_cuda_server_wait_for(void* sv, int64_t id, double timeout_ms, double* latency_ms) {
     Server* s = (Server*)sv;
     if (!s) return 1;
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->requests.find(id);
     if (it == s->requests.end()) return 1;
     vc::Request* r = it->second;
-    s->cv_done.wait(lk, [r] { return r->status != 0; });
+    auto finished = [r] { return r->status != 0; };
+    if (timeout_ms < 0) {
+        s->cv_done.wait(lk, finished);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), finished)) {
+        return 2;
+    }
     if (latency_ms)
         *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
-    const int rc = r->status == 1 ? 0 : 1;
+    const int rc = r->status == 1 ? 0 : (r->status == -2 ? 3 : 1);
     s->requests.erase(it);
     delete r;
     return rc;
+}
+
+// Block until request `id` finished (no time limit); same results as wait_for.
+int vfhe_cuda_server_wait(void* sv, int64_t id, double* latency_ms) {
+    return vfhe_cuda_server_wait_for(sv, id, -1.0, latency_ms);
+}
+
+// Cancel a request that no batch has taken yet.  Returns 0 when it was cancelled (its
+// wait returns 3), 1 when it already runs or finished (it completes normally), -1
+// when the id is unknown.
+int vfhe_cuda_server_cancel(void* sv, int64_t id) {
+    Server* s = (Server*)sv;
+    if (!s) return -1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return -1;
+    vc::Request* r = it->second;
+    if (r->status != 0 || r->started) return 1;
+    auto drop = [r](std::deque<vc::Request*>& q) {
+        auto pos = std::find(q.begin(), q.end(), r);
+        if (pos == q.end()) return false;
+        q.erase(pos);
+        return true;
+    };
+    bool found = drop(s->arrivals);
+    for (auto& kv : s->pending)
+        if (!found) found = drop(kv.second);
+    if (!found) return 1;
+    s->fail_request(r, -2);
+    s->cv_done.notify_all();
+    return 0;
+}
+
+// Hold (paused = 1) or resume (0) the admission of queued requests into batches;
+// running batches finish either way.
+int vfhe_cuda_server_pause(void* sv, int paused) {
+    Server* s = (Server*)sv;
+    if (!s) return 1;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->paused = paused != 0;
+    }
+    s->cv_work.notify_all();
+    return 0;
+}
+
+// Batch deadline (ms; 0 = none): the requests of a batch still running after it fail
+// with "batch deadline exceeded"; the batch's stream and scratch are released when its
+// device work has really finished.
+int vfhe_cuda_server_set_batch_timeout(void* sv, double timeout_ms) {
+    Server* s = (Server*)sv;
+    if (!s || !(timeout_ms >= 0)) return 1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->batch_timeout_ms = timeout_ms;
+    return 0;
+}
+
+// Host-side fault injection, for tests of the failure paths (no GPU fault is made):
+//   kind 1: the next `count` batch launches fail before enqueuing anything;
+//   kind 2: the next `count` batch scratch allocations fail (the batch is re-queued);
+//   kind 3: the next `count` batches' completions go unobserved until the batch
+//           deadline (vfhe_cuda_server_set_batch_timeout) fails their requests.
+int vfhe_cuda_server_inject_fault(void* sv, int kind, uint32_t count) {
+    Server* s = (Server*)sv;
+    if (!s || kind < 1 || kind > 3) return 1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    (kind == 1 ? s->inject_launch : kind == 2 ? s->inject_alloc : s->inject_stall) += (int)count;
+    return 0;
+}
+
+// Failure counters: out[0] batches failed by the deadline, out[1] scratch allocation
+// retries, out[2] cancelled requests, out[3] injected faults not yet consumed.
+int vfhe_cuda_server_fault_stats(void* sv, uint64_t* out4) {
+    Server* s = (Server*)sv;
+    if (!s || !out4) return 1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    out4[0] = s->expired_batches;
+    out4[1] = s->oom_retries;
+    out4[2] = s->cancelled;
+    out4[3] = (uint64_t)(s->inject_launch + s->inject_alloc + s->inject_stall);
+    return 0;
 }
 
 // Counters: out[0] completed, out[1] failed, out[2] batches launched, out[3] requests

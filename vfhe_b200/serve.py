@@ -101,12 +101,54 @@ class Server:
             raise EngineError("server submit rejected (bad class or arguments)")
         return int(rid)
 
-    def wait(self, rid: int) -> float:
+    def wait(self, rid: int, timeout_ms: float | None = None) -> float:
+        """Latency (ms) of request `rid` once it finished.  Raises EngineError when it
+        failed or was cancelled, TimeoutError when `timeout_ms` ran out (the request is
+        kept: wait again or cancel it)."""
         ms = self.ffi.new("double*")
-        if self.lib.vfhe_cuda_server_wait(self.handle, rid, ms) != 0:
+        rc = self.lib.vfhe_cuda_server_wait_for(self.handle, rid, -1.0 if timeout_ms is None else float(timeout_ms), ms)
+        if rc == 2:
+            raise TimeoutError(f"server request {rid} not finished after {timeout_ms} ms")
+        if rc == 3:
+            raise EngineError(f"server request {rid} was cancelled")
+        if rc != 0:
             self.engine.check("server request")
             raise EngineError(f"server request {rid} failed")
         return float(ms[0])
+
+    def poll(self, rid: int, timeout_ms: float = 0.0) -> int:
+        """Raw wait status: 0 done, 1 failed or unknown, 2 not finished yet, 3 cancelled
+        (a finished request is forgotten, as with wait)."""
+        return int(self.lib.vfhe_cuda_server_wait_for(self.handle, rid, float(timeout_ms), self.ffi.NULL))
+
+    def cancel(self, rid: int) -> bool:
+        """Cancel a request no batch has taken yet; False when it already runs or finished."""
+        rc = self.lib.vfhe_cuda_server_cancel(self.handle, rid)
+        if rc < 0:
+            raise EngineError(f"unknown server request {rid}")
+        return rc == 0
+
+    def pause(self, paused: bool = True) -> None:
+        """Hold (or resume) the admission of queued requests into batches."""
+        self.lib.vfhe_cuda_server_pause(self.handle, 1 if paused else 0)
+
+    def set_batch_timeout(self, ms: float) -> None:
+        """Fail the requests of any batch still running `ms` after its launch (0: never)."""
+        if self.lib.vfhe_cuda_server_set_batch_timeout(self.handle, float(ms)) != 0:
+            raise EngineError("bad batch timeout")
+
+    def inject_fault(self, kind: str, count: int = 1) -> None:
+        """Host-side fault injection for tests: 'launch' (the next batch launches fail),
+        'alloc' (the next scratch allocations fail; batches are re-queued) or 'stall'
+        (the next batches' completions go unobserved until the batch deadline)."""
+        k = {"launch": 1, "alloc": 2, "stall": 3}[kind]
+        if self.lib.vfhe_cuda_server_inject_fault(self.handle, k, count) != 0:
+            raise EngineError("fault injection refused")
+
+    def fault_stats(self) -> dict:
+        out = self.ffi.new("uint64_t[4]")
+        self.lib.vfhe_cuda_server_fault_stats(self.handle, out)
+        return {"expired_batches": out[0], "alloc_retries": out[1], "cancelled": out[2], "injected_pending": out[3]}
 
     def stats(self) -> dict:
         out = self.ffi.new("uint64_t[5]")
