@@ -508,6 +508,53 @@ int vfhe_cuda_cggi_fft_keyswitch_batch(uint32_t *d_out, const uint32_t *d_in, ui
 int vfhe_cuda_cggi_fft_external_product(uint32_t *d_out, const uint32_t *d_c, uint64_t batch, const double *d_ggsw_f,
                                         uint32_t N, uint32_t base_log, uint32_t levels, double *d_frac,
                                         void *stream);
+/* Torus keys generated on the GPU from the caller's secret keys d_s [n], d_S [N] (small
+ * signed int32, e.g. binary): d_bsk_rows [n][2 bs_levels][2][N] uint32, row (i, c levels
+ * + l) = GLWE_S(0) with s_i 2^(32 - bs_base_log (l + 1)) added to coefficient 0 of
+ * component c (GGSW(s_i); to_fourier gives the spectra bootstrap_batch reads), and
+ * d_ksk [N][ks_levels][n+1] uint32, row (j, l) = LWE_s(S_j 2^(32 - ks_base_log (l + 1))).
+ * Masks uniform, noise rounded Gaussians of width sigma 2^32 (lwe_sigma for the key
+ * switch, glwe_sigma for the bootstrapping key), drawn from the engine's ChaCha20
+ * stream.  The layout is TorusKeys.generate's in vfhe_b200/cggi_fft.py. */
+int vfhe_cuda_cggi_fft_gen_keys(uint32_t *d_bsk_rows, uint32_t *d_ksk, const int32_t *d_s, const int32_t *d_S,
+                                uint32_t n, uint32_t N, uint32_t bs_base_log, uint32_t bs_levels,
+                                uint32_t ks_base_log, uint32_t ks_levels, double lwe_sigma, double glwe_sigma,
+                                void *stream);
+
+/* Evaluation-key files (no counterpart in the reference, which keeps keys in process
+ * memory only): a versioned 656-byte header (magic "VFHEKEY", format version 1, kind,
+ * element size, shape, the moduli of the limb axis, kind-specific aux words, payload
+ * size, FNV-1a-64 checksum of the payload over 64-bit words) followed by the key tensor
+ * in row-major order.  Host buffers only (no GPU needed); the byte layout is spelled
+ * out in vfhe_b200/csrc/keyfile.cu.  Kinds and shapes:
+ *   VFHE_KEY_KSK        key-switching key (rlk / Galois), u64 [D][2][L+1][N], NTT domain;
+ *                       aux[0] Galois element (0: relinearisation), aux[1] level
+ *   VFHE_KEY_MGSW_BSK   RNS CGGI16 bootstrapping key, u64 [n][2 L0][2][L0+1][N], NTT domain
+ *   VFHE_KEY_TORUS_BSK  torus bootstrapping-key rows, u32 [n][2 levels][2][N];
+ *                       aux[0] base_log, aux[1] levels
+ *   VFHE_KEY_TORUS_KSK  torus key-switching key, u32 [N][levels][n+1]; aux as above
+ * write: 0 on success.  read_header: fills hdr from the file.  read: validates the
+ * header, the payload size and the checksum, fills hdr and host_data (capacity_bytes
+ * at least payload_bytes(hdr)); 1 on any mismatch, with the reason in last_error. */
+enum {
+    VFHE_KEY_KSK = 1,
+    VFHE_KEY_MGSW_BSK = 2,
+    VFHE_KEY_TORUS_BSK = 3,
+    VFHE_KEY_TORUS_KSK = 4
+};
+typedef struct VfheKeyHeader {
+    uint32_t kind;
+    uint32_t elem_bytes;
+    uint32_t ndims;
+    uint32_t nmoduli;
+    uint64_t dims[8];
+    uint64_t aux[4];
+    uint64_t moduli[64];
+} VfheKeyHeader;
+uint64_t vfhe_cuda_keyfile_payload_bytes(const VfheKeyHeader *hdr);
+int vfhe_cuda_keyfile_write(const char *path, const VfheKeyHeader *hdr, const void *host_data);
+int vfhe_cuda_keyfile_read_header(const char *path, VfheKeyHeader *hdr);
+int vfhe_cuda_keyfile_read(const char *path, VfheKeyHeader *hdr, void *host_data, uint64_t capacity_bytes);
 
 /* Serving loop (continuous batching on one GPU).  Requests name device-resident
  * ciphertexts and keys; a native worker thread queues them per (operation, class),

@@ -193,6 +193,62 @@ def gen_galois_key_batch(scheme, key, gen: int, lvl: int = 0, **kw) -> torch.Ten
     return gen_ksk_batch(scheme, key, [p.automorphism(gen) for p in key.poly], lvl, **kw)
 
 
+def gen_bootstrap_key_batch(cggi, input_key, output_key, sigma: float | None = None, engine: Engine | None = None,
+                            stream=None) -> torch.Tensor:
+    """RNS CGGI16 bootstrapping key generated on the GPU: the batched
+    CGGI16.generate_bootstrap_key (cggi16.py:26-44), i.e. MGSW_Scheme.encrypt
+    (mgsw.py:18-55) of every input-key coefficient s_k under the output key, as the
+    device tensor [n][2 ell][2][L0+1][N] (NTT domain) that bootstrap_key_tensor() gives
+    for a key encrypted one row at a time: rows (0, i) encrypt -s_out s_k (P mod q_i) e_i,
+    rows (1, i) encrypt s_k (P mod q_i) e_i.  One vfhe_cuda_gen_ksk_batch call draws all
+    of them (it also draws the special prime's digit of each source, whose gadget factor
+    is P mod P = 0; those rows are dropped)."""
+    from .mlwe import MLWE_Key
+
+    engine = engine or cuda_engine()
+    ffi, lib = engine.ffi, engine.lib
+    ms = cggi.mgsw_scheme
+    scheme = ms.mlwe_scheme
+    if scheme.r != 1:
+        raise EngineError("gen_bootstrap_key_batch: rank-1 schemes only")
+    sring = ms.ring
+    lwe_key = input_key.extract_lwe_key() if isinstance(input_key, MLWE_Key) else input_key
+    s_in = [int(v) for v in lwe_key.get_s()]
+    if any(abs(v) >= 1 << 13 for v in s_in):
+        raise EngineError("gen_bootstrap_key_batch: input key coefficients must be small integers")
+    n, L, N, ell = len(s_in), sring.ell, sring.N, ms.ell
+    P = sring.modulus_ratio(scheme.rings[0])
+    factors = ffi.new("uint64_t[]", [int(P % q) for q in sring.primes])
+    so = Polynomial(sring).from_array(output_key.key[0])
+    so.to_NTT()
+    one = Polynomial(sring).from_array([1] + [0] * (N - 1))
+    one.to_NTT()
+    S, O = so.rows(), one.rows()
+    q = np.array(sring.primes, dtype=np.uint64)[:, None]
+    src = np.empty((n, 2, L, N), dtype=np.uint64)
+    for k, c in enumerate(s_in):
+        mag = np.uint64(abs(c))
+        ms_k = (S * mag) % q          # |c| s_out, below 2^63 before the reduction
+        m_k = (O * mag) % q           # |c| (the NTT of a constant)
+        if c > 0:                     # source 0 is -s_out c, source 1 is c
+            ms_k = (q - ms_k) % q
+        else:
+            m_k = (q - m_k) % q
+        src[k, 0], src[k, 1] = ms_k, m_k
+    d_src = to_device(src.reshape(2 * n, L, N))
+    d_sk = to_device(S)
+    out = torch.empty((2 * n * L, 2, L, N), dtype=torch.int64, device="cuda")
+    limbs = ffi.new("uint32_t[]", list(sring.prime_indices))
+    st = stream or torch.cuda.current_stream()
+    rc = lib.vfhe_cuda_gen_ksk_batch(sring.NTT, _ptr(ffi, out), _ptr(ffi, d_src), 2 * n, limbs, L, factors,
+                                     _ptr(ffi, d_sk), float(output_key.sigma_err if sigma is None else sigma),
+                                     ffi.cast("void*", st.cuda_stream))
+    if rc != 0:
+        engine.check("gen_bootstrap_key_batch")
+        raise EngineError("gen_bootstrap_key_batch")
+    return out.view(n, 2, L, 2, L, N)[:, :, :ell].reshape(n, 2 * ell, 2, L, N).contiguous()
+
+
 class WireFormat:
     """Compact host <-> device format of residue rows (vfhe_cuda_pack_rows): each row
     of N residues of a b-bit prime is a bit stream of N b bits, so a ciphertext at the

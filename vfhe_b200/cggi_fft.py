@@ -129,6 +129,31 @@ def test_vector(lut, params: TorusParams) -> np.ndarray:
     return _u32(lut[np.arange(p.N) // (p.N // p.t)] * p.delta)
 
 
+def generate_device_keys(params: TorusParams, rng: np.random.Generator, engine: Engine | None = None) -> "TorusKeys":
+    """Torus keys whose random material is drawn on the GPU (vfhe_cuda_cggi_fft_gen_keys):
+    the secret keys s and S come from `rng` on the host; the bootstrapping-key rows and
+    the key-switching key are generated in HBM from the engine's ChaCha20 stream and
+    stay there (bsk / ksk of the returned keys are None; bsk_d / ksk_d hold them)."""
+    engine = engine or cuda_engine()
+    ffi, lib = engine.ffi, engine.lib
+    p = params
+    s = rng.integers(0, 2, p.n).astype(np.int32)
+    S = rng.integers(0, 2, p.N).astype(np.int32)
+    bsk_d = torch.empty((p.n, 2 * p.bs_levels, 2, p.N), dtype=torch.int32, device="cuda")
+    ksk_d = torch.empty((p.N, p.ks_levels, p.n + 1), dtype=torch.int32, device="cuda")
+    ds, dS = torch.from_numpy(s).cuda(), torch.from_numpy(S).cuda()
+    rc = lib.vfhe_cuda_cggi_fft_gen_keys(_p32(ffi, bsk_d), _p32(ffi, ksk_d), ffi.cast("int32_t*", ds.data_ptr()),
+                                         ffi.cast("int32_t*", dS.data_ptr()), p.n, p.N, p.bs_base_log, p.bs_levels,
+                                         p.ks_base_log, p.ks_levels, p.lwe_sigma, p.glwe_sigma,
+                                         ffi.cast("void*", torch.cuda.current_stream().cuda_stream))
+    if rc != 0:
+        engine.check("cggi_fft_gen_keys")
+        raise EngineError("cggi_fft_gen_keys")
+    keys = TorusKeys(p, s, S, None, None)
+    keys.bsk_d, keys.ksk_d = bsk_d, ksk_d
+    return keys
+
+
 def _p32(ffi, t: torch.Tensor):
     assert t.is_cuda and t.is_contiguous()
     return ffi.cast("uint32_t*", t.data_ptr())
@@ -142,12 +167,17 @@ class CggiFft:
         self.ffi, self.lib = self.engine.ffi, self.engine.lib
         self.keys = keys
         p = self.params = keys.params
-        rows = torch.from_numpy(keys.bsk.reshape(-1, p.N).view(np.int32)).cuda()
+        bsk_d = getattr(keys, "bsk_d", None)
+        if bsk_d is not None:  # generated on the device
+            rows = bsk_d.reshape(-1, p.N)
+        else:
+            rows = torch.from_numpy(keys.bsk.reshape(-1, p.N).view(np.int32)).cuda()
         self.bsk_f = torch.empty((rows.shape[0], p.N // 2, 2), dtype=torch.float64, device="cuda")
         self._check(self.lib.vfhe_cuda_cggi_fft_to_fourier(self.ffi.cast("double*", self.bsk_f.data_ptr()),
                                                            _p32(self.ffi, rows), rows.shape[0], p.N, self._st()),
                     "cggi_fft_to_fourier")
-        self.ksk = torch.from_numpy(np.ascontiguousarray(keys.ksk).view(np.int32)).cuda()
+        ksk_d = getattr(keys, "ksk_d", None)
+        self.ksk = ksk_d if ksk_d is not None else torch.from_numpy(np.ascontiguousarray(keys.ksk).view(np.int32)).cuda()
         torch.cuda.synchronize()
 
     def _st(self, stream=None):

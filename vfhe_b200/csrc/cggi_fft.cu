@@ -669,6 +669,91 @@ int launch_to_fourier(int N, double2* outp, const uint32_t* rows, long long coun
 
 using namespace vc;
 
+namespace vc {
+namespace {
+
+// ---- torus key generation on the device (the big random material of the keys; the
+// secret keys s and S are the caller's)
+//
+// Bootstrapping key: row (i, r), r = c levels + l, is a GLWE encryption of zero under
+// S, (a, a S + e), with s_i 2^(32 - base_log (l + 1)) added to coefficient 0 of
+// component c -- GGSW(s_i) in the layout vfhe_cuda_cggi_fft_bootstrap_batch reads.
+// Key-switching key: row (j, l) is an LWE encryption under s of S_j 2^(32 - ks_base_log
+// (l + 1)).  a is uniform over the torus, e a rounded Gaussian of width sigma 2^32.
+// Randomness: the engine's ChaCha20 stream, uniform and Gaussian nonces, blocks counted
+// from u0 / g0 per row.
+
+__device__ __forceinline__ int32_t torus_gauss(const PrngKey& key, uint64_t counter, int k, double sigma32) {
+    uint32_t blk[16];
+    chacha20_block(key, counter, kStreamGaussian, blk);
+    const double u1 = unit_open_low(block_u64(blk, 2 * (k & 3))), u2 = unit_closed_low(block_u64(blk, 2 * (k & 3) + 1));
+    return (int32_t)(int64_t)llrint(sigma32 * sqrt(-2.0 * log(u1)) * cospi(2.0 * u2));
+}
+
+// one CTA of N threads per bootstrapping-key row; thread k computes coefficient k
+__global__ void k_torus_bsk_rows(uint32_t* __restrict__ rows, const int32_t* __restrict__ s,
+                                 const int32_t* __restrict__ S, int N, int levels, int base_log, double sigma32,
+                                 const __grid_constant__ PrngKey key, uint64_t u0, uint64_t g0) {
+    extern __shared__ uint32_t tsm[];  // a [N], S [N]
+    uint32_t* a = tsm;
+    uint32_t* Ssh = tsm + N;
+    const long long row = blockIdx.x;  // i * 2 levels + r
+    const int i = (int)(row / (2 * levels)), r = (int)(row - (long long)i * 2 * levels);
+    const int k = threadIdx.x;
+    const uint64_t per_row = (uint64_t)(N / 16);
+    if ((k & 15) == 0) {
+        uint32_t blk[16];
+        chacha20_block(key, u0 + (uint64_t)row * per_row + (uint64_t)(k >> 4), kStreamUniform, blk);
+#pragma unroll
+        for (int w = 0; w < 16; ++w) a[k + w] = blk[w];
+    }
+    Ssh[k] = (uint32_t)S[k];
+    __syncthreads();
+    // (a S)_k = sum_j a_j S_(k-j) with the sign of the wrap (X^N = -1)
+    uint32_t acc = 0;  // products mod 2^32: a small signed key entry multiplies as its residue
+    for (int j = 0; j <= k; ++j) acc += a[j] * Ssh[k - j];
+    for (int j = k + 1; j < N; ++j) acc -= a[j] * Ssh[k - j + N];
+    const int32_t e = torus_gauss(key, g0 + (uint64_t)row * (uint64_t)(N / 4) + (uint64_t)(k >> 2), k, sigma32);
+    uint32_t b = acc + (uint32_t)e;
+    uint32_t av = a[k];
+    const int c = r / levels, l = r - c * levels;
+    if (k == 0) {
+        const uint32_t m = (uint32_t)s[i] << (32 - base_log * (l + 1));
+        if (c == 0) av += m;
+        else b += m;
+    }
+    uint32_t* out = rows + (size_t)row * 2 * N;
+    out[k] = av;
+    out[N + k] = b;
+}
+
+// one thread per key-switching-key row (j, l): mask, then body
+__global__ void k_torus_ksk_rows(uint32_t* __restrict__ ksk, const int32_t* __restrict__ s,
+                                 const int32_t* __restrict__ S, int n, int N, int levels, int base_log, double sigma32,
+                                 const __grid_constant__ PrngKey key, uint64_t u0, uint64_t g0) {
+    const long long rows = (long long)N * levels;
+    for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < rows;
+         row += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(row / levels), l = (int)(row - (long long)j * levels);
+        uint32_t* out = ksk + (size_t)row * (n + 1);
+        const uint64_t per_row = (uint64_t)((n + 15) / 16);
+        uint32_t dot = 0;
+        for (int c = 0; c < n; c += 16) {
+            uint32_t blk[16];
+            chacha20_block(key, u0 + (uint64_t)row * per_row + (uint64_t)(c >> 4), kStreamUniform, blk);
+            for (int w = 0; w < 16 && c + w < n; ++w) {
+                out[c + w] = blk[w];
+                dot += blk[w] * (uint32_t)s[c + w];
+            }
+        }
+        const int32_t e = torus_gauss(key, g0 + (uint64_t)row, 0, sigma32);
+        out[n] = dot + (uint32_t)e + ((uint32_t)S[j] << (32 - base_log * (l + 1)));
+    }
+}
+
+}  // namespace
+}  // namespace vc
+
 extern "C" {
 
 int vfhe_cuda_cggi_fft_to_fourier(double* d_out, const uint32_t* d_rows, uint64_t count, uint32_t N, void* stream) {
@@ -733,6 +818,37 @@ int vfhe_cuda_cggi_fft_external_product(uint32_t* d_out, const uint32_t* d_c, ui
     const int e = dispatch_nl<ExtprodF>((int)N, (int)levels, d_out, d_c, (long long)batch, (const double2*)d_ggsw_f,
                                         (int)base_log, ft, d_frac, (cudaStream_t)stream);
     return check_cuda(e, where) ? 0 : 1;
+}
+
+// Torus CGGI keys generated on the device from the caller's secret keys (binary or
+// small signed int32): d_bsk_rows [n][2 bs_levels][2][N] uint32 (then to_fourier for the
+// spectra the bootstrap reads) and d_ksk [N][ks_levels][n+1] uint32.
+int vfhe_cuda_cggi_fft_gen_keys(uint32_t* d_bsk_rows, uint32_t* d_ksk, const int32_t* d_s, const int32_t* d_S,
+                                uint32_t n, uint32_t N, uint32_t bs_base_log, uint32_t bs_levels, uint32_t ks_base_log,
+                                uint32_t ks_levels, double lwe_sigma, double glwe_sigma, void* stream) {
+    if (!ensure_ready()) return 1;
+    const char* where = "vfhe_cuda_cggi_fft_gen_keys";
+    if (!d_bsk_rows || !d_ksk || !d_s || !d_S || n == 0 || n > (1u << 16) || (N != 512 && N != 1024 && N != 2048) ||
+        bs_levels == 0 || bs_levels * bs_base_log > 32 || ks_levels == 0 || ks_levels * ks_base_log > 32 ||
+        !(lwe_sigma >= 0.0) || !(glwe_sigma >= 0.0)) {
+        set_error(where, "bad buffers, n, N (512/1024/2048), gadget shapes or noise widths");
+        return 1;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t bsk_rows = (uint64_t)n * 2 * bs_levels;
+    const uint64_t ksk_rows = (uint64_t)N * ks_levels;
+    const uint64_t u0 = prng_advance(bsk_rows * (N / 16) + ksk_rows * ((n + 15) / 16));
+    const uint64_t g0 = prng_advance(bsk_rows * (N / 4) + ksk_rows);
+    const PrngKey key = prng_key();
+    k_torus_bsk_rows<<<(unsigned)bsk_rows, N, 2 * N * sizeof(uint32_t), st>>>(
+        d_bsk_rows, d_s, d_S, (int)N, (int)bs_levels, (int)bs_base_log, glwe_sigma * 4294967296.0, key, u0, g0);
+    note_launch();
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    k_torus_ksk_rows<<<(unsigned)((ksk_rows + 255) / 256), 256, 0, st>>>(
+        d_ksk, d_s, d_S, (int)n, (int)N, (int)ks_levels, (int)ks_base_log, lwe_sigma * 4294967296.0, key,
+        u0 + bsk_rows * (N / 16), g0 + bsk_rows * (N / 4));
+    note_launch();
+    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
 
 }  // extern "C"
