@@ -253,27 +253,40 @@ def whole_job_rate(units_per_rank: int, world: int, ms: float) -> float:
 # ----------------------------------------------------------------------------- gpu arm
 def worklist_leg(eng, count: int, reps: int) -> dict:
     """Uneven batch: `count` jobs, N in 2^12..2^16, L in 2..24, half NTT->product->INTT
-    chains and half key switches, as one work-list graph launch vs one call per job."""
+    chains and half key switches, as one persistent work-list launch per run, beside
+    the graph of per-pool launches and one call per job."""
     import torch
 
     from vfhe_b200.worklist import WorkList, per_call_workspace, run_per_call, uneven_jobs
 
     jobs = uneven_jobs(eng, count=count, seed=SEED + 3)
-    wl = WorkList(eng)
-    for j in jobs:
-        wl.add(j)
     stream = torch.cuda.current_stream()
-    wl.run(stream)  # compile + capture + first replay
-    torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    profile_range(None, "worklist", True)
-    ev0.record(stream)
-    for _ in range(reps):
-        wl.run(stream)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    profile_range(None, "worklist", False)
-    ms_wl = ev0.elapsed_time(ev1) / reps
+
+    def timed(mode, profile):
+        w = WorkList(eng, mode=mode)
+        for j in jobs:
+            w.add(j)
+        w.run(stream)  # compile (+ capture) + first run
+        torch.cuda.synchronize()
+        if profile:
+            profile_range(None, "worklist", True)
+        ev0.record(stream)
+        for _ in range(reps):
+            w.run(stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if profile:
+            profile_range(None, "worklist", False)
+        return w, ev0.elapsed_time(ev1) / reps
+
+    wg, ms_graph = timed(1, False)
+    graph_launches = wg.launches
+    graph_out = [j.out.clone() for j in jobs]
+    wg.close()
+    wl, ms_wl = timed(0, True)
+    persistent_exact = all(torch.equal(j.out, g) for j, g in zip(jobs, graph_out))
+    del graph_out
     outs = [torch.empty_like(j.out) for j in jobs]
     ws = per_call_workspace(eng, jobs)
     calls = run_per_call(eng, jobs, outs, ws, stream)
@@ -290,7 +303,10 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
         "jobs": count, "jobs_per_s": count / (ms_wl * 1e-3), "ms_per_run": ms_wl,
         "per_call_jobs_per_s": count / (ms_pc * 1e-3), "per_call_ms": ms_pc, "per_call_calls": calls,
         "speedup_vs_per_call": ms_pc / ms_wl, "bit_exact_vs_per_call": bool(exact),
-        "graph_kernels_per_run": wl.launches, "device_bytes": wl.device_bytes,
+        "kernels_per_run": wl.launches, "persistent": wl.persistent,
+        "graph_of_pool_launches": {"jobs_per_s": count / (ms_graph * 1e-3), "ms_per_run": ms_graph,
+                                   "kernels_per_run": graph_launches, "bit_exact_vs_persistent": bool(persistent_exact)},
+        "device_bytes": wl.device_bytes,
         "algorithmic_gb_per_s": moved / (ms_wl * 1e-3) / 1e9,
         "mix": {"chain": sum(j.kind == "chain" for j in jobs), "keyswitch": sum(j.kind == "keyswitch" for j in jobs)},
     }

@@ -457,9 +457,14 @@ int vfhe_cuda_clear_device_faults(void);
  * CUDA error.  Clear the flag afterwards with vfhe_cuda_clear_device_faults. */
 int vfhe_cuda_selfcheck_bounded_wait(int32_t tries);
 
-/* Work list: independent jobs of any mix of ring degree and limb count, run as ONE
- * CUDA-graph launch (grouped per transform pool; each stage of a group is one launch
- * over a device-resident row table).  Jobs:
+/* Work list: independent jobs of any mix of ring degree and limb count, run together.
+ * Mode 0 (default): when every job has 2^8 <= N/split <= 2^16, a run is ONE
+ * persistent cooperative kernel whose CTAs walk six phases (forward column passes,
+ * forward tile passes, products and key multiply-accumulates, inverse tile passes,
+ * inverse column passes, special-prime divisions) over the device-resident row tables
+ * of every transform pool, with a bounded grid barrier between phases (a barrier that
+ * gives up raises the flag vfhe_cuda_device_faults reads).  Mode 1, and mode 0 for
+ * other sizes: a CUDA graph with one launch per stage per transform pool.  Jobs:
  *   chain      d_out = INTT(NTT(d_a) * NTT(d_b)), [nlimbs][N] each (as
  *              vfhe_cuda_ntt_mul_intt_batch with batch 1);
  *   keyswitch  as vfhe_cuda_keyswitch_batch with batch 1 (d_ct [2][nlimbs][N],
@@ -479,6 +484,8 @@ int vfhe_cuda_worklist_compile(void *wl);
 int vfhe_cuda_worklist_run(void *wl, void *stream);
 uint64_t vfhe_cuda_worklist_device_bytes(void *wl);
 int vfhe_cuda_worklist_launches(void *wl);
+int vfhe_cuda_worklist_set_mode(void *wl, int mode);
+int vfhe_cuda_worklist_is_persistent(void *wl);
 
 /* CGGI over the 32-bit torus with FP64 FFT external products (the TFHE bootstrap,
  * Chillotti et al., J. Cryptology 33, 2020, with the reference's CGGI16 blind-rotation

@@ -11,8 +11,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("count,logn,limbs,seed", [(24, (10, 13), (2, 6), 5), (6, (14, 16), (2, 3), 6)])
-def test_worklist_matches_per_call_and_oracle(cuda, oracle_engine, count, logn, limbs, seed):
+@pytest.mark.parametrize("mode", [0, 1], ids=["persistent", "graph"])
+@pytest.mark.parametrize("count,logn,limbs,seed", [(24, (10, 13), (2, 6), 5), (6, (14, 16), (2, 3), 6),
+                                                   (40, (10, 16), (2, 5), 9)])
+def test_worklist_matches_per_call_and_oracle(cuda, oracle_engine, count, logn, limbs, seed, mode):
     import torch
 
     from tests.helpers import job_on_engine
@@ -20,16 +22,20 @@ def test_worklist_matches_per_call_and_oracle(cuda, oracle_engine, count, logn, 
 
     jobs = uneven_jobs(cuda, count=count, seed=seed, logn=logn, limbs=limbs)
     assert {j.kind for j in jobs} == {"chain", "keyswitch"}
-    wl = WorkList(cuda)
+    wl = WorkList(cuda, mode=mode)
     for j in jobs:
         wl.add(j)
     wl.run()
     torch.cuda.synchronize()
     first = [j.out.clone() for j in jobs]
-    wl.run()  # replay of the captured graph
+    wl.run()  # a second run (the persistent kernel's barriers start from zero again)
     torch.cuda.synchronize()
     assert all(torch.equal(f, j.out) for f, j in zip(first, jobs))
-    assert wl.launches > 0
+    if mode == 0:
+        assert wl.persistent and wl.launches == 1
+    else:
+        assert not wl.persistent and wl.launches > 1
+    assert cuda.lib.vfhe_cuda_device_faults() == 0
 
     outs = [torch.empty_like(j.out) for j in jobs]
     run_per_call(cuda, jobs, outs, per_call_workspace(cuda, jobs))

@@ -248,13 +248,16 @@ int vfhe_cuda_device_faults(void) {
     if (!check_cuda(read_tile_fault(&f), "vfhe_cuda_device_faults")) return -1;
     int m = 0;
     if (!check_cuda(read_mac_fault(&m), "vfhe_cuda_device_faults")) return -1;
-    return f | m;
+    int w = 0;
+    if (!check_cuda(read_wl_fault(&w), "vfhe_cuda_device_faults")) return -1;
+    return f | m | w;
 }
 
 int vfhe_cuda_clear_device_faults(void) {
     if (!vc::ensure_ready()) return 1;
     if (!check_cuda(clear_tile_fault(), "vfhe_cuda_clear_device_faults")) return 1;
     if (!check_cuda(clear_mac_fault(), "vfhe_cuda_clear_device_faults")) return 1;
+    if (!check_cuda(clear_wl_fault(), "vfhe_cuda_clear_device_faults")) return 1;
     return 0;
 }
 

@@ -114,6 +114,10 @@ int prepare_ckks_kernels();
 int read_mac_fault(int* out);
 int clear_mac_fault();
 
+// The flag the persistent work-list kernel raises when a grid-barrier wait gave up.
+int read_wl_fault(int* out);
+int clear_wl_fault();
+
 // Launch a one-thread kernel whose bounded mbarrier wait can never be satisfied (a
 // transaction count no copy delivers) with a limit of `tries` attempts; on return
 // *gave_up is 1 when the wait gave up and raised the staged-MAC fault flag.

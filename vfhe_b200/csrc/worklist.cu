@@ -14,11 +14,16 @@
 // Compilation groups the jobs by transform pool (same N, split and prime tables) and
 // writes, per group, device-resident row tables: one descriptor per P-point row to
 // transform, per limb row to multiply, per (job, limb) to multiply-accumulate and per
-// (job, component) to divide.  Each stage of a group is ONE launch over its table,
-// whatever the mix of L and job kinds (the transform kernels read their row, prime
-// and twiddles from the descriptor); groups are independent branches of the graph,
-// so small-N groups run beside large ones.  Transform launch shapes come from the
-// tuned schedule of (log2 P, rows) (vfhe_cuda_ntt_set_schedule).
+// (job, component) to divide.
+//
+// A run is ONE persistent kernel (when every row has 2^8 <= P <= 2^16): a cooperative
+// launch whose CTAs walk six phases over the tables of every group -- forward column
+// passes, forward tile passes, products and key multiply-accumulates, inverse tile
+// passes, inverse column passes, special-prime divisions -- with a bounded grid
+// barrier between phases, so jobs of every N and L share one launch and small jobs
+// fill the gaps of large ones.  The fallback (and mode 1) is a CUDA graph of one launch
+// per stage per group, groups as independent branches, transform shapes from the tuned
+// schedule of (log2 P, rows) (vfhe_cuda_ntt_set_schedule).
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -29,6 +34,7 @@
 #include "abi_common.cuh"
 #include "fp64mod.cuh"
 #include "keyswitch.cuh"
+#include "ntt_f64_dev.cuh"
 
 namespace vc {
 
@@ -65,17 +71,12 @@ struct DownDesc {
 
 constexpr int kWlThreads = 256;
 
+// Product of slot x (all S blocks) of one limb row.
 template <int S>
-__global__ void __launch_bounds__(kWlThreads) k_wl_product(const ProdDesc* __restrict__ tab, long long chunks,
-                                                           int logP) {
-    const long long e = blockIdx.x / chunks;
-    const long long chunk = blockIdx.x - e * chunks;
-    const ProdDesc d = tab[e];
+__device__ __forceinline__ void wl_product_one(const ProdDesc& d, long long x, int logP) {
     const PrimeInfo& pi = *d.pi;
     const uint64_t q = pi.q;
     const long long P = 1LL << logP;
-    const long long x = chunk * kWlThreads + threadIdx.x;
-    if (x >= P) return;
     uint64_t av[S], bv[S], res[S];
 #pragma unroll
     for (int j = 0; j < S; ++j) {
@@ -104,35 +105,47 @@ __global__ void __launch_bounds__(kWlThreads) k_wl_product(const ProdDesc* __res
     for (int o = 0; o < S; ++o) d.out[o * P + x] = res[o];
 }
 
-// -sum_j D_j (*) K_j for one (job, extended limb).  S <= 4: one thread per slot x
-// computes all S blocks (mac_slots); larger S: one thread per (block, slot).
 template <int S>
-__global__ void __launch_bounds__(kWlThreads) k_wl_mac(const MacDesc* __restrict__ tab, long long chunks,
-                                                       long long N) {
+__global__ void __launch_bounds__(kWlThreads) k_wl_product(const ProdDesc* __restrict__ tab, long long chunks,
+                                                           int logP) {
     const long long e = blockIdx.x / chunks;
     const long long chunk = blockIdx.x - e * chunks;
-    const MacDesc d = tab[e];
-    const long long idx = chunk * kWlThreads + threadIdx.x;
+    const long long x = chunk * kWlThreads + threadIdx.x;
+    if (x >= (1LL << logP)) return;
+    wl_product_one<S>(tab[e], x, logP);
+}
+
+// -sum_j D_j (*) K_j for one (job, extended limb).  S <= 4: one thread per slot x
+// computes all S blocks (mac_slots); larger S: one thread per (block, slot).  idx below
+// wl_mac_work(S, N).
+__host__ __device__ __forceinline__ long long wl_mac_work(int S, long long N) { return (S == 2 || S == 4) ? N / S : N; }
+
+template <int S>
+__device__ __forceinline__ void wl_mac_one(const MacDesc& d, long long idx, long long N) {
     const long long P = N / S;
     const long long dstr = (long long)d.ne * N;
     if (S == 2 || S == 4) {
-        if (idx >= P) return;
         mac_slots<(S == 2 ? 2 : 4)>(d.oa, d.oa + dstr, d.d, dstr, d.k, d.k + dstr, 2 * dstr, d.nd, P, idx, *d.pi);
         return;
     }
-    if (idx >= N) return;
     const int o = (int)(idx / P);
     const long long x = idx - o * P;
     mac_slot(d.oa, d.oa + dstr, d.d, dstr, d.k, d.k + dstr, 2 * dstr, d.nd, S, P, x, o, *d.pi);
 }
 
-__global__ void __launch_bounds__(kWlThreads) k_wl_moddown(const DownDesc* __restrict__ tab, long long chunks,
-                                                           long long N, const PrimeInfo* __restrict__ primes) {
+template <int S>
+__global__ void __launch_bounds__(kWlThreads) k_wl_mac(const MacDesc* __restrict__ tab, long long chunks,
+                                                       long long N) {
     const long long e = blockIdx.x / chunks;
     const long long chunk = blockIdx.x - e * chunks;
-    const DownDesc d = tab[e];
-    const long long x = chunk * kWlThreads + threadIdx.x;
-    if (x >= N) return;
+    const long long idx = chunk * kWlThreads + threadIdx.x;
+    if (idx >= wl_mac_work(S, N)) return;
+    wl_mac_one<S>(tab[e], idx, N);
+}
+
+// Special-prime division of coefficient x of one (job, component).
+__device__ __forceinline__ void wl_down_one(const DownDesc& d, long long x, long long N,
+                                            const PrimeInfo* __restrict__ primes) {
     const ModDownConsts& mc = *d.mc;
     if (mc.fp64) {
         // exact FP64 form of the loop below (every intermediate an integer below 2^52)
@@ -158,6 +171,199 @@ __global__ void __launch_bounds__(kWlThreads) k_wl_moddown(const DownDesc* __res
         d.out[(long long)i * N + x] = v;
     }
 }
+
+__global__ void __launch_bounds__(kWlThreads) k_wl_moddown(const DownDesc* __restrict__ tab, long long chunks,
+                                                           long long N, const PrimeInfo* __restrict__ primes) {
+    const long long e = blockIdx.x / chunks;
+    const long long chunk = blockIdx.x - e * chunks;
+    const long long x = chunk * kWlThreads + threadIdx.x;
+    if (x >= N) return;
+    wl_down_one(tab[e], x, N, primes);
+}
+
+// ---- the persistent work-list kernel
+
+// One group's tables as the persistent kernel reads them (device memory).
+struct WlGroupPlan {
+    RowSet fwd_first;   // column pass (K < logP) or the only tile pass (K == logP)
+    RowSet fwd_second;  // tile pass after the column pass
+    RowSet inv_first;   // inverse tile pass
+    RowSet inv_second;  // inverse column pass (K < logP)
+    const ProdDesc* prod;
+    const MacDesc* mac;
+    const DownDesc* down;
+    const PrimeInfo* info;
+    long long nprod, nmac, ndown;
+    long long N;
+    int logP, K, S, logS;
+};
+
+struct WlPlan {
+    const WlGroupPlan* groups;
+    int ngroups;
+    unsigned* barrier;  // [0] arrivals, [1] generation
+};
+
+constexpr int kWlPThreads = 256;
+constexpr long long kWlBarrierSpins = 1LL << 25;  // ~2 s of 64 ns sleeps
+
+__device__ int vc_wl_fault;  // nonzero: a work-list grid barrier gave up waiting
+
+// Grid-wide barrier of a cooperative launch (every CTA is resident, so every CTA
+// arrives).  The wait is bounded: if it runs out, the fault flag is raised and the CTA
+// carries on (results are then wrong; vfhe_cuda_device_faults reports it).
+__device__ __forceinline__ void wl_grid_barrier(unsigned* bar) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g) {
+                if (++spins > kWlBarrierSpins) {
+                    atomicExch(&vc_wl_fault, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// All tiles of one group's tile pass, TPC = 256 / 2^(K-4) tiles per CTA step.  Threads
+// whose tile would lie past the end recompute the last tile without storing, so every
+// thread reaches every barrier.
+template <int K, bool INV, bool TWO>
+__device__ __forceinline__ void wl_tiles(const RowSet& rows, double* fsm) {
+    constexpr int TPT = 1 << (K - 4), TPC = kWlPThreads / TPT, PADDED = (1 << K) + (1 << (K - 4));
+    const int tiles_per_row = 1 << (rows.logP - K);
+    const long long ntiles = rows.table_rows * tiles_per_row;
+    const long long ngroups = (ntiles + TPC - 1) / TPC;
+    const int lt = threadIdx.x / TPT, t = threadIdx.x - lt * TPT;
+    double* sm = fsm + lt * PADDED;
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        const long long tile = grp * TPC + lt;
+        const bool valid = tile < ntiles;
+        const Tile r = locate<true>(rows, nullptr, K, valid ? tile : ntiles - 1, tiles_per_row);
+        if constexpr (INV) tile_inv_one<K, !TWO, false>(r, rows, sm, t, valid);
+        else tile_fwd_one<K, TWO, false>(r, rows, sm, t, valid);
+        __syncthreads();  // the next step reuses the exchange buffers
+    }
+}
+
+template <bool INV, bool TWO>
+__device__ __forceinline__ void wl_tiles_k(int K, const RowSet& rows, double* fsm) {
+    switch (K) {
+        case 8: wl_tiles<8, INV, TWO>(rows, fsm); break;
+        case 9: wl_tiles<9, INV, TWO>(rows, fsm); break;
+        case 10: wl_tiles<10, INV, TWO>(rows, fsm); break;
+        case 11: wl_tiles<11, INV, TWO>(rows, fsm); break;
+        default: wl_tiles<12, INV, TWO>(rows, fsm); break;
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void wl_cols(int K1, const RowSet& rows, int KT) {
+    const long long ncols = rows.table_rows << KT;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long gc = (long long)blockIdx.x * blockDim.x + threadIdx.x; gc < ncols; gc += stride) {
+        switch (K1) {
+            case 1: col_one<1, INV>(rows, nullptr, gc, KT); break;
+            case 2: col_one<2, INV>(rows, nullptr, gc, KT); break;
+            case 3: col_one<3, INV>(rows, nullptr, gc, KT); break;
+            default: col_one<4, INV>(rows, nullptr, gc, KT); break;
+        }
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void wl_products_s(const WlGroupPlan& G) {
+    const int logP = G.logP;
+    const long long total = G.nprod << logP;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+        wl_product_one<S>(G.prod[i >> logP], i & ((1LL << logP) - 1), logP);
+}
+
+template <int S>
+__device__ __forceinline__ void wl_macs_s(const WlGroupPlan& G) {
+    const long long work = wl_mac_work(S, G.N);
+    const int lw = 63 - __clzll(work);
+    const long long total = G.nmac << lw;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+        wl_mac_one<S>(G.mac[i >> lw], i & (work - 1), G.N);
+}
+
+__global__ void __launch_bounds__(kWlPThreads, 2) k_wl_persistent(const __grid_constant__ WlPlan plan) {
+    extern __shared__ __align__(128) double fsm[];
+    // 1: forward column passes
+    for (int g = 0; g < plan.ngroups; ++g) {
+        const WlGroupPlan& G = plan.groups[g];
+        if (G.K < G.logP && G.fwd_first.table_rows) wl_cols<false>(G.logP - G.K, G.fwd_first, G.K);
+    }
+    wl_grid_barrier(plan.barrier);
+    // 2: forward tile passes (after a column pass they read its centred doubles)
+    for (int g = 0; g < plan.ngroups; ++g) {
+        const WlGroupPlan& G = plan.groups[g];
+        if (!G.fwd_first.table_rows) continue;
+        if (G.K < G.logP) wl_tiles_k<false, true>(G.K, G.fwd_second, fsm);
+        else wl_tiles_k<false, false>(G.K, G.fwd_first, fsm);
+    }
+    wl_grid_barrier(plan.barrier);
+    // 3: products of the chains and multiply-accumulates of the key switches
+    for (int g = 0; g < plan.ngroups; ++g) {
+        const WlGroupPlan& G = plan.groups[g];
+        if (G.nprod) {
+            switch (G.S) {
+                case 1: wl_products_s<1>(G); break;
+                case 2: wl_products_s<2>(G); break;
+                default: wl_products_s<4>(G); break;
+            }
+        }
+        if (G.nmac) {
+            switch (G.S) {
+                case 1: wl_macs_s<1>(G); break;
+                case 2: wl_macs_s<2>(G); break;
+                default: wl_macs_s<4>(G); break;
+            }
+        }
+    }
+    wl_grid_barrier(plan.barrier);
+    // 4: inverse tile passes (before a column pass they leave centred doubles)
+    for (int g = 0; g < plan.ngroups; ++g) {
+        const WlGroupPlan& G = plan.groups[g];
+        if (!G.inv_first.table_rows) continue;
+        if (G.K < G.logP) wl_tiles_k<true, true>(G.K, G.inv_first, fsm);
+        else wl_tiles_k<true, false>(G.K, G.inv_first, fsm);
+    }
+    wl_grid_barrier(plan.barrier);
+    // 5: inverse column passes
+    for (int g = 0; g < plan.ngroups; ++g) {
+        const WlGroupPlan& G = plan.groups[g];
+        if (G.K < G.logP && G.inv_second.table_rows) wl_cols<true>(G.logP - G.K, G.inv_second, G.K);
+    }
+    wl_grid_barrier(plan.barrier);
+    // 6: special-prime divisions
+    for (int g = 0; g < plan.ngroups; ++g) {
+        const WlGroupPlan& G = plan.groups[g];
+        if (!G.ndown) continue;
+        const int ln = 63 - __clzll(G.N);
+        const long long total = G.ndown << ln;
+        const long long stride = (long long)gridDim.x * blockDim.x;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+            wl_down_one(G.down[i >> ln], i & (G.N - 1), G.N, G.info);
+    }
+}
+
+constexpr size_t kWlPSmem = sizeof(double) * kWlPThreads * 17;  // TPC tiles of 17 TPT doubles, any K
 
 struct Job {
     int kind;  // 0 chain, 1 keyswitch
@@ -196,10 +402,17 @@ struct WorkList {
     size_t dev_bytes = 0;
     cudaGraphExec_t exec = nullptr;
     int launches_per_run = 0;
+    int mode = 0;  // 0: one persistent launch when the jobs allow it; 1: graph of per-group launches
+    // persistent path
+    bool persistent = false;
+    WlPlan plan = {};
+    int grid = 0;
 
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
+        persistent = false;
+        plan = WlPlan{};
         if (dev) cudaFree(dev);
         dev = nullptr;
         dev_bytes = 0;
@@ -272,7 +485,13 @@ int compile(WorkList& w) {
         tab_bytes += align256(nf * sizeof(RowDesc)) + align256(ni * sizeof(RowDesc)) +
                      align256(np * sizeof(ProdDesc)) + align256(nm * sizeof(MacDesc)) + align256(nd * sizeof(DownDesc));
     }
-    w.dev_bytes = ws_bytes + mc_bytes + tab_bytes;
+    // persistent path: every row between 2^8 and 2^16 points (tile passes of at most
+    // 2^12 points after a column pass of radix at most 16), split degree at most 4
+    bool persist = w.mode == 0;
+    for (const Group& G : w.groups)
+        persist = persist && G.t->logP >= 8 && G.t->logP <= 16 && G.t->pub.split_degree <= 4;
+    const size_t plan_bytes = persist ? align256(w.groups.size() * sizeof(WlGroupPlan)) + 256 : 0;
+    w.dev_bytes = ws_bytes + mc_bytes + tab_bytes + plan_bytes;
     if (!check_cuda(cudaMalloc(&w.dev, w.dev_bytes), kWhere)) {
         w.dev = nullptr;
         return 1;
@@ -350,6 +569,60 @@ int compile(WorkList& w) {
             (!G.down.empty() && !check_cuda(cudaMemcpy(G.d_down, G.down.data(), G.down.size() * sizeof(DownDesc),
                                                        cudaMemcpyHostToDevice), kWhere)))
             return 1;
+    }
+
+    if (persist) {
+        // the group plans and the barrier words sit at the end of the buffer
+        WlGroupPlan* d_plans = (WlGroupPlan*)((char*)w.dev + ws_bytes + mc_bytes + tab_bytes);
+        unsigned* d_bar = (unsigned*)((char*)d_plans + plan_bytes - 256);
+        std::vector<WlGroupPlan> plans(w.groups.size());
+        for (size_t g = 0; g < w.groups.size(); ++g) {
+            const Group& Gr = w.groups[g];
+            IncNtt* t = Gr.t;
+            WlGroupPlan& P = plans[g];
+            memset(&P, 0, sizeof P);
+            P.logP = t->logP;
+            P.K = t->logP <= 12 ? t->logP : 12;
+            P.S = (int)t->pub.split_degree;
+            P.logS = 0;
+            while ((1 << P.logS) < P.S) ++P.logS;
+            P.N = (long long)t->pub.N;
+            P.info = t->d_info;
+            auto table_set = [&](RowSet& rs, const RowDesc* tab, size_t n, int reduce, int src_is_dst) {
+                memset(&rs, 0, sizeof rs);
+                rs.logP = t->logP;
+                rs.split = P.S;
+                rs.fp64 = 1;
+                rs.reduce_input = reduce;
+                rs.table = tab;
+                rs.table_rows = (long long)n;
+                rs.table_src_is_dst = src_is_dst;
+            };
+            table_set(P.fwd_first, Gr.d_fwd, Gr.fwd.size(), 1, 0);
+            table_set(P.fwd_second, Gr.d_fwd, Gr.fwd.size(), 0, 1);
+            table_set(P.inv_first, Gr.d_inv, Gr.inv.size(), 0, 0);
+            table_set(P.inv_second, Gr.d_inv, Gr.inv.size(), 0, 1);
+            P.prod = Gr.d_prod;
+            P.nprod = (long long)Gr.prod.size();
+            P.mac = Gr.d_mac;
+            P.nmac = (long long)Gr.mac.size();
+            P.down = Gr.d_down;
+            P.ndown = (long long)Gr.down.size();
+        }
+        int nb = 0;
+        int err = (int)cudaMemcpy(d_plans, plans.data(), plans.size() * sizeof(WlGroupPlan), cudaMemcpyHostToDevice);
+        if (!err) err = (int)cudaMemset(d_bar, 0, 256);
+        if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_wl_persistent, kWlPThreads, kWlPSmem);
+        if (!err && nb >= 1) {
+            w.plan.groups = d_plans;
+            w.plan.ngroups = (int)plans.size();
+            w.plan.barrier = d_bar;
+            w.grid = nb * sm_count();
+            w.persistent = true;
+            w.launches_per_run = 1;
+            return 0;
+        }
+        cudaGetLastError();  // the per-group graph below serves instead
     }
 
     // capture: one branch per group, forked from and joined into one capture stream
@@ -454,6 +727,15 @@ int compile(WorkList& w) {
 
 }  // namespace
 
+int read_wl_fault(int* out) {
+    return (int)cudaMemcpyFromSymbol(out, vc_wl_fault, sizeof(int));
+}
+
+int clear_wl_fault() {
+    const int zero = 0;
+    return (int)cudaMemcpyToSymbol(vc_wl_fault, &zero, sizeof(int));
+}
+
 }  // namespace vc
 
 using vc::WorkList;
@@ -539,10 +821,46 @@ int vfhe_cuda_worklist_run(void* wl, void* stream_) {
         vc::set_error("vfhe_cuda_worklist_run", "empty work list");
         return 1;
     }
-    if (!w->exec && vc::compile(*w)) return 1;
-    if (!vc::check_cuda(cudaGraphLaunch(w->exec, (cudaStream_t)stream_), "vfhe_cuda_worklist_run")) return 1;
+    if (!w->exec && !w->persistent && vc::compile(*w)) return 1;
+    cudaStream_t st = (cudaStream_t)stream_;
+    if (w->persistent) {
+        // a cooperative launch: every CTA is resident, so the grid barriers between the
+        // phases cannot wait on a CTA that has not started
+        if (!vc::check_cuda(cudaMemsetAsync(w->plan.barrier, 0, 2 * sizeof(unsigned), st), "vfhe_cuda_worklist_run"))
+            return 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)w->grid, 1, 1);
+        cfg.blockDim = dim3(vc::kWlPThreads, 1, 1);
+        cfg.dynamicSmemBytes = vc::kWlPSmem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (!vc::check_cuda(cudaLaunchKernelEx(&cfg, vc::k_wl_persistent, w->plan), "vfhe_cuda_worklist_run")) return 1;
+        vc::note_launch(1);
+        return 0;
+    }
+    if (!vc::check_cuda(cudaGraphLaunch(w->exec, st), "vfhe_cuda_worklist_run")) return 1;
     vc::note_launch(w->launches_per_run);
     return 0;
+}
+
+int vfhe_cuda_worklist_set_mode(void* wl, int mode) {
+    WorkList* w = (WorkList*)wl;
+    if (!w || mode < 0 || mode > 1) {
+        vc::set_error("vfhe_cuda_worklist_set_mode", "mode is 0 (one persistent launch) or 1 (graph of launches)");
+        return 1;
+    }
+    if (mode != w->mode) w->release();
+    w->mode = mode;
+    return 0;
+}
+
+int vfhe_cuda_worklist_is_persistent(void* wl) {
+    WorkList* w = (WorkList*)wl;
+    return w && w->persistent ? 1 : 0;
 }
 
 uint64_t vfhe_cuda_worklist_device_bytes(void* wl) {

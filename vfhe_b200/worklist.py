@@ -1,8 +1,11 @@
 """Uneven batched work list over the C ABI (vfhe_cuda_worklist_*).
 
 Jobs of any mix of ring degree N and limb count L -- NTT -> product -> INTT chains and
-GHS key switches -- are compiled once into device-resident row tables and one CUDA
-graph, then replayed with one launch per run.  ``run_per_call`` executes the same jobs
+GHS key switches -- are compiled once into device-resident row tables and run as ONE
+persistent cooperative kernel per run (mode 0; six phases over every group's tables
+with grid barriers between them), or as a CUDA graph of one launch per stage per
+transform pool (mode 1, and the fallback for rows outside 2^8..2^16 points or split
+degrees above 4).  ``run_per_call`` executes the same jobs
 one entry-point call each (vfhe_cuda_ntt_mul_intt_batch / vfhe_cuda_keyswitch_batch
 with batch 1): the plain path the work list is measured against, and its parity
 reference on the GPU.
@@ -53,13 +56,14 @@ class Job:
 
 
 class WorkList:
-    """Compiled-once, replayed-many batch of independent jobs (one graph launch per run)."""
+    """Compiled-once, replayed-many batch of independent jobs (one launch per run)."""
 
-    def __init__(self, engine: Engine | None = None):
+    def __init__(self, engine: Engine | None = None, mode: int = 0):
         self.engine = engine or cuda_engine()
         self.ffi, self.lib = self.engine.ffi, self.engine.lib
         self.handle = self.lib.vfhe_cuda_worklist_new()
         self.jobs: list[Job] = []
+        self._check(self.lib.vfhe_cuda_worklist_set_mode(self.handle, mode), "worklist_set_mode")
 
     def _check(self, rc: int, what: str) -> None:
         if rc != 0:
@@ -89,7 +93,12 @@ class WorkList:
 
     @property
     def launches(self) -> int:
+        """Kernels one run launches (1 on the persistent path)."""
         return int(self.lib.vfhe_cuda_worklist_launches(self.handle))
+
+    @property
+    def persistent(self) -> bool:
+        return bool(self.lib.vfhe_cuda_worklist_is_persistent(self.handle))
 
     @property
     def device_bytes(self) -> int:
