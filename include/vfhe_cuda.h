@@ -486,6 +486,10 @@ uint64_t vfhe_cuda_worklist_device_bytes(void *wl);
 int vfhe_cuda_worklist_launches(void *wl);
 int vfhe_cuda_worklist_set_mode(void *wl, int mode);
 int vfhe_cuda_worklist_is_persistent(void *wl);
+/* Persistent path: wall time (ms, device global timer, seen by CTA 0 at each grid
+ * barrier) of the last run's six phases -- forward column, forward tile, products and
+ * MACs, inverse tile, inverse column, divisions.  1 when not on the persistent path. */
+int vfhe_cuda_worklist_phase_ms(void *wl, double *out6);
 
 /* CGGI over the 32-bit torus with FP64 FFT external products (the TFHE bootstrap,
  * Chillotti et al., J. Cryptology 33, 2020, with the reference's CGGI16 blind-rotation

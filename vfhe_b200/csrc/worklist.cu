@@ -201,8 +201,17 @@ struct WlGroupPlan {
 struct WlPlan {
     const WlGroupPlan* groups;
     int ngroups;
-    unsigned* barrier;  // [0] arrivals, [1] generation
+    unsigned* barrier;              // [0] arrivals, [1] generation
+    unsigned long long* phase_ns;   // [7]: start and the end of every phase (global timer), CTA 0
 };
+
+__device__ __forceinline__ void wl_stamp(const WlPlan& plan, int k) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        plan.phase_ns[k] = t;
+    }
+}
 
 constexpr int kWlPThreads = 256;
 constexpr long long kWlBarrierSpins = 1LL << 25;  // ~2 s of 64 ns sleeps
@@ -302,14 +311,17 @@ __device__ __forceinline__ void wl_macs_s(const WlGroupPlan& G) {
         wl_mac_one<S>(G.mac[i >> lw], i & (work - 1), G.N);
 }
 
-__global__ void __launch_bounds__(kWlPThreads, 2) k_wl_persistent(const __grid_constant__ WlPlan plan) {
+template <int MINB>
+__global__ void __launch_bounds__(kWlPThreads, MINB) k_wl_persistent(const __grid_constant__ WlPlan plan) {
     extern __shared__ __align__(128) double fsm[];
+    wl_stamp(plan, 0);
     // 1: forward column passes
     for (int g = 0; g < plan.ngroups; ++g) {
         const WlGroupPlan& G = plan.groups[g];
         if (G.K < G.logP && G.fwd_first.table_rows) wl_cols<false>(G.logP - G.K, G.fwd_first, G.K);
     }
     wl_grid_barrier(plan.barrier);
+    wl_stamp(plan, 1);
     // 2: forward tile passes (after a column pass they read its centred doubles)
     for (int g = 0; g < plan.ngroups; ++g) {
         const WlGroupPlan& G = plan.groups[g];
@@ -318,6 +330,7 @@ __global__ void __launch_bounds__(kWlPThreads, 2) k_wl_persistent(const __grid_c
         else wl_tiles_k<false, false>(G.K, G.fwd_first, fsm);
     }
     wl_grid_barrier(plan.barrier);
+    wl_stamp(plan, 2);
     // 3: products of the chains and multiply-accumulates of the key switches
     for (int g = 0; g < plan.ngroups; ++g) {
         const WlGroupPlan& G = plan.groups[g];
@@ -337,6 +350,7 @@ __global__ void __launch_bounds__(kWlPThreads, 2) k_wl_persistent(const __grid_c
         }
     }
     wl_grid_barrier(plan.barrier);
+    wl_stamp(plan, 3);
     // 4: inverse tile passes (before a column pass they leave centred doubles)
     for (int g = 0; g < plan.ngroups; ++g) {
         const WlGroupPlan& G = plan.groups[g];
@@ -345,12 +359,14 @@ __global__ void __launch_bounds__(kWlPThreads, 2) k_wl_persistent(const __grid_c
         else wl_tiles_k<true, false>(G.K, G.inv_first, fsm);
     }
     wl_grid_barrier(plan.barrier);
+    wl_stamp(plan, 4);
     // 5: inverse column passes
     for (int g = 0; g < plan.ngroups; ++g) {
         const WlGroupPlan& G = plan.groups[g];
         if (G.K < G.logP && G.inv_second.table_rows) wl_cols<true>(G.logP - G.K, G.inv_second, G.K);
     }
     wl_grid_barrier(plan.barrier);
+    wl_stamp(plan, 5);
     // 6: special-prime divisions
     for (int g = 0; g < plan.ngroups; ++g) {
         const WlGroupPlan& G = plan.groups[g];
@@ -361,6 +377,8 @@ __global__ void __launch_bounds__(kWlPThreads, 2) k_wl_persistent(const __grid_c
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
             wl_down_one(G.down[i >> ln], i & (G.N - 1), G.N, G.info);
     }
+    wl_grid_barrier(plan.barrier);
+    wl_stamp(plan, 6);
 }
 
 constexpr size_t kWlPSmem = sizeof(double) * kWlPThreads * 17;  // TPC tiles of 17 TPT doubles, any K
@@ -487,7 +505,7 @@ int compile(WorkList& w) {
     }
     // persistent path: every row between 2^8 and 2^16 points (tile passes of at most
     // 2^12 points after a column pass of radix at most 16), split degree at most 4
-    bool persist = w.mode == 0;
+    bool persist = w.mode == 0 || w.mode == 2;
     for (const Group& G : w.groups)
         persist = persist && G.t->logP >= 8 && G.t->logP <= 16 && G.t->pub.split_degree <= 4;
     const size_t plan_bytes = persist ? align256(w.groups.size() * sizeof(WlGroupPlan)) + 256 : 0;
@@ -582,7 +600,14 @@ int compile(WorkList& w) {
             WlGroupPlan& P = plans[g];
             memset(&P, 0, sizeof P);
             P.logP = t->logP;
-            P.K = t->logP <= 12 ? t->logP : 12;
+            // tile bits: the tuned schedule's for this (P, rows) class when it fits the
+            // persistent kernel (tiles of 2^8..2^12 after a column pass of radix <= 16)
+            const NttSchedule sc = get_ntt_schedule(t->logP, (long long)std::max(Gr.fwd.size(), Gr.inv.size()));
+            int K = t->logP <= 12 ? t->logP : 12;
+            if (sc.tile_bits >= 8 && sc.tile_bits <= 12 && sc.tile_bits <= t->logP && t->logP - sc.tile_bits <= 4 &&
+                sc.ctas_per_sm != -1)
+                K = sc.tile_bits;
+            P.K = K;
             P.S = (int)t->pub.split_degree;
             P.logS = 0;
             while ((1 << P.logS) < P.S) ++P.logS;
@@ -612,11 +637,14 @@ int compile(WorkList& w) {
         int nb = 0;
         int err = (int)cudaMemcpy(d_plans, plans.data(), plans.size() * sizeof(WlGroupPlan), cudaMemcpyHostToDevice);
         if (!err) err = (int)cudaMemset(d_bar, 0, 256);
-        if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_wl_persistent, kWlPThreads, kWlPSmem);
+        if (!err)
+            err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &nb, w.mode == 2 ? k_wl_persistent<3> : k_wl_persistent<2>, kWlPThreads, kWlPSmem);
         if (!err && nb >= 1) {
             w.plan.groups = d_plans;
             w.plan.ngroups = (int)plans.size();
             w.plan.barrier = d_bar;
+            w.plan.phase_ns = (unsigned long long*)((char*)d_bar + 64);
             w.grid = nb * sm_count();
             w.persistent = true;
             w.launches_per_run = 1;
@@ -838,7 +866,9 @@ int vfhe_cuda_worklist_run(void* wl, void* stream_) {
         attr[0].val.cooperative = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        if (!vc::check_cuda(cudaLaunchKernelEx(&cfg, vc::k_wl_persistent, w->plan), "vfhe_cuda_worklist_run")) return 1;
+        const cudaError_t le = w->mode == 2 ? cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<3>, w->plan)
+                                            : cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<2>, w->plan);
+        if (!vc::check_cuda(le, "vfhe_cuda_worklist_run")) return 1;
         vc::note_launch(1);
         return 0;
     }
@@ -849,12 +879,23 @@ int vfhe_cuda_worklist_run(void* wl, void* stream_) {
 
 int vfhe_cuda_worklist_set_mode(void* wl, int mode) {
     WorkList* w = (WorkList*)wl;
-    if (!w || mode < 0 || mode > 1) {
-        vc::set_error("vfhe_cuda_worklist_set_mode", "mode is 0 (one persistent launch) or 1 (graph of launches)");
+    if (!w || mode < 0 || mode > 2) {
+        vc::set_error("vfhe_cuda_worklist_set_mode",
+                      "mode is 0 (one persistent launch), 1 (graph of launches) or 2 (persistent, 3 CTAs per SM)");
         return 1;
     }
     if (mode != w->mode) w->release();
     w->mode = mode;
+    return 0;
+}
+
+int vfhe_cuda_worklist_phase_ms(void* wl, double* out6) {
+    WorkList* w = (WorkList*)wl;
+    if (!w || !out6 || !w->persistent) return 1;
+    unsigned long long t[7];
+    if (!vc::check_cuda(cudaMemcpy(t, w->plan.phase_ns, sizeof t, cudaMemcpyDeviceToHost), "vfhe_cuda_worklist_phase_ms"))
+        return 1;
+    for (int k = 0; k < 6; ++k) out6[k] = (double)(t[k + 1] - t[k]) * 1e-6;
     return 0;
 }
 
