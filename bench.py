@@ -284,8 +284,6 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
     graph_launches = wg.launches
     graph_out = [j.out.clone() for j in jobs]
     wg.close()
-    w3, ms_p3 = timed(2, False)
-    w3.close()
     wl, ms_wl = timed(0, True)
     persistent_exact = all(torch.equal(j.out, g) for j, g in zip(jobs, graph_out))
     del graph_out
@@ -308,7 +306,6 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
         "kernels_per_run": wl.launches, "persistent": wl.persistent,
         "graph_of_pool_launches": {"jobs_per_s": count / (ms_graph * 1e-3), "ms_per_run": ms_graph,
                                    "kernels_per_run": graph_launches, "bit_exact_vs_persistent": bool(persistent_exact)},
-        "persistent_3_ctas_per_sm": {"jobs_per_s": count / (ms_p3 * 1e-3), "ms_per_run": ms_p3},
         "device_bytes": wl.device_bytes,
         "algorithmic_gb_per_s": moved / (ms_wl * 1e-3) / 1e9,
         "mix": {"chain": sum(j.kind == "chain" for j in jobs), "keyswitch": sum(j.kind == "keyswitch" for j in jobs)},

@@ -458,13 +458,14 @@ int vfhe_cuda_clear_device_faults(void);
 int vfhe_cuda_selfcheck_bounded_wait(int32_t tries);
 
 /* Work list: independent jobs of any mix of ring degree and limb count, run together.
- * Mode 0 (default): when every job has 2^8 <= N/split <= 2^16, a run is ONE
- * persistent cooperative kernel whose CTAs walk six phases (forward column passes,
- * forward tile passes, products and key multiply-accumulates, inverse tile passes,
- * inverse column passes, special-prime divisions) over the device-resident row tables
- * of every transform pool, with a bounded grid barrier between phases (a barrier that
- * gives up raises the flag vfhe_cuda_device_faults reads).  Mode 1, and mode 0 for
- * other sizes: a CUDA graph with one launch per stage per transform pool.  Jobs:
+ * Mode 0 (default): when every job has 2^8 <= N/split <= 2^16 and split <= 4, a run is
+ * three persistent cooperative kernels whose CTAs walk six phases (forward column
+ * passes | forward tile passes; products and key multiply-accumulates; inverse tile
+ * passes | inverse column passes | special-prime divisions) over the device-resident
+ * row tables of every transform pool, with a bounded grid barrier between the phases of
+ * a kernel (a barrier that gives up raises the flag vfhe_cuda_device_faults reads).
+ * Mode 1, and mode 0 for other shapes: a CUDA graph with one launch per stage per
+ * transform pool.  Jobs:
  *   chain      d_out = INTT(NTT(d_a) * NTT(d_b)), [nlimbs][N] each (as
  *              vfhe_cuda_ntt_mul_intt_batch with batch 1);
  *   keyswitch  as vfhe_cuda_keyswitch_batch with batch 1 (d_ct [2][nlimbs][N],
@@ -486,9 +487,10 @@ uint64_t vfhe_cuda_worklist_device_bytes(void *wl);
 int vfhe_cuda_worklist_launches(void *wl);
 int vfhe_cuda_worklist_set_mode(void *wl, int mode);
 int vfhe_cuda_worklist_is_persistent(void *wl);
-/* Persistent path: wall time (ms, device global timer, seen by CTA 0 at each grid
- * barrier) of the last run's six phases -- forward column, forward tile, products and
- * MACs, inverse tile, inverse column, divisions.  1 when not on the persistent path. */
+/* Persistent path: wall time (ms, device global timer, seen by CTA 0 at the grid
+ * barriers) of the last run's six phases -- forward column, forward tile, products and
+ * MACs (with the launch gap before it), inverse tile (with its launch gap), inverse
+ * column, divisions.  1 when not on the persistent path. */
 int vfhe_cuda_worklist_phase_ms(void *wl, double *out6);
 
 /* CGGI over the 32-bit torus with FP64 FFT external products (the TFHE bootstrap,

@@ -32,7 +32,7 @@ def test_worklist_matches_per_call_and_oracle(cuda, oracle_engine, count, logn, 
     torch.cuda.synchronize()
     assert all(torch.equal(f, j.out) for f, j in zip(first, jobs))
     if mode == 0:
-        assert wl.persistent and wl.launches == 1
+        assert wl.persistent and wl.launches == 3
     else:
         assert not wl.persistent and wl.launches > 1
     assert cuda.lib.vfhe_cuda_device_faults() == 0

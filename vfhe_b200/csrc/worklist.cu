@@ -16,12 +16,14 @@
 // transform, per limb row to multiply, per (job, limb) to multiply-accumulate and per
 // (job, component) to divide.
 //
-// A run is ONE persistent kernel (when every row has 2^8 <= P <= 2^16): a cooperative
-// launch whose CTAs walk six phases over the tables of every group -- forward column
-// passes, forward tile passes, products and key multiply-accumulates, inverse tile
-// passes, inverse column passes, special-prime divisions -- with a bounded grid
-// barrier between phases, so jobs of every N and L share one launch and small jobs
-// fill the gaps of large ones.  The fallback (and mode 1) is a CUDA graph of one launch
+// A run is three persistent cooperative kernels (when every row has 2^8 <= P <= 2^16
+// and the split degree is at most 4) whose CTAs walk six phases over the tables of
+// every group -- forward column passes and forward tile passes; products and key
+// multiply-accumulates; inverse tile passes, inverse column passes and special-prime
+// divisions -- with a bounded grid barrier between the phases inside a kernel, so jobs
+// of every N and L share each launch and small jobs fill the gaps of large ones.  Three
+// kernels instead of one let each keep the register budget (and so the occupancy) its
+// phases need.  The fallback (and mode 1) is a CUDA graph of one launch
 // per stage per group, groups as independent branches, transform shapes from the tuned
 // schedule of (log2 P, rows) (vfhe_cuda_ntt_set_schedule).
 #include <cuda_runtime.h>
@@ -311,74 +313,84 @@ __device__ __forceinline__ void wl_macs_s(const WlGroupPlan& G) {
         wl_mac_one<S>(G.mac[i >> lw], i & (work - 1), G.N);
 }
 
-template <int MINB>
-__global__ void __launch_bounds__(kWlPThreads, MINB) k_wl_persistent(const __grid_constant__ WlPlan plan) {
+// The run as three cooperative kernels, each with the register budget its phases need
+// (so the memory-bound phases keep enough warps in flight):
+//   PART 0: forward column passes | grid barrier | forward tile passes
+//   PART 1: products of the chains and multiply-accumulates of the key switches
+//   PART 2: inverse tile passes | barrier | inverse column passes | barrier | divisions
+template <int PART>
+struct WlPartBlocks {
+    static constexpr int value = PART == 1 ? 2 : 3;
+};
+
+template <int PART>
+__global__ void __launch_bounds__(kWlPThreads, WlPartBlocks<PART>::value) k_wl_persistent(const __grid_constant__ WlPlan plan) {
     extern __shared__ __align__(128) double fsm[];
-    wl_stamp(plan, 0);
-    // 1: forward column passes
-    for (int g = 0; g < plan.ngroups; ++g) {
-        const WlGroupPlan& G = plan.groups[g];
-        if (G.K < G.logP && G.fwd_first.table_rows) wl_cols<false>(G.logP - G.K, G.fwd_first, G.K);
-    }
-    wl_grid_barrier(plan.barrier);
-    wl_stamp(plan, 1);
-    // 2: forward tile passes (after a column pass they read its centred doubles)
-    for (int g = 0; g < plan.ngroups; ++g) {
-        const WlGroupPlan& G = plan.groups[g];
-        if (!G.fwd_first.table_rows) continue;
-        if (G.K < G.logP) wl_tiles_k<false, true>(G.K, G.fwd_second, fsm);
-        else wl_tiles_k<false, false>(G.K, G.fwd_first, fsm);
-    }
-    wl_grid_barrier(plan.barrier);
-    wl_stamp(plan, 2);
-    // 3: products of the chains and multiply-accumulates of the key switches
-    for (int g = 0; g < plan.ngroups; ++g) {
-        const WlGroupPlan& G = plan.groups[g];
-        if (G.nprod) {
-            switch (G.S) {
-                case 1: wl_products_s<1>(G); break;
-                case 2: wl_products_s<2>(G); break;
-                default: wl_products_s<4>(G); break;
+    if constexpr (PART == 0) {
+        wl_stamp(plan, 0);
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (G.K < G.logP && G.fwd_first.table_rows) wl_cols<false>(G.logP - G.K, G.fwd_first, G.K);
+        }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 1);
+        // forward tile passes (after a column pass they read its centred doubles)
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (!G.fwd_first.table_rows) continue;
+            if (G.K < G.logP) wl_tiles_k<false, true>(G.K, G.fwd_second, fsm);
+            else wl_tiles_k<false, false>(G.K, G.fwd_first, fsm);
+        }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 2);
+    } else if constexpr (PART == 1) {
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (G.nprod) {
+                switch (G.S) {
+                    case 1: wl_products_s<1>(G); break;
+                    case 2: wl_products_s<2>(G); break;
+                    default: wl_products_s<4>(G); break;
+                }
+            }
+            if (G.nmac) {
+                switch (G.S) {
+                    case 1: wl_macs_s<1>(G); break;
+                    case 2: wl_macs_s<2>(G); break;
+                    default: wl_macs_s<4>(G); break;
+                }
             }
         }
-        if (G.nmac) {
-            switch (G.S) {
-                case 1: wl_macs_s<1>(G); break;
-                case 2: wl_macs_s<2>(G); break;
-                default: wl_macs_s<4>(G); break;
-            }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 3);
+    } else {
+        // inverse tile passes (before a column pass they leave centred doubles)
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (!G.inv_first.table_rows) continue;
+            if (G.K < G.logP) wl_tiles_k<true, true>(G.K, G.inv_first, fsm);
+            else wl_tiles_k<true, false>(G.K, G.inv_first, fsm);
         }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 4);
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (G.K < G.logP && G.inv_second.table_rows) wl_cols<true>(G.logP - G.K, G.inv_second, G.K);
+        }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 5);
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (!G.ndown) continue;
+            const int ln = 63 - __clzll(G.N);
+            const long long total = G.ndown << ln;
+            const long long stride = (long long)gridDim.x * blockDim.x;
+            for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+                wl_down_one(G.down[i >> ln], i & (G.N - 1), G.N, G.info);
+        }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 6);
     }
-    wl_grid_barrier(plan.barrier);
-    wl_stamp(plan, 3);
-    // 4: inverse tile passes (before a column pass they leave centred doubles)
-    for (int g = 0; g < plan.ngroups; ++g) {
-        const WlGroupPlan& G = plan.groups[g];
-        if (!G.inv_first.table_rows) continue;
-        if (G.K < G.logP) wl_tiles_k<true, true>(G.K, G.inv_first, fsm);
-        else wl_tiles_k<true, false>(G.K, G.inv_first, fsm);
-    }
-    wl_grid_barrier(plan.barrier);
-    wl_stamp(plan, 4);
-    // 5: inverse column passes
-    for (int g = 0; g < plan.ngroups; ++g) {
-        const WlGroupPlan& G = plan.groups[g];
-        if (G.K < G.logP && G.inv_second.table_rows) wl_cols<true>(G.logP - G.K, G.inv_second, G.K);
-    }
-    wl_grid_barrier(plan.barrier);
-    wl_stamp(plan, 5);
-    // 6: special-prime divisions
-    for (int g = 0; g < plan.ngroups; ++g) {
-        const WlGroupPlan& G = plan.groups[g];
-        if (!G.ndown) continue;
-        const int ln = 63 - __clzll(G.N);
-        const long long total = G.ndown << ln;
-        const long long stride = (long long)gridDim.x * blockDim.x;
-        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
-            wl_down_one(G.down[i >> ln], i & (G.N - 1), G.N, G.info);
-    }
-    wl_grid_barrier(plan.barrier);
-    wl_stamp(plan, 6);
 }
 
 constexpr size_t kWlPSmem = sizeof(double) * kWlPThreads * 17;  // TPC tiles of 17 TPT doubles, any K
@@ -424,7 +436,7 @@ struct WorkList {
     // persistent path
     bool persistent = false;
     WlPlan plan = {};
-    int grid = 0;
+    int grid[3] = {0, 0, 0};  // CTAs of each part (all resident)
 
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -505,7 +517,7 @@ int compile(WorkList& w) {
     }
     // persistent path: every row between 2^8 and 2^16 points (tile passes of at most
     // 2^12 points after a column pass of radix at most 16), split degree at most 4
-    bool persist = w.mode == 0 || w.mode == 2;
+    bool persist = w.mode == 0;
     for (const Group& G : w.groups)
         persist = persist && G.t->logP >= 8 && G.t->logP <= 16 && G.t->pub.split_degree <= 4;
     const size_t plan_bytes = persist ? align256(w.groups.size() * sizeof(WlGroupPlan)) + 256 : 0;
@@ -637,17 +649,19 @@ int compile(WorkList& w) {
         int nb = 0;
         int err = (int)cudaMemcpy(d_plans, plans.data(), plans.size() * sizeof(WlGroupPlan), cudaMemcpyHostToDevice);
         if (!err) err = (int)cudaMemset(d_bar, 0, 256);
-        if (!err)
-            err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &nb, w.mode == 2 ? k_wl_persistent<3> : k_wl_persistent<2>, kWlPThreads, kWlPSmem);
+        int nbp[3] = {0, 0, 0};
+        if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp[0], k_wl_persistent<0>, kWlPThreads, kWlPSmem);
+        if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp[1], k_wl_persistent<1>, kWlPThreads, kWlPSmem);
+        if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp[2], k_wl_persistent<2>, kWlPThreads, kWlPSmem);
+        nb = std::min(nbp[0], std::min(nbp[1], nbp[2]));
         if (!err && nb >= 1) {
+            for (int k = 0; k < 3; ++k) w.grid[k] = nbp[k] * sm_count();
             w.plan.groups = d_plans;
             w.plan.ngroups = (int)plans.size();
             w.plan.barrier = d_bar;
             w.plan.phase_ns = (unsigned long long*)((char*)d_bar + 64);
-            w.grid = nb * sm_count();
             w.persistent = true;
-            w.launches_per_run = 1;
+            w.launches_per_run = 3;
             return 0;
         }
         cudaGetLastError();  // the per-group graph below serves instead
@@ -856,20 +870,23 @@ int vfhe_cuda_worklist_run(void* wl, void* stream_) {
         // phases cannot wait on a CTA that has not started
         if (!vc::check_cuda(cudaMemsetAsync(w->plan.barrier, 0, 2 * sizeof(unsigned), st), "vfhe_cuda_worklist_run"))
             return 1;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)w->grid, 1, 1);
-        cfg.blockDim = dim3(vc::kWlPThreads, 1, 1);
-        cfg.dynamicSmemBytes = vc::kWlPSmem;
-        cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
         attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        const cudaError_t le = w->mode == 2 ? cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<3>, w->plan)
-                                            : cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<2>, w->plan);
-        if (!vc::check_cuda(le, "vfhe_cuda_worklist_run")) return 1;
-        vc::note_launch(1);
+        for (int part = 0; part < 3; ++part) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)w->grid[part], 1, 1);
+            cfg.blockDim = dim3(vc::kWlPThreads, 1, 1);
+            cfg.dynamicSmemBytes = vc::kWlPSmem;
+            cfg.stream = st;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const cudaError_t le = part == 0   ? cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<0>, w->plan)
+                                   : part == 1 ? cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<1>, w->plan)
+                                               : cudaLaunchKernelEx(&cfg, vc::k_wl_persistent<2>, w->plan);
+            if (!vc::check_cuda(le, "vfhe_cuda_worklist_run")) return 1;
+        }
+        vc::note_launch(3);
         return 0;
     }
     if (!vc::check_cuda(cudaGraphLaunch(w->exec, st), "vfhe_cuda_worklist_run")) return 1;
@@ -879,9 +896,8 @@ int vfhe_cuda_worklist_run(void* wl, void* stream_) {
 
 int vfhe_cuda_worklist_set_mode(void* wl, int mode) {
     WorkList* w = (WorkList*)wl;
-    if (!w || mode < 0 || mode > 2) {
-        vc::set_error("vfhe_cuda_worklist_set_mode",
-                      "mode is 0 (one persistent launch), 1 (graph of launches) or 2 (persistent, 3 CTAs per SM)");
+    if (!w || mode < 0 || mode > 1) {
+        vc::set_error("vfhe_cuda_worklist_set_mode", "mode is 0 (three persistent launches) or 1 (graph of launches)");
         return 1;
     }
     if (mode != w->mode) w->release();

@@ -1,11 +1,12 @@
 """Uneven batched work list over the C ABI (vfhe_cuda_worklist_*).
 
 Jobs of any mix of ring degree N and limb count L -- NTT -> product -> INTT chains and
-GHS key switches -- are compiled once into device-resident row tables and run as ONE
-persistent cooperative kernel per run (mode 0; six phases over every group's tables
-with grid barriers between them), or as a CUDA graph of one launch per stage per
-transform pool (mode 1, and the fallback for rows outside 2^8..2^16 points or split
-degrees above 4).  ``run_per_call`` executes the same jobs
+GHS key switches -- are compiled once into device-resident row tables and run as three
+persistent cooperative kernels per run (mode 0: forward transforms, products and
+multiply-accumulates, inverse transforms and divisions, each walking the tables of
+every transform pool with grid barriers between its phases), or as a CUDA graph of one
+launch per stage per transform pool (mode 1, and the fallback for rows outside
+2^8..2^16 points or split degrees above 4).  ``run_per_call`` executes the same jobs
 one entry-point call each (vfhe_cuda_ntt_mul_intt_batch / vfhe_cuda_keyswitch_batch
 with batch 1): the plain path the work list is measured against, and its parity
 reference on the GPU.
@@ -93,7 +94,7 @@ class WorkList:
 
     @property
     def launches(self) -> int:
-        """Kernels one run launches (1 on the persistent path)."""
+        """Kernels one run launches (3 on the persistent path)."""
         return int(self.lib.vfhe_cuda_worklist_launches(self.handle))
 
     @property
