@@ -27,6 +27,7 @@
 // per stage per group, groups as independent branches, transform shapes from the tuned
 // schedule of (log2 P, rows) (vfhe_cuda_ntt_set_schedule).
 #include <cuda_runtime.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -313,11 +314,22 @@ __device__ __forceinline__ void wl_macs_s(const WlGroupPlan& G) {
         wl_mac_one<S>(G.mac[i >> lw], i & (work - 1), G.N);
 }
 
+__device__ __forceinline__ void wl_downs(const WlGroupPlan& G) {
+    if (!G.ndown) return;
+    const int ln = 63 - __clzll(G.N);
+    const long long total = G.ndown << ln;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+        wl_down_one(G.down[i >> ln], i & (G.N - 1), G.N, G.info);
+}
+
 // The run as three cooperative kernels, each with the register budget its phases need
 // (so the memory-bound phases keep enough warps in flight):
-//   PART 0: forward column passes | grid barrier | forward tile passes
+//   PART 0: column passes of two-pass pools + one-pass transforms | grid barrier |
+//           tile passes of two-pass pools
 //   PART 1: products of the chains and multiply-accumulates of the key switches
-//   PART 2: inverse tile passes | barrier | inverse column passes | barrier | divisions
+//   PART 2: inverse tile passes | barrier | inverse column passes of two-pass pools +
+//           divisions of one-pass pools | barrier | divisions of two-pass pools
 template <int PART>
 struct WlPartBlocks {
     static constexpr int value = PART == 1 ? 2 : 3;
@@ -328,18 +340,22 @@ __global__ void __launch_bounds__(kWlPThreads, WlPartBlocks<PART>::value) k_wl_p
     extern __shared__ __align__(128) double fsm[];
     if constexpr (PART == 0) {
         wl_stamp(plan, 0);
+        // column passes of the two-pass pools, and beside them (they depend on no column
+        // pass) the whole transforms of the one-pass pools
         for (int g = 0; g < plan.ngroups; ++g) {
             const WlGroupPlan& G = plan.groups[g];
             if (G.K < G.logP && G.fwd_first.table_rows) wl_cols<false>(G.logP - G.K, G.fwd_first, G.K);
         }
-        wl_grid_barrier(plan.barrier);
-        wl_stamp(plan, 1);
-        // forward tile passes (after a column pass they read its centred doubles)
         for (int g = 0; g < plan.ngroups; ++g) {
             const WlGroupPlan& G = plan.groups[g];
-            if (!G.fwd_first.table_rows) continue;
-            if (G.K < G.logP) wl_tiles_k<false, true>(G.K, G.fwd_second, fsm);
-            else wl_tiles_k<false, false>(G.K, G.fwd_first, fsm);
+            if (G.K == G.logP && G.fwd_first.table_rows) wl_tiles_k<false, false>(G.K, G.fwd_first, fsm);
+        }
+        wl_grid_barrier(plan.barrier);
+        wl_stamp(plan, 1);
+        // tile passes of the two-pass pools (reading the column passes' centred doubles)
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (G.K < G.logP && G.fwd_first.table_rows) wl_tiles_k<false, true>(G.K, G.fwd_second, fsm);
         }
         wl_grid_barrier(plan.barrier);
         wl_stamp(plan, 2);
@@ -373,20 +389,21 @@ __global__ void __launch_bounds__(kWlPThreads, WlPartBlocks<PART>::value) k_wl_p
         }
         wl_grid_barrier(plan.barrier);
         wl_stamp(plan, 4);
+        // inverse column passes of the two-pass pools, and beside them the divisions of
+        // the one-pass pools (whose transforms are complete)
         for (int g = 0; g < plan.ngroups; ++g) {
             const WlGroupPlan& G = plan.groups[g];
             if (G.K < G.logP && G.inv_second.table_rows) wl_cols<true>(G.logP - G.K, G.inv_second, G.K);
+        }
+        for (int g = 0; g < plan.ngroups; ++g) {
+            const WlGroupPlan& G = plan.groups[g];
+            if (G.K == G.logP) wl_downs(G);
         }
         wl_grid_barrier(plan.barrier);
         wl_stamp(plan, 5);
         for (int g = 0; g < plan.ngroups; ++g) {
             const WlGroupPlan& G = plan.groups[g];
-            if (!G.ndown) continue;
-            const int ln = 63 - __clzll(G.N);
-            const long long total = G.ndown << ln;
-            const long long stride = (long long)gridDim.x * blockDim.x;
-            for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
-                wl_down_one(G.down[i >> ln], i & (G.N - 1), G.N, G.info);
+            if (G.K < G.logP) wl_downs(G);
         }
         wl_grid_barrier(plan.barrier);
         wl_stamp(plan, 6);
