@@ -270,21 +270,27 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
         w.run(stream)  # compile (+ capture) + first run
         torch.cuda.synchronize()
         if profile:
-            profile_range(None, "worklist", True)
+            profile_range(None, PROFILE_LEG, True)
         ev0.record(stream)
         for _ in range(reps):
             w.run(stream)
         ev1.record(stream)
         torch.cuda.synchronize()
         if profile:
-            profile_range(None, "worklist", False)
+            profile_range(None, PROFILE_LEG, False)
         return w, ev0.elapsed_time(ev1) / reps
 
-    wg, ms_graph = timed(1, False)
+    wg, ms_graph = timed(1, PROFILE_LEG == "worklist_graph")
     graph_launches = wg.launches
     graph_out = [j.out.clone() for j in jobs]
     wg.close()
-    wl, ms_wl = timed(0, True)
+    wl, ms_wl = timed(0, PROFILE_LEG == "worklist")
+    ph = eng.ffi.new("double[6]")
+    phases = None
+    if eng.lib.vfhe_cuda_worklist_phase_ms(wl.handle, ph) == 0:
+        phases = dict(zip(["forward_columns_and_one_pass", "forward_tiles_two_pass", "products_and_macs",
+                           "inverse_tiles", "inverse_columns_and_one_pass_divisions", "divisions_two_pass"],
+                          [round(ph[k], 3) for k in range(6)]))
     persistent_exact = all(torch.equal(j.out, g) for j, g in zip(jobs, graph_out))
     del graph_out
     outs = [torch.empty_like(j.out) for j in jobs]
@@ -303,7 +309,7 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
         "jobs": count, "jobs_per_s": count / (ms_wl * 1e-3), "ms_per_run": ms_wl,
         "per_call_jobs_per_s": count / (ms_pc * 1e-3), "per_call_ms": ms_pc, "per_call_calls": calls,
         "speedup_vs_per_call": ms_pc / ms_wl, "bit_exact_vs_per_call": bool(exact),
-        "kernels_per_run": wl.launches, "persistent": wl.persistent,
+        "kernels_per_run": wl.launches, "persistent": wl.persistent, "phase_ms_last_run": phases,
         "graph_of_pool_launches": {"jobs_per_s": count / (ms_graph * 1e-3), "ms_per_run": ms_graph,
                                    "kernels_per_run": graph_launches, "bit_exact_vs_persistent": bool(persistent_exact)},
         "device_bytes": wl.device_bytes,
@@ -1054,7 +1060,7 @@ def main() -> None:
     ap.add_argument("--no-cggi-million", action="store_true",
                     help="skip bootstrapping 10^6 LWEs to count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
-    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist"],
+    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist", "worklist_graph"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()
     global PROFILE_LEG
