@@ -33,6 +33,19 @@ struct LimbPrimes {
     uint32_t p[kMaxLimbs];
 };
 
+// Pass-through components folded into a key-switch accumulator before its inverse
+// transform: acc_i += (P mod q_i) * pass_i for the first nl extended limbs (the special
+// limbs get nothing, P mod P = 0).  Round division by P then yields acc / P + pass
+// exactly -- the reference adds pass after the division (mlwe.c:737-756) -- because
+// (acc_i + P pass_i + P/2 - t) P^-1 = (acc_i + P/2 - t) P^-1 + pass_i mod q_i, with t the
+// special limb's residue (unchanged by the fold).  pass rows are NTT domain.
+struct FoldConsts {
+    const uint64_t* pass;  // ciphertext b's component c: pass + b * stride + c * comp_stride (null: no fold)
+    long long stride, comp_stride;
+    int nl;
+    double pf[kMaxLimbs], pfq[kMaxLimbs];  // P mod q_i, centred, and fl(./q_i)
+};
+
 // Block o, slot x of the incomplete product u (*) v over S blocks of P slots
 // (polynomial_mul_RNS_polynomial, rns_polynomial.c:311-356).
 __device__ __forceinline__ uint64_t inc_prod_slot(const uint64_t* u, const uint64_t* v, int S, long long P,
@@ -413,7 +426,7 @@ __global__ void __launch_bounds__(256) k_mac_staged(uint64_t* __restrict__ acc, 
                                                     const uint64_t* __restrict__ order,
                                                     const __grid_constant__ LimbPrimes lp,
                                                     const PrimeInfo* __restrict__ primes, int nd, int ne,
-                                                    long long N) {
+                                                    long long N, const __grid_constant__ FoldConsts fold) {
     extern __shared__ __align__(128) uint64_t msm[];
     __shared__ uint64_t bars[kMacStages];
     const int by = blockIdx.y;
@@ -464,11 +477,26 @@ __global__ void __launch_bounds__(256) k_mac_staged(uint64_t* __restrict__ acc, 
         }
     }
     uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N + x0 + r;
+    sa0 = -sa0;
+    sa1 = -sa1;
+    sb0 = -sb0;
+    sb1 = -sb1;
+    if (fold.pass && i < fold.nl) {
+        // + (P mod q_i) pass_i (|sum| <= 3.5q + 3q/4 < 2^52)
+        const uint64_t* pa = fold.pass + (long long)b * fold.stride + (long long)i * N + x0 + r;
+        const ulonglong2 da = *reinterpret_cast<const ulonglong2*>(pa);
+        const ulonglong2 db = *reinterpret_cast<const ulonglong2*>(pa + fold.comp_stride);
+        const double w = fold.pf[i], wq = fold.pfq[i];
+        sa0 = __dadd_rn(sa0, f_mulmod(f_from_u64(da.x), w, wq, q));
+        sa1 = __dadd_rn(sa1, f_mulmod(f_from_u64(da.y), w, wq, q));
+        sb0 = __dadd_rn(sb0, f_mulmod(f_from_u64(db.x), w, wq, q));
+        sb1 = __dadd_rn(sb1, f_mulmod(f_from_u64(db.y), w, wq, q));
+    }
     ulonglong2 ra, rb;
-    ra.x = f_to_canonical(-sa0, q, qinv, pi.q);
-    ra.y = f_to_canonical(-sa1, q, qinv, pi.q);
-    rb.x = f_to_canonical(-sb0, q, qinv, pi.q);
-    rb.y = f_to_canonical(-sb1, q, qinv, pi.q);
+    ra.x = f_to_canonical(sa0, q, qinv, pi.q);
+    ra.y = f_to_canonical(sa1, q, qinv, pi.q);
+    rb.x = f_to_canonical(sb0, q, qinv, pi.q);
+    rb.y = f_to_canonical(sb1, q, qinv, pi.q);
     *reinterpret_cast<ulonglong2*>(oa) = ra;
     *reinterpret_cast<ulonglong2*>(oa + dstride) = rb;
 }
@@ -477,7 +505,14 @@ __global__ void __launch_bounds__(256) k_mac_staged(uint64_t* __restrict__ acc, 
 // so the pointwise one keeps its small register footprint).
 // keys_aligned: every key polynomial starts on a 16-byte boundary.
 void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
-                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned);
+                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned,
+                const FoldConsts* fold = nullptr);
+
+// Whether launch_mac takes the staged pointwise kernel (the only one that folds
+// pass-through components): split 1, FP64 primes, aligned rows, N a multiple of the
+// chunk.
+bool mac_staged_ok(IncNtt* t, const uint64_t* acc, const uint64_t* D, const LimbPrimes& lpe, int ne, long long N,
+                   bool keys_aligned);
 
 // Grid for one launch of a per-coefficient kernel; every call site launches exactly
 // one kernel with it, so it also counts the launch.
@@ -489,15 +524,24 @@ dim3 grid_xy(long long n, long long y) {
     return dim3((unsigned)blocks, (unsigned)y, 1);
 }
 
-void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
-                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned) {
+bool mac_staged_ok(IncNtt* t, const uint64_t* acc, const uint64_t* D, const LimbPrimes& lpe, int ne, long long N,
+                   bool keys_aligned) {
     bool pointwise = t->pub.split_degree == 1 && keys_aligned && (N & 1) == 0 &&
                      ((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(D)) & 15) == 0;
     for (int i = 0; i < ne && pointwise; ++i) pointwise = t->info[lpe.p[i]].fp64 != 0;
-    if (pointwise && N % kMacChunk == 0 && prepare_ckks_kernels() == 0) {
+    return pointwise && N % kMacChunk == 0 && prepare_ckks_kernels() == 0;
+}
+
+void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
+                const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned,
+                const FoldConsts* fold) {
+    if (mac_staged_ok(t, acc, D, lpe, ne, N, keys_aligned)) {
         note_launch();
         const dim3 g((unsigned)(N / kMacChunk), (unsigned)(B * ne), 1);
-        k_mac_staged<<<g, kMacChunk / 2, kMacSmem, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N);
+        FoldConsts none;
+        memset(&none, 0, sizeof none);
+        k_mac_staged<<<g, kMacChunk / 2, kMacSmem, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N,
+                                                          fold ? *fold : none);
         return;
     }
     const dim3 g = grid_xy(N, (long long)B * ne);
@@ -571,6 +615,27 @@ int blocks_transform(IncNtt* t, uint64_t* data, uint64_t count, const uint32_t* 
     rs.batch = (int)count;
     rs.batch_stride = (long long)nl * N;
     rs.in_batch_stride = rs.batch_stride;
+    mark_fp64(rs, t);
+    return launch_ntt(rs, t->d_info, inverse, st);
+}
+
+// In-place transform of the first [nl][N] block of `count` polynomials `stride` apart.
+int strided_transform(IncNtt* t, uint64_t* data, uint64_t count, long long stride, const uint32_t* lim, int nl,
+                      bool inverse, cudaStream_t st) {
+    const long long N = (long long)t->pub.N;
+    RowSet rs;
+    memset(&rs, 0, sizeof rs);
+    for (int i = 0; i < nl; ++i) {
+        rs.in[i] = data + (long long)i * N;
+        rs.out[i] = data + (long long)i * N;
+        rs.prime[i] = lim[i];
+    }
+    rs.nlimbs = nl;
+    rs.split = (int)t->pub.split_degree;
+    rs.logP = t->logP;
+    rs.batch = (int)count;
+    rs.batch_stride = stride;
+    rs.in_batch_stride = stride;
     mark_fp64(rs, t);
     return launch_ntt(rs, t->d_info, inverse, st);
 }
@@ -837,15 +902,41 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
         default: k_tensor<16><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
     }
     if (!check_cuda(cudaGetLastError(), where)) return 1;
-    if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
+    const bool rlk_aligned = (reinterpret_cast<uintptr_t>(rlk) & 15) == 0;
+    // d1 and d2 pass through the key switch: when the staged MAC runs they stay in the
+    // NTT domain and are folded into the accumulator (FoldConsts), so only d0 -- whose
+    // limbs are the digits -- goes back to the coefficient domain
+    const bool fold = mac_staged_ok(t, acc, D, lpe, ne, N, rlk_aligned) &&
+                      (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (N & 1) == 0;
+    if (fold) {
+        if (!check_cuda(strided_transform(t, T, B, 3LL * nl * N, limbs, nl, true, st), where)) return 1;
+    } else {
+        if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
+    }
     if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
-    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st,
-               (reinterpret_cast<uintptr_t>(rlk) & 15) == 0);
+    FoldConsts fc;
+    memset(&fc, 0, sizeof fc);
+    if (fold) {
+        fc.pass = T + (long long)nl * N;
+        fc.stride = 3LL * nl * N;
+        fc.comp_stride = (long long)nl * N;
+        fc.nl = nl;
+        const uint64_t P = t->info[special].q;
+        for (int i = 0; i < nl; ++i) {
+            const uint64_t q = t->info[limbs[i]].q;
+            const uint64_t r = P % q;
+            fc.pf[i] = r > q / 2 ? (double)r - (double)q : (double)r;
+            fc.pfq[i] = fc.pf[i] / (double)q;
+        }
+    }
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st, rlk_aligned,
+               fold ? &fc : nullptr);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
+    const int use_pass = fold ? 0 : 1;
     k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, T, 3LL * nl * N, (long long)nl * N,
-                                                            2LL * nl * N, 1, 1, mc, t->d_info, nl, 1, N);
+                                                            2LL * nl * N, use_pass, use_pass, mc, t->d_info, nl, 1, N);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
 }
 
