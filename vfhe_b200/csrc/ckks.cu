@@ -62,10 +62,13 @@ __device__ __forceinline__ uint64_t inc_prod_slot(const uint64_t* u, const uint6
 }
 
 // d0 = a1 a2, d1 = a1 b2 + b1 a2, d2 = b1 b2 in the NTT domain (mlwe.c:665-709 at rank 1).
+// dd (may be null, split 1 only): also write d0's limb k to dd + b dd_stride + k dd_step
+// -- the spectrum of key-switch digit k modulo its own prime, NTT(INTT(d0_k)) = d0_k.
 template <int S>
 __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ c1,
                          const uint64_t* __restrict__ c2, const __grid_constant__ LimbPrimes lp,
-                         const PrimeInfo* __restrict__ primes, int L, long long N) {
+                         const PrimeInfo* __restrict__ primes, int L, long long N, uint64_t* __restrict__ dd,
+                         long long dd_stride, long long dd_step) {
     const int by = blockIdx.y;
     const int b = by / L, k = by - b * L;
     const PrimeInfo pi = primes[lp.p[k]];
@@ -75,6 +78,7 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
     const uint64_t* a2 = c2 + b * cs + k * N;
     const uint64_t* b2 = a2 + LN;
     uint64_t* t0 = T + b * ts + k * N;
+    uint64_t* d0k = dd ? dd + b * dd_stride + k * dd_step : nullptr;
     if (S == 1 && pi.fp64 && (N & 1) == 0 &&
         ((reinterpret_cast<uintptr_t>(a1) | reinterpret_cast<uintptr_t>(a2) | reinterpret_cast<uintptr_t>(t0)) & 15) ==
             0) {
@@ -100,6 +104,7 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
             one(ua1.x, ub1.x, ua2.x, ub2.x, r0.x, r1.x, r2.x);
             one(ua1.y, ub1.y, ua2.y, ub2.y, r0.y, r1.y, r2.y);
             *reinterpret_cast<ulonglong2*>(t0 + x) = r0;
+            if (d0k) *reinterpret_cast<ulonglong2*>(d0k + x) = r0;
             *reinterpret_cast<ulonglong2*>(t0 + x + LN) = r1;
             *reinterpret_cast<ulonglong2*>(t0 + x + 2 * LN) = r2;
         }
@@ -110,6 +115,7 @@ __global__ void k_tensor(uint64_t* __restrict__ T, const uint64_t* __restrict__ 
              x += (long long)gridDim.x * blockDim.x) {
             const uint64_t va1 = a1[x], vb1 = b1[x], va2 = a2[x], vb2 = b2[x];
             t0[x] = mul_mod(va1, va2, pi);
+            if (d0k) d0k[x] = t0[x];
             t0[x + LN] = add_mod(mul_mod(va1, vb2, pi), mul_mod(vb1, va2, pi), pi.q);
             t0[x + 2 * LN] = mul_mod(vb1, vb2, pi);
         }
@@ -573,18 +579,22 @@ bool check_shape(IncNtt* t, const uint32_t* limbs, uint32_t L, uint32_t special,
 
 // Forward transforms of every digit: D[b][j][i] = NTT(d_j mod q_i), reading digit
 // rows from src (limb j at src + j N, polynomials src_stride apart).
+// skip_diag: the rows i == j are already in D (k_tensor's dd) and are not transformed.
 int digits_forward(IncNtt* t, uint64_t* D, const uint64_t* src, long long src_stride, uint64_t B,
-                   const uint32_t* ext, int nd, int ne, cudaStream_t st) {
+                   const uint32_t* ext, int nd, int ne, cudaStream_t st, bool skip_diag = false) {
     const long long N = (long long)t->pub.N;
     for (int j = 0; j < nd; ++j) {
         RowSet rs;
         memset(&rs, 0, sizeof rs);
+        int k = 0;
         for (int i = 0; i < ne; ++i) {
-            rs.in[i] = src + (long long)j * N;
-            rs.out[i] = D + ((long long)j * ne + i) * N;
-            rs.prime[i] = ext[i];
+            if (skip_diag && i == j) continue;
+            rs.in[k] = src + (long long)j * N;
+            rs.out[k] = D + ((long long)j * ne + i) * N;
+            rs.prime[k] = ext[i];
+            ++k;
         }
-        rs.nlimbs = ne;
+        rs.nlimbs = k;
         rs.split = (int)t->pub.split_degree;
         rs.logP = t->logP;
         rs.batch = (int)B;
@@ -892,28 +902,33 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
 
     std::vector<const uint64_t*> kp(B, rlk);
     if (!check_cuda(upload_small(keyptrs, (const uint64_t*)kp.data(), B, st), where)) return 1;
-    switch (t->pub.split_degree) {
-        case 1:  // the FP64 path takes two coefficients per thread
-            k_tensor<1><<<grid_xy((N + 1) / 2, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N);
-            break;
-        case 2: k_tensor<2><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
-        case 4: k_tensor<4><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
-        case 8: k_tensor<8><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
-        default: k_tensor<16><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N); break;
-    }
-    if (!check_cuda(cudaGetLastError(), where)) return 1;
     const bool rlk_aligned = (reinterpret_cast<uintptr_t>(rlk) & 15) == 0;
-    // d1 and d2 pass through the key switch: when the staged MAC runs they stay in the
-    // NTT domain and are folded into the accumulator (FoldConsts), so only d0 -- whose
-    // limbs are the digits -- goes back to the coefficient domain
+    // When the staged MAC runs: d1 and d2 pass through the key switch and stay in the
+    // NTT domain, folded into the accumulator (FoldConsts), so only d0 -- whose limbs are
+    // the digits -- goes back to the coefficient domain; and the spectrum of digit j
+    // modulo its own prime is d0's limb j itself, which the tensor kernel writes into the
+    // digit buffer, so those nl digit rows are not transformed.
     const bool fold = mac_staged_ok(t, acc, D, lpe, ne, N, rlk_aligned) &&
                       (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (N & 1) == 0;
+    const bool diag = fold;
+    switch (t->pub.split_degree) {
+        case 1:  // the FP64 path takes two coefficients per thread
+            k_tensor<1><<<grid_xy((N + 1) / 2, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N,
+                                                                              diag ? D : nullptr, (long long)nl * ne * N,
+                                                                              (long long)(ne + 1) * N);
+            break;
+        case 2: k_tensor<2><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N, nullptr, 0, 0); break;
+        case 4: k_tensor<4><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N, nullptr, 0, 0); break;
+        case 8: k_tensor<8><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N, nullptr, 0, 0); break;
+        default: k_tensor<16><<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(T, ct1, ct2, lp, t->d_info, nl, N, nullptr, 0, 0); break;
+    }
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (fold) {
         if (!check_cuda(strided_transform(t, T, B, 3LL * nl * N, limbs, nl, true, st), where)) return 1;
     } else {
         if (!check_cuda(blocks_transform(t, T, 3 * B, limbs, nl, true, st), where)) return 1;
     }
-    if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st), where)) return 1;
+    if (!check_cuda(digits_forward(t, D, T, 3LL * nl * N, B, ext, nl, ne, st, diag), where)) return 1;
     FoldConsts fc;
     memset(&fc, 0, sizeof fc);
     if (fold) {
