@@ -83,41 +83,68 @@ def decoded_error(s, key, ct, expect, delta) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms over the with-block.
+
+    Entering waits (at most 10 s) for the sampler's first line, so sampling is running
+    when the timed region starts; leaving waits (at most 1 s) for one more line, so a
+    region shorter than the sampling period still gets a sample taken at its end.  Only
+    lines that arrive after the first one are kept."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 50
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.out = None
+        self.lines: list[str] = []
+        self.kept: list[str] = []
+        self.thread = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+
+    def _wait_lines(self, n: int, limit_s: float) -> None:
+        t0 = time.monotonic()
+        while len(self.lines) < n and time.monotonic() - t0 < limit_s and self.thread.is_alive():
+            time.sleep(0.005)
 
     def __enter__(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.PERIOD_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        self._wait_lines(1, 10.0)
+        self.first = len(self.lines)
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out = ""
+        if self.proc is None:
+            return
+        self._wait_lines(self.first + 1, 1.0)
+        self.kept = list(self.lines[self.first:])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
 
     def summary(self) -> dict:
-        if not self.out:
+        if not self.kept:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.out.strip().splitlines():
+        for line in self.kept:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -1047,7 +1074,7 @@ def run_cuda_arm(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--pairs", type=int, default=PAIRS,
