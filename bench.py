@@ -791,6 +791,12 @@ def run_cuda_arm(args) -> None:
     from vfhe_b200.native import cuda_engine
 
     eng = cuda_engine()
+    for spec in args.ntt_schedule:
+        lp, rest = spec.split(":")
+        sched = [int(v) for v in rest.split(",")]
+        for bucket in range(32):
+            if eng.lib.vfhe_cuda_ntt_set_schedule(int(lp), bucket, *sched) != 0:
+                raise SystemExit(f"--ntt-schedule {spec}: refused by the engine")
     PAIRS = args.pairs  # noqa: N806  (the workload's batch; 256 unless profiling a small case)
     s, key, rlk, gks, rot_steps, zs, cts = build_workload(eng, PAIRS, SEED + rank)
     for c in cts:
@@ -949,6 +955,8 @@ def run_cuda_arm(args) -> None:
         kname = f"k_tile_fwd_f<{kt},0>"
     elif sched[2] == -1:
         kname = f"k_fused_fwd_f<{kt},{14 - kt}> (thread-block cluster)"
+    elif sched[2] == -2:
+        kname = f"k_flow_f<{kt},{14 - kt}> (column and tile passes in one dataflow launch)"
     else:
         kname = f"k_col_f<{14 - kt},0> + k_tile_fwd_f<{kt},1>"
     alg_bytes = PAIRS * ne * 16 * N_DEG
@@ -1029,7 +1037,8 @@ def run_cuda_arm(args) -> None:
         "vs_baseline": None,
         "dtype": "u64 (RNS residues < 2^50)",
         "data": "synthetic (seeded keys, noise and unit-disk slots)",
-        "config": dict(CONFIG, pairs_per_step=PAIRS),
+        "config": dict(CONFIG, pairs_per_step=PAIRS, **({"ntt_schedule_override": args.ntt_schedule}
+                                                         if args.ntt_schedule else {})),
         "e2e": {"value": e2e_value_plain, "unit": "pairs/s", "h2d_bytes_per_step": int(host1.nbytes + host2.nbytes),
                 "d2h_bytes_per_step": int(hout[0].numel() * 8), "ms_per_step": e2e_ms_plain,
                 "transport": "uint64 residue rows, the layout the cdef hands callers",
@@ -1087,6 +1096,9 @@ def main() -> None:
     ap.add_argument("--no-cggi-million", action="store_true",
                     help="skip bootstrapping 10^6 LWEs to count lookup mismatches (about a minute)")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per arrival rate in the serving leg")
+    ap.add_argument("--ntt-schedule", action="append", default=[], metavar="LOGP:K,TPC,CPS",
+                    help="override the tuned transform schedule of every row-count class of 2^LOGP-point rows "
+                         "(vfhe_cuda_ntt_set_schedule), e.g. 14:10,2,-2 for the dataflow launch")
     ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist", "worklist_graph"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()

@@ -435,16 +435,21 @@ int vfhe_cuda_keyswitch_batch(void *ntt, uint64_t *d_out, const uint64_t *d_ct, 
  * picked by the autotuner: tile_bits (P-point rows are split into a radix-2^(logP -
  * tile_bits) column pass and tiles of 2^tile_bits; == logP for one pass; 8..13),
  * tiles_per_cta (rows or row segments one CTA holds), ctas_per_sm (0: one CTA per tile
- * group; k: persistent grid of k CTAs per SM).  Zero = built-in default.  Schedules
+ * group; k: persistent grid of k CTAs per SM; -1: the row on a thread-block cluster of
+ * 2^(logP - tile_bits) CTAs, tile_bits 11..13; -2: column pass and tile pass as one
+ * dataflow launch, tile_bits 10..13 with logP - tile_bits 2..4, outside stream capture,
+ * tiles_per_cta then giving the work items per ticket, 1 or 2 (0: two); the two kernels
+ * otherwise).  Zero = built-in default.  Schedules
  * never change results.  get_schedule writes the three fields for a launch of `rows`
  * rows.  No counterpart in the reference (its transforms are single-threaded loops). */
 int vfhe_cuda_ntt_set_schedule(uint32_t logP, uint32_t rows_log2, int32_t tile_bits, int32_t tiles_per_cta,
                                int32_t ctas_per_sm);
 int vfhe_cuda_ntt_get_schedule(uint32_t logP, uint64_t rows, int32_t *out3);
 
-/* Nonzero when a kernel's bounded wait for a bulk copy gave up (a persistent transform
- * or the staged key-switch MAC; its results are then wrong); -1 when the flags cannot
- * be read.  Stays 0 in normal operation. */
+/* Nonzero when a kernel's bounded wait gave up (for a bulk copy in a persistent
+ * transform or the staged key-switch MAC, for a grid barrier of the persistent work
+ * list, or for the first pass of a dataflow transform; its results are then wrong);
+ * -1 when the flags cannot be read.  Stays 0 in normal operation. */
 int vfhe_cuda_device_faults(void);
 
 /* Reset the flags vfhe_cuda_device_faults reads.  0 on success. */

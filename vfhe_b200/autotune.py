@@ -45,7 +45,21 @@ def candidates(logP: int) -> list[tuple[int, int, int]]:
     for k in (11, 12, 13):
         if 1 <= logP - k <= 3:
             out.append((k, 0, -1))
+    # column pass and tile pass as one dataflow launch (ctas_per_sm = -2; tiles_per_cta =
+    # work items per ticket)
+    for k in (10, 11, 12, 13):
+        if flow_supported(k, logP - k):
+            out.extend((k, per, -2) for per in (1, 2))
     return out
+
+
+def flow_supported(k: int, k1: int) -> bool:
+    """Shapes of the dataflow launch (ntt_flow.cu): 2^k-point tiles, a radix-2^k1 column
+    pass, and the tiles of one 256-thread item in one row."""
+    if not (10 <= k <= 13 and 2 <= k1 <= 4):
+        return False
+    per_item = 1 if k >= 12 else (2 if k == 11 else 4)
+    return per_item <= (1 << k1)
 
 
 def _time_shape(engine: Engine, logP: int, rows: int, cands, reps: int = 5) -> list[tuple[float, tuple]]:
@@ -141,11 +155,17 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(DEFAULT_TABLE))
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--logp", type=int, nargs="*", default=None, help="tune only these log2 P (default 8..17)")
+    ap.add_argument("--merge", action="store_true", help="keep the --out table's entries for other log2 P")
     args = ap.parse_args()
     import torch
 
     eng = cuda_engine(apply_tuned=False)
-    table = tune(eng, reps=args.reps, verbose=True)
+    table = tune(eng, logps=args.logp or range(8, 18), reps=args.reps, verbose=True)
+    if args.merge:
+        old = load(Path(args.out)) or {}
+        old.update(table)
+        table = old
     out = {"device": torch.cuda.get_device_name(0), "table": table,
            "note": "ms = forward + inverse transform of 2^bucket rows of 2^logP, CUDA events"}
     Path(args.out).parent.mkdir(parents=True, exist_ok=True)

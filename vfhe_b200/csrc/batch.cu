@@ -250,7 +250,9 @@ int vfhe_cuda_device_faults(void) {
     if (!check_cuda(read_mac_fault(&m), "vfhe_cuda_device_faults")) return -1;
     int w = 0;
     if (!check_cuda(read_wl_fault(&w), "vfhe_cuda_device_faults")) return -1;
-    return f | m | w;
+    int d = 0;
+    if (!check_cuda(read_flow_fault(&d), "vfhe_cuda_device_faults")) return -1;
+    return f | m | w | d;
 }
 
 int vfhe_cuda_clear_device_faults(void) {
@@ -258,6 +260,7 @@ int vfhe_cuda_clear_device_faults(void) {
     if (!check_cuda(clear_tile_fault(), "vfhe_cuda_clear_device_faults")) return 1;
     if (!check_cuda(clear_mac_fault(), "vfhe_cuda_clear_device_faults")) return 1;
     if (!check_cuda(clear_wl_fault(), "vfhe_cuda_clear_device_faults")) return 1;
+    if (!check_cuda(clear_flow_fault(), "vfhe_cuda_clear_device_faults")) return 1;
     return 0;
 }
 

@@ -60,6 +60,8 @@ int vfhe_cuda_ntt_mul_intt_batch_noalloc(void* ntt, uint64_t* d_out, const uint6
     // ensure_ready only selects the device and creates the engine's stream; it
     // allocates no device memory
     if (!ensure_ready()) return 1;
+    // transform schedules that would allocate a counter buffer fall back to kernels that do not
+    const FlowNoAlloc no_alloc;
     IncNtt* t = as_ntt(ntt);
     if (!t || !limbs || !d_out || !d_a || !d_b || nlimbs == 0 || nlimbs > (uint32_t)kMaxLimbs || batch == 0) {
         set_error(where, "bad pool, buffers or limb list");

@@ -100,6 +100,27 @@ void forget_launches(uint64_t n);
 // stream capture, so that launches recorded into graphs make no attribute calls.
 int prepare_ntt_kernels();
 
+// Two-pass transform (radix-2^K1 column pass + 2^K-point tiles) as one dataflow launch
+// (ntt_flow.cu).  `first` / `second` are the two passes' row sets as launch_ntt_f64
+// builds them.  Returns kFlowUnavailable, having enqueued nothing, where the launch
+// cannot be made (stream capture, no counter buffer under FlowNoAlloc, an unsupported
+// shape); the caller then runs the two kernels.
+constexpr int kFlowUnavailable = -2;
+bool flow_supported(int K, int K1);
+// `per`: work items (one CTA's worth of columns or tiles) per ticket: 1 or 2 (0 = two).
+int flow_dispatch(int K, int K1, const RowSet& first, const RowSet& second, const PrimeInfo* d_primes, bool inverse,
+                  int per, cudaStream_t stream);
+// While one lives on this thread, transform launches allocate no device memory.
+struct FlowNoAlloc {
+    FlowNoAlloc();
+    ~FlowNoAlloc();
+    FlowNoAlloc(const FlowNoAlloc&) = delete;
+    FlowNoAlloc& operator=(const FlowNoAlloc&) = delete;
+};
+// The flag a dataflow launch raises when a wait for its first pass gave up (0 = never).
+int read_flow_fault(int* out);
+int clear_flow_fault();
+
 // Copy the device flag that persistent transform kernels raise when a bounded wait
 // for a tile copy gave up (0 = never).
 int read_tile_fault(int* out);

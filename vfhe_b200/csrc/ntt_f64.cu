@@ -600,11 +600,12 @@ bool set_ntt_schedule(int logP, int rows_log2, const NttSchedule& s) {
     if (logP < 8 || logP > kSchedMaxLogP || rows_log2 < 0 || rows_log2 >= kSchedRowBuckets) return false;
     if (s.tile_bits != 0 && (s.tile_bits < 8 || s.tile_bits > 13 || s.tile_bits > logP || logP - s.tile_bits > 5))
         return false;
-    if (s.tiles_per_cta < 0 || s.tiles_per_cta > 64 || s.ctas_per_sm < -1 || s.ctas_per_sm > 64) return false;
+    if (s.tiles_per_cta < 0 || s.tiles_per_cta > 64 || s.ctas_per_sm < -2 || s.ctas_per_sm > 64) return false;
     if (s.ctas_per_sm == -1) {  // fused cluster transform: K in 11..13, logP - K in 1..3
         const int K = s.tile_bits;
         if (K < 11 || K > 13 || logP - K < 1 || logP - K > 3) return false;
     }
+    if (s.ctas_per_sm == -2 && !flow_supported(s.tile_bits, logP - s.tile_bits)) return false;  // dataflow launch
     g_sched[logP][rows_log2] = s;
     return true;
 }
@@ -634,6 +635,10 @@ int launch_ntt_f64(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, 
     second.reduce_input = 0;
     second.table_src_is_dst = 1;
     int e;
+    if (sc.ctas_per_sm == -2 && flow_supported(K, K1)) {
+        e = flow_dispatch(K, K1, rows, second, d_primes, inverse, sc.tiles_per_cta, stream);
+        if (e != kFlowUnavailable) return e;
+    }
     if (!inverse) {
         e = col_dispatch(K1, rows, d_primes, false, K, stream);
         if (e) return e;

@@ -296,12 +296,27 @@ __device__ __forceinline__ double load_in(const uint64_t* p, bool in_double, boo
     return reduce ? f_reduce(v, c.q, c.qinv) : v;
 }
 
+// Barrier of one tile's threads.  GROUP: the CTA holds several independent tiles, and
+// each tile's 2^(K-4) threads (a multiple of 32) meet at their own named barrier 1 + grp,
+// so one tile's exchanges never wait for another's; otherwise the whole CTA meets.
+template <int K, bool GROUP>
+__device__ __forceinline__ void tile_sync(int grp) {
+    if constexpr (GROUP) {
+        static_assert((1 << (K - 4)) % 32 == 0, "a named barrier counts whole warps");
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "n"(1 << (K - 4)) : "memory");
+    } else {
+        __syncthreads();
+    }
+}
+
 // Forward transform of the low K bits of tile r (16 residues per thread t; the tile's
 // padded exchange buffer at sm).  STAGED: the input was copied into sm by a bulk copy;
 // otherwise it is read from r.src.  store: write the canonical output to r.dst (a
-// thread whose tile only pads out a group computes without storing).
-template <int K, bool IN_D, bool STAGED>
-__device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store) {
+// thread whose tile only pads out a group computes without storing).  GROUP, grp: the
+// tile's threads synchronise at named barrier 1 + grp (tile_sync).
+template <int K, bool IN_D, bool STAGED, bool GROUP = false>
+__device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store,
+                                             int grp = 0) {
     const PrimeInfo& pi = *r.pi;
     FCtx c;
     c.q = pi.qd;
@@ -325,7 +340,7 @@ __device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, 
         const uint64_t* staged = reinterpret_cast<const uint64_t*>(sm);
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = load_in(staged + own<L1>(t, m), IN_D, red, c);
-        __syncthreads();  // every input is in registers before the exchanges reuse the buffer
+        tile_sync<K, GROUP>(grp);  // every input is in registers before the exchanges reuse the buffer
     } else {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = load_in(r.src + own<L1>(t, m), IN_D, red, c);
@@ -334,23 +349,23 @@ __device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, 
     PassTw<L2, L1 - 1, L2> tw2;
     f_fwd_tw<K, L2, L1 - 1, L2>(tw2, t, hi, logP, c);
     fput<L1>(sm, x, t);
-    __syncthreads();
+    tile_sync<K, GROUP>(grp);
     fget<L2>(x, sm, t);
     f_fwd_bits<K, L2, L1 - 1, L2>(x, tw2, c);
     if constexpr (L2 > 0) {
         PassTw<L3, L2 - 1, L3> tw3;
         f_fwd_tw<K, L3, L2 - 1, L3>(tw3, t, hi, logP, c);
-        __syncthreads();
+        tile_sync<K, GROUP>(grp);
         fput<L2>(sm, x, t);
-        __syncthreads();
+        tile_sync<K, GROUP>(grp);
         fget<L3>(x, sm, t);
         f_fwd_bits<K, L3, L2 - 1, L3>(x, tw3, c);
         if constexpr (L3 > 0) {
             PassTw<0, L3 - 1, 0> tw4;
             f_fwd_tw<K, 0, L3 - 1, 0>(tw4, t, hi, logP, c);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fput<L3>(sm, x, t);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fget<0>(x, sm, t);
             f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
         }
@@ -361,8 +376,9 @@ __device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, 
 // Inverse transform of the low K bits of tile r.  FINAL (K == logP): P^-1 folded in,
 // canonical output; otherwise centred doubles for the column pass.  STAGED and store as
 // for tile_fwd_one.
-template <int K, bool FINAL, bool STAGED>
-__device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store) {
+template <int K, bool FINAL, bool STAGED, bool GROUP = false>
+__device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store,
+                                             int grp = 0) {
     const PrimeInfo& pi = *r.pi;
     FCtx c;
     c.q = pi.qd;
@@ -387,7 +403,7 @@ __device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, 
     } else {
         load16_u64(x, r.src + 16 * t);
     }
-    if (STAGED) __syncthreads();  // every input is in registers before the exchanges reuse the buffer
+    if (STAGED) tile_sync<K, GROUP>(grp);  // every input is in registers before the exchanges reuse the buffer
     PassTw<0, 0, 3> tw1;
     f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c);
     f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
@@ -395,37 +411,37 @@ __device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, 
         PassTw<F1, 4, K - 1> tw2;
         f_inv_tw<K, F1, 4, K - 1, FINAL>(tw2, t, hi, logP, c);
         fput<0>(sm, x, t);
-        __syncthreads();
+        tile_sync<K, GROUP>(grp);
         fget<F1>(x, sm, t);
         f_inv_bits<K, F1, 4, K - 1, FINAL>(x, tw2, c, pi);
     } else {
         PassTw<F1, 4, 7> tw2;
         f_inv_tw<K, F1, 4, 7, false>(tw2, t, hi, logP, c);
         fput<0>(sm, x, t);
-        __syncthreads();
+        tile_sync<K, GROUP>(grp);
         fget<F1>(x, sm, t);
         f_inv_bits<K, F1, 4, 7, false>(x, tw2, c, pi);
         if constexpr (K <= 12) {
             PassTw<F2, 8, K - 1> tw3;
             f_inv_tw<K, F2, 8, K - 1, FINAL>(tw3, t, hi, logP, c);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fput<F1>(sm, x, t);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fget<F2>(x, sm, t);
             f_inv_bits<K, F2, 8, K - 1, FINAL>(x, tw3, c, pi);
         } else {
             PassTw<F2, 8, 11> tw3;
             f_inv_tw<K, F2, 8, 11, false>(tw3, t, hi, logP, c);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fput<F1>(sm, x, t);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fget<F2>(x, sm, t);
             f_inv_bits<K, F2, 8, 11, false>(x, tw3, c, pi);
             PassTw<F3, 12, K - 1> tw4;
             f_inv_tw<K, F3, 12, K - 1, FINAL>(tw4, t, hi, logP, c);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fput<F2>(sm, x, t);
-            __syncthreads();
+            tile_sync<K, GROUP>(grp);
             fget<F3>(x, sm, t);
             f_inv_bits<K, F3, 12, K - 1, FINAL>(x, tw4, c, pi);
         }
