@@ -330,6 +330,9 @@ __device__ __forceinline__ void wl_downs(const WlGroupPlan& G) {
 //   PART 1: products of the chains and multiply-accumulates of the key switches
 //   PART 2: inverse tile passes | barrier | inverse column passes of two-pass pools +
 //           divisions of one-pass pools | barrier | divisions of two-pass pools
+// Resident CTAs per SM asked of the compiler: three for the transform phases (80
+// registers; the forward phase spills 388 bytes per thread, yet two CTAs per SM at 128
+// registers without spills measured 5% slower), two for the MACs.
 template <int PART>
 struct WlPartBlocks {
     static constexpr int value = PART == 1 ? 2 : 3;
