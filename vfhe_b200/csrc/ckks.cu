@@ -404,92 +404,45 @@ __global__ void k_permute_batch(uint64_t* __restrict__ out, const uint64_t* __re
 }
 
 // k_mac at split 1 for FP64 primes, its operands staged through shared memory by bulk
-// copies: block (chunk, row) walks the digits of kMacChunk residues of one extended
-// limb, and thread 0 keeps kMacStages digits (the digit chunk and both key chunks) in
-// flight ahead of the one being multiplied; the digits stream from HBM, the keys mostly
-// from L2.  Same result as k_mac<1>, which takes the shapes this kernel does not: N a
-// multiple of kMacChunk and every row 16-byte aligned (checked by the launcher).
+// copies: block (chunk, pair, limb) walks the digits of kMacChunk residues of one
+// extended limb for two ciphertexts that use the same key, and thread 0 keeps
+// kMacStages digits (both ciphertexts' digit chunks and one copy of the two key chunks)
+// in flight ahead of the one being multiplied; the digits stream from HBM, the keys
+// mostly from L2, each key chunk once per pair.  Same result as k_mac<1>, which takes
+// the shapes this kernel does not: N a multiple of kMacChunk and every row 16-byte
+// aligned (checked by the launcher).  Against one ciphertext per block, the pairs cut
+// the kernel's time by 12% (the key chunks' L2 traffic halves).
 constexpr int kMacChunk = 512;   // residues per block: two per thread
 constexpr int kMacStages = 4;    // digits in flight per block
-constexpr int kMacStageWords = 3 * kMacChunk;
+constexpr int kMacStageWords = 4 * kMacChunk;  // two digit chunks, two key chunks
 constexpr size_t kMacSmem = (size_t)kMacStages * kMacStageWords * 8;
 
 __device__ int vc_mac_fault;  // nonzero: a staged MAC copy wait gave up
 
-// Thread 0: request digit j's chunk and both key chunks into stage j mod kMacStages.
-__device__ __forceinline__ void mac_issue(uint64_t* msm, uint64_t* bars, const uint64_t* d, const uint64_t* ka, int j,
-                                          long long dstride, long long kstride) {
+// Thread 0: request digit j's chunks of both ciphertexts (d1 null: one ciphertext) and
+// both key chunks into stage j mod kMacStages.
+__device__ __forceinline__ void mac2_issue(uint64_t* msm, uint64_t* bars, const uint64_t* d0, const uint64_t* d1,
+                                           const uint64_t* ka, int j, long long dstride, long long kstride) {
     uint64_t* st = msm + (j % kMacStages) * kMacStageWords;
     uint64_t* bar = &bars[j % kMacStages];
-    mbar_expect_tx(bar, kMacStageWords * 8);
-    bulk_load(st, d + j * dstride, kMacChunk * 8, bar);
-    bulk_load(st + kMacChunk, ka + j * kstride, kMacChunk * 8, bar);
-    bulk_load(st + 2 * kMacChunk, ka + j * kstride + dstride, kMacChunk * 8, bar);
+    mbar_expect_tx(bar, (d1 ? 4 : 3) * kMacChunk * 8);
+    bulk_load(st, d0 + j * dstride, kMacChunk * 8, bar);
+    if (d1) bulk_load(st + kMacChunk, d1 + j * dstride, kMacChunk * 8, bar);
+    bulk_load(st + 2 * kMacChunk, ka + j * kstride, kMacChunk * 8, bar);
+    bulk_load(st + 3 * kMacChunk, ka + j * kstride + dstride, kMacChunk * 8, bar);
 }
 
-__global__ void __launch_bounds__(256) k_mac_staged(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
-                                                    const uint64_t* const* __restrict__ keys,
-                                                    const uint64_t* __restrict__ order,
-                                                    const __grid_constant__ LimbPrimes lp,
-                                                    const PrimeInfo* __restrict__ primes, int nd, int ne,
-                                                    long long N, const __grid_constant__ FoldConsts fold) {
-    extern __shared__ __align__(128) uint64_t msm[];
-    __shared__ uint64_t bars[kMacStages];
-    const int by = blockIdx.y;
-    const int bo = by / ne, i = by - bo * ne;
-    const int b = order ? (int)order[bo] : bo;
-    const long long x0 = (long long)blockIdx.x * kMacChunk;
-    const long long dstride = (long long)ne * N;
-    const long long kstride = (long long)2 * ne * N;
-    const uint64_t* d = D + (long long)b * nd * dstride + (long long)i * N + x0;
-    const uint64_t* ka = keys[b] + (long long)i * N + x0;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kMacStages; ++s) mbar_init(&bars[s], 1);
-        fence_mbar_init();
-        for (int j = 0; j < nd && j < kMacStages; ++j) mac_issue(msm, bars, d, ka, j, dstride, kstride);
-    }
-    __syncthreads();
-    const PrimeInfo& pi = primes[lp.p[i]];
-    const double q = pi.qd, qinv = pi.qinv;
-    const int r = 2 * threadIdx.x;
-    double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;
-    for (int j = 0; j < nd; ++j) {
-        const int s = j % kMacStages;
-        mbar_wait_bounded(&bars[s], (uint32_t)((j / kMacStages) & 1), &vc_mac_fault);
-        const uint64_t* st = msm + s * kMacStageWords;
-        const ulonglong2 dv = *reinterpret_cast<const ulonglong2*>(st + r);
-        const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(st + kMacChunk + r);
-        const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(st + 2 * kMacChunk + r);
-        // the digit is the multiplier of both key products (one quotient for two
-        // products; uncentred operands below 2^50, each term |t| <= 3q/4)
-        const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
-        const double vq0 = __dmul_rn(v0, qinv), vq1 = __dmul_rn(v1, qinv);
-        const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
-        const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
-        __syncthreads();  // every thread has read stage s: it may be refilled
-        if (threadIdx.x == 0 && j + kMacStages < nd) {
-            fence_proxy_async_smem();
-            mac_issue(msm, bars, d, ka, j + kMacStages, dstride, kstride);
-        }
-        sa0 = __dadd_rn(sa0, f_mulmod(wa0, v0, vq0, q));
-        sa1 = __dadd_rn(sa1, f_mulmod(wa1, v1, vq1, q));
-        sb0 = __dadd_rn(sb0, f_mulmod(wb0, v0, vq0, q));
-        sb1 = __dadd_rn(sb1, f_mulmod(wb1, v1, vq1, q));
-        if ((j & 3) == 3) {
-            sa0 = f_reduce(sa0, q, qinv);
-            sa1 = f_reduce(sa1, q, qinv);
-            sb0 = f_reduce(sb0, q, qinv);
-            sb1 = f_reduce(sb1, q, qinv);
-        }
-    }
-    uint64_t* oa = acc + (long long)b * 2 * dstride + (long long)i * N + x0 + r;
+// acc_k = -sum_j D_j (*) key_j (+ fold) for one ciphertext's two residues at r.
+__device__ __forceinline__ void mac2_store(uint64_t* acc, long long b, long long dstride, long long off, int i,
+                                           double sa0, double sa1, double sb0, double sb1,
+                                           const FoldConsts& fold, double q, double qinv, uint64_t qi) {
     sa0 = -sa0;
     sa1 = -sa1;
     sb0 = -sb0;
     sb1 = -sb1;
     if (fold.pass && i < fold.nl) {
         // + (P mod q_i) pass_i (|sum| <= 3.5q + 3q/4 < 2^52)
-        const uint64_t* pa = fold.pass + (long long)b * fold.stride + (long long)i * N + x0 + r;
+        const uint64_t* pa = fold.pass + b * fold.stride + off;
         const ulonglong2 da = *reinterpret_cast<const ulonglong2*>(pa);
         const ulonglong2 db = *reinterpret_cast<const ulonglong2*>(pa + fold.comp_stride);
         const double w = fold.pf[i], wq = fold.pfq[i];
@@ -499,24 +452,126 @@ __global__ void __launch_bounds__(256) k_mac_staged(uint64_t* __restrict__ acc, 
         sb1 = __dadd_rn(sb1, f_mulmod(f_from_u64(db.y), w, wq, q));
     }
     ulonglong2 ra, rb;
-    ra.x = f_to_canonical(sa0, q, qinv, pi.q);
-    ra.y = f_to_canonical(sa1, q, qinv, pi.q);
-    rb.x = f_to_canonical(sb0, q, qinv, pi.q);
-    rb.y = f_to_canonical(sb1, q, qinv, pi.q);
+    ra.x = f_to_canonical(sa0, q, qinv, qi);
+    ra.y = f_to_canonical(sa1, q, qinv, qi);
+    rb.x = f_to_canonical(sb0, q, qinv, qi);
+    rb.y = f_to_canonical(sb1, q, qinv, qi);
+    uint64_t* oa = acc + b * 2 * dstride + off;
     *reinterpret_cast<ulonglong2*>(oa) = ra;
     *reinterpret_cast<ulonglong2*>(oa + dstride) = rb;
+}
+
+// pairs[k] = b0 | (b1 + 1) << 32 (b1 = -1: b0 alone).
+__global__ void __launch_bounds__(256) k_mac_paired(uint64_t* __restrict__ acc, const uint64_t* __restrict__ D,
+                                                    const uint64_t* const* __restrict__ keys,
+                                                    const uint64_t* __restrict__ pairs,
+                                                    const __grid_constant__ LimbPrimes lp,
+                                                    const PrimeInfo* __restrict__ primes, int nd, int ne,
+                                                    long long N, const __grid_constant__ FoldConsts fold) {
+    extern __shared__ __align__(128) uint64_t msm[];
+    __shared__ uint64_t bars[kMacStages];
+    const int by = blockIdx.y;
+    const int bp = by / ne, i = by - bp * ne;
+    const uint64_t pr = pairs[bp];
+    const long long b0 = (long long)(pr & 0xffffffffULL);
+    const long long b1 = (long long)(pr >> 32) - 1;
+    const bool two = b1 >= 0;
+    const long long x0 = (long long)blockIdx.x * kMacChunk;
+    const long long dstride = (long long)ne * N;
+    const long long kstride = (long long)2 * ne * N;
+    const uint64_t* d0 = D + b0 * nd * dstride + (long long)i * N + x0;
+    const uint64_t* d1 = two ? D + b1 * nd * dstride + (long long)i * N + x0 : nullptr;
+    const uint64_t* ka = keys[b0] + (long long)i * N + x0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kMacStages; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+        for (int j = 0; j < nd && j < kMacStages; ++j) mac2_issue(msm, bars, d0, d1, ka, j, dstride, kstride);
+    }
+    __syncthreads();
+    const PrimeInfo& pi = primes[lp.p[i]];
+    const double q = pi.qd, qinv = pi.qinv;
+    const int r = 2 * threadIdx.x;
+    double sa0 = 0.0, sb0 = 0.0, sa1 = 0.0, sb1 = 0.0;  // ciphertext b0
+    double ta0 = 0.0, tb0 = 0.0, ta1 = 0.0, tb1 = 0.0;  // ciphertext b1
+    for (int j = 0; j < nd; ++j) {
+        const int s = j % kMacStages;
+        mbar_wait_bounded(&bars[s], (uint32_t)((j / kMacStages) & 1), &vc_mac_fault);
+        const uint64_t* st = msm + s * kMacStageWords;
+        const ulonglong2 dv = *reinterpret_cast<const ulonglong2*>(st + r);
+        const ulonglong2 ev = two ? *reinterpret_cast<const ulonglong2*>(st + kMacChunk + r) : make_ulonglong2(0, 0);
+        const ulonglong2 av = *reinterpret_cast<const ulonglong2*>(st + 2 * kMacChunk + r);
+        const ulonglong2 bv = *reinterpret_cast<const ulonglong2*>(st + 3 * kMacChunk + r);
+        // each digit multiplies both key products (one quotient for two products;
+        // uncentred operands below 2^50, each term |t| <= 3q/4)
+        const double v0 = f_from_u64(dv.x), v1 = f_from_u64(dv.y);
+        const double u0 = f_from_u64(ev.x), u1 = f_from_u64(ev.y);
+        const double wa0 = f_from_u64(av.x), wa1 = f_from_u64(av.y);
+        const double wb0 = f_from_u64(bv.x), wb1 = f_from_u64(bv.y);
+        __syncthreads();  // every thread has read stage s: it may be refilled
+        if (threadIdx.x == 0 && j + kMacStages < nd) {
+            fence_proxy_async_smem();
+            mac2_issue(msm, bars, d0, d1, ka, j + kMacStages, dstride, kstride);
+        }
+        const double vq0 = __dmul_rn(v0, qinv), vq1 = __dmul_rn(v1, qinv);
+        sa0 = __dadd_rn(sa0, f_mulmod(wa0, v0, vq0, q));
+        sa1 = __dadd_rn(sa1, f_mulmod(wa1, v1, vq1, q));
+        sb0 = __dadd_rn(sb0, f_mulmod(wb0, v0, vq0, q));
+        sb1 = __dadd_rn(sb1, f_mulmod(wb1, v1, vq1, q));
+        if (two) {
+            const double uq0 = __dmul_rn(u0, qinv), uq1 = __dmul_rn(u1, qinv);
+            ta0 = __dadd_rn(ta0, f_mulmod(wa0, u0, uq0, q));
+            ta1 = __dadd_rn(ta1, f_mulmod(wa1, u1, uq1, q));
+            tb0 = __dadd_rn(tb0, f_mulmod(wb0, u0, uq0, q));
+            tb1 = __dadd_rn(tb1, f_mulmod(wb1, u1, uq1, q));
+        }
+        if ((j & 3) == 3) {
+            sa0 = f_reduce(sa0, q, qinv);
+            sa1 = f_reduce(sa1, q, qinv);
+            sb0 = f_reduce(sb0, q, qinv);
+            sb1 = f_reduce(sb1, q, qinv);
+            ta0 = f_reduce(ta0, q, qinv);
+            ta1 = f_reduce(ta1, q, qinv);
+            tb0 = f_reduce(tb0, q, qinv);
+            tb1 = f_reduce(tb1, q, qinv);
+        }
+    }
+    const long long off = (long long)i * N + x0 + r;
+    mac2_store(acc, b0, dstride, off, i, sa0, sa1, sb0, sb1, fold, q, qinv, pi.q);
+    if (two) mac2_store(acc, b1, dstride, off, i, ta0, ta1, tb0, tb1, fold, q, qinv, pi.q);
 }
 
 // One k_mac launch for the ring's split degree (each split degree is its own kernel,
 // so the pointwise one keeps its small register footprint).
 // keys_aligned: every key polynomial starts on a 16-byte boundary.
+// pairs (device, npairs entries, see k_mac_paired): the staged kernel runs when they are
+// given and its shape conditions hold (mac_staged_ok); k_mac otherwise.
 void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
                 const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned,
-                const FoldConsts* fold = nullptr);
+                const FoldConsts* fold = nullptr, const uint64_t* pairs = nullptr, uint64_t npairs = 0);
 
-// Whether launch_mac takes the staged pointwise kernel (the only one that folds
-// pass-through components): split 1, FP64 primes, aligned rows, N a multiple of the
-// chunk.
+// Pairs of consecutive ciphertexts (in `order`, or 0..B-1) whose key pointers are
+// equal, singles elsewhere, in k_mac_paired's encoding; returns the count.
+uint64_t key_pairs(const uint64_t* const* keys, const uint64_t* order, uint64_t B, uint64_t* out) {
+    uint64_t n = 0;
+    for (uint64_t p = 0; p < B;) {
+        const uint64_t b0 = order ? order[p] : p;
+        if (p + 1 < B) {
+            const uint64_t b1 = order ? order[p + 1] : p + 1;
+            if (keys[b0] == keys[b1]) {
+                out[n++] = b0 | ((b1 + 1) << 32);
+                p += 2;
+                continue;
+            }
+        }
+        out[n++] = b0;
+        p += 1;
+    }
+    return n;
+}
+
+// Whether launch_mac, given key pairs, takes the staged pointwise kernel (the only one
+// that folds pass-through components): split 1, FP64 primes, aligned rows, N a multiple
+// of the chunk.
 bool mac_staged_ok(IncNtt* t, const uint64_t* acc, const uint64_t* D, const LimbPrimes& lpe, int ne, long long N,
                    bool keys_aligned);
 
@@ -540,13 +595,14 @@ bool mac_staged_ok(IncNtt* t, const uint64_t* acc, const uint64_t* D, const Limb
 
 void launch_mac(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* const* keys, const uint64_t* order,
                 const LimbPrimes& lpe, int nd, int ne, long long N, uint64_t B, cudaStream_t st, bool keys_aligned,
-                const FoldConsts* fold) {
-    if (mac_staged_ok(t, acc, D, lpe, ne, N, keys_aligned)) {
+                const FoldConsts* fold, const uint64_t* pairs, uint64_t npairs) {
+    // (the callers that fold pass-through components check mac_staged_ok and pass pairs)
+    if (pairs && npairs && mac_staged_ok(t, acc, D, lpe, ne, N, keys_aligned)) {
         note_launch();
-        const dim3 g((unsigned)(N / kMacChunk), (unsigned)(B * ne), 1);
         FoldConsts none;
         memset(&none, 0, sizeof none);
-        k_mac_staged<<<g, kMacChunk / 2, kMacSmem, st>>>(acc, D, keys, order, lpe, t->d_info, nd, ne, N,
+        const dim3 g((unsigned)(N / kMacChunk), (unsigned)(npairs * ne), 1);
+        k_mac_paired<<<g, kMacChunk / 2, kMacSmem, st>>>(acc, D, keys, pairs, lpe, t->d_info, nd, ne, N,
                                                           fold ? *fold : none);
         return;
     }
@@ -783,7 +839,7 @@ int prepare_ckks_kernels() {
     static std::once_flag once;
     static int err = 0;
     std::call_once(once, [] {
-        err = (int)cudaFuncSetAttribute(k_mac_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMacSmem);
+        err = (int)cudaFuncSetAttribute(k_mac_paired, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMacSmem);
     });
     return err;
 }
@@ -872,7 +928,7 @@ uint64_t ckks_mul_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
 
 uint64_t ckks_rot_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
     const uint64_t ne = L + 1;
-    return B * N * (2 * L + L * ne + 2 * ne) + 3 * B + 64;
+    return B * N * (2 * L + L * ne + 2 * ne) + 4 * B + 64;
 }
 
 int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const uint64_t* ct2, uint64_t B,
@@ -900,6 +956,7 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     uint64_t* acc = D + B * (uint64_t)nl * ne * N;      // [B][2][ne][N]
     uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
 
+    uint64_t* d_pairs = keyptrs + B;                    // [B]
     std::vector<const uint64_t*> kp(B, rlk);
     if (!check_cuda(upload_small(keyptrs, (const uint64_t*)kp.data(), B, st), where)) return 1;
     const bool rlk_aligned = (reinterpret_cast<uintptr_t>(rlk) & 15) == 0;
@@ -944,8 +1001,12 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
             fc.pfq[i] = fc.pf[i] / (double)q;
         }
     }
+    // every ciphertext uses the relinearisation key: pairs (0, 1), (2, 3), ...
+    std::vector<uint64_t> pairs(B);
+    const uint64_t npairs = key_pairs(kp.data(), nullptr, B, pairs.data());
+    if (!check_cuda(upload_small(d_pairs, pairs.data(), npairs, st), where)) return 1;
     launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st, rlk_aligned,
-               fold ? &fc : nullptr);
+               fold ? &fc : nullptr, d_pairs, npairs);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
@@ -990,6 +1051,7 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     uint64_t* keyptrs = acc + B * 2 * ne * N;           // [B]
     uint64_t* d_gens = keyptrs + B;                     // [B]
     uint64_t* d_order = d_gens + B;                     // [B]
+    uint64_t* d_pairs = d_order + B;                    // [B]
     if (!check_cuda(upload_small(keyptrs, (const uint64_t*)gks, B, st), where)) return 1;
     // ciphertexts grouped by key (stable), so each key is read from HBM about once
     std::vector<uint64_t> order(B);
@@ -1018,8 +1080,12 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     if (!check_cuda(digits_forward(t, D, src, 2LL * nl * N, B, ext, nl, ne, st), where)) return 1;
     bool keys_aligned = true;
     for (uint64_t b = 0; b < B; ++b) keys_aligned = keys_aligned && (reinterpret_cast<uintptr_t>(gks[b]) & 15) == 0;
+    // ciphertexts that share a Galois key (adjacent in the key-grouped order) in pairs
+    std::vector<uint64_t> pairs(B);
+    const uint64_t npairs = key_pairs(gks, order.data(), B, pairs.data());
+    if (!check_cuda(upload_small(d_pairs, pairs.data(), npairs, st), where)) return 1;
     launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st,
-               keys_aligned);
+               keys_aligned, nullptr, d_pairs, npairs);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
