@@ -964,7 +964,7 @@ def run_cuda_arm(args) -> None:
     achieved = alg_bytes / (ntt_ms * 1e-3) / 1e9
     del buf
 
-    # ---- secondary: N = 2^16, L = 24 forward NTT limbs/s (the survey's NTT metric), on
+    # ---- secondary: N = 2^16, L = 24 forward NTT limbs/s (the NTT headline metric), on
     # 64 polynomials (805 MB, larger than L2, so every transform streams from HBM)
     from vfhe_b200.arith import Ring
 

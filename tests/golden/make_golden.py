@@ -6,8 +6,8 @@ portable engine from its sources (oracle/_ref/libvfhe_ref_portable.so):
     python tests/golden/make_golden.py
 
 Writes ntt_kats.json:
-  * "forward": for the rings of the survey's known-answer table (N=4096 at split 4 and
-    1, and the N=2^14 CKKS chain) -- limb-0 input (0x123456789ABCDEF + i) mod q in the
+  * "forward": for the rings of the independent known-answer table in
+    tests/test_golden.py (N=4096 at split 4 and 1, and the N=2^14 CKKS chain) -- limb-0 input (0x123456789ABCDEF + i) mod q in the
     raw row layout, forward transform through polynomial_RNSc_to_RNS; the ring primes,
     the first 64 outputs of every limb, a SHA-256 of all output rows, and w[0][0:8] of
     the pool's twist table;

@@ -1,7 +1,7 @@
 """Golden vectors generated by the reference's own library (tests/golden/make_golden.py):
-the oracle (CPU) and the cuda engine (GPU) must reproduce them bit for bit.  The survey's
-independent known-answer table (fwd[0:4] of limb 0 and w[0][0:2] per ring) pins the
-fixture itself."""
+the oracle (CPU) and the cuda engine (GPU) must reproduce them bit for bit.  An
+independent known-answer table (fwd[0:4] of limb 0 and w[0][0:2] per ring, taken from
+the reference's portable and IFMA engines, which agree) pins the fixture itself."""
 
 from __future__ import annotations
 
@@ -63,7 +63,7 @@ def check_engine(engine):
         assert _sha(got) == case["sha256"]
 
 
-def test_fixture_agrees_with_the_survey_table():
+def test_fixture_agrees_with_the_known_answer_table():
     for (N, split, fwd4, w2), case in zip(REFERENCE_KAT, GOLDEN["forward"]):
         assert (case["N"], case["split"]) == (N, split)
         assert case["head"][0][:4] == fwd4
