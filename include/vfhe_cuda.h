@@ -297,7 +297,11 @@ int vfhe_cuda_poly_mul_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a, co
                              uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
 
 /* Fused NTT -> incomplete product -> INTT for `batch` pairs of coefficient-domain
- * polynomials [batch][nlimbs][N]: d_out = INTT(NTT(d_a) * NTT(d_b)). */
+ * polynomials [batch][nlimbs][N]: d_out = INTT(NTT(d_a) * NTT(d_b)).  One kernel, no
+ * scratch, for primes below 2^50, N <= 2^13, 2^9 <= N / split_degree and 16-byte
+ * aligned buffers (one CTA per row); otherwise four launches with engine scratch.
+ * Replaces the chain polynomial_RNSc_to_RNS x2, polynomial_mul_RNS_polynomial,
+ * polynomial_RNS_to_RNSc (rns_polynomial.c:311-356, 582-614). */
 int vfhe_cuda_ntt_mul_intt_batch(void *ntt, uint64_t *d_out, const uint64_t *d_a, const uint64_t *d_b,
                                  uint64_t batch, const uint32_t *limbs, uint32_t nlimbs, void *stream);
 

@@ -137,6 +137,11 @@ int vfhe_cuda_ntt_mul_intt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_a
     IncNtt* t = as_ntt(ntt);
     if (!t) return 1;
     cudaStream_t st = (cudaStream_t)stream_;
+    if (d_out && d_a && d_b && limbs) {
+        // one kernel per chain where the shape allows (chain.cu); the same residues
+        const int e = launch_chain(t, d_out, d_a, d_b, batch, limbs, nlimbs, st);
+        if (e != kChainUnavailable) return check_cuda(e, "vfhe_cuda_ntt_mul_intt_batch") ? 0 : 1;
+    }
     uint64_t* tmp = engine_workspace(batch * nlimbs * t->pub.N * 8, st);
     if (!tmp) return 1;
     int rc = vfhe_cuda_ntt_batch(ntt, 0, tmp, d_b, batch, limbs, nlimbs, stream_);

@@ -162,6 +162,15 @@ int upload_small(uint64_t* d_dst, const uint64_t* h_src, uint64_t n, cudaStream_
 int launch_inc_product(int mode, const EwSet& set, int split, int logP, const PrimeInfo* d_primes,
                        cudaStream_t st);
 
+// NTT -> product -> INTT of batch x nlimbs rows ([batch][nlimbs][N], 16-byte aligned)
+// in one kernel (chain.cu): FP64 primes, N <= 2^13, 2^9 <= P <= 2^13.  Returns
+// kChainUnavailable, having enqueued nothing, for other shapes; else a cudaError_t.
+constexpr int kChainUnavailable = -2;
+int launch_chain(IncNtt* t, uint64_t* out, const uint64_t* a, const uint64_t* b, uint64_t batch,
+                 const uint32_t* limbs, uint32_t nlimbs, cudaStream_t st);
+// Shared-memory attributes of the chain kernels, set once outside any stream capture.
+int prepare_chain_kernels();
+
 // Galois permutation x -> x^gen (rns_polynomial.c:996-1035).
 int launch_permute(const EwSet& set, uint64_t N, int split, uint64_t gen, const PrimeInfo* d_primes,
                    cudaStream_t st);

@@ -585,8 +585,11 @@ int clear_tile_fault() {
     return (int)cudaMemcpyToSymbol(vc_tile_fault, &zero, sizeof(int));
 }
 
+int prepare_chain_kernels();
+
 int prepare_ntt_kernels() {
     int e = prepare_ckks_kernels();
+    if (!e) e = prepare_chain_kernels();
     if (!e) e = prepare_k<8>();
     if (!e) e = prepare_k<9>();
     if (!e) e = prepare_k<10>();

@@ -309,14 +309,17 @@ __device__ __forceinline__ void tile_sync(int grp) {
     }
 }
 
-// Forward transform of the low K bits of tile r (16 residues per thread t; the tile's
-// padded exchange buffer at sm).  STAGED: the input was copied into sm by a bulk copy;
-// otherwise it is read from r.src.  store: write the canonical output to r.dst (a
-// thread whose tile only pads out a group computes without storing).  GROUP, grp: the
-// tile's threads synchronise at named barrier 1 + grp (tile_sync).
+// Forward transform of the low K bits of tile r of a 2^logP-point row (16 residues per
+// thread t; the tile's padded exchange buffer at sm); red: reduce each input modulo the
+// row's prime on load.  STAGED: the input was copied into sm by a bulk copy; otherwise
+// it is read from r.src.  tile_fwd_regs leaves the result in x (x[m] at index 16 t + m
+// of the tile, |x| < 2^51, not reduced); tile_fwd_one stores it canonically to r.dst
+// when `store` is set (a thread whose tile only pads out a group computes without
+// storing).  GROUP, grp: the tile's threads synchronise at named barrier 1 + grp
+// (tile_sync).
 template <int K, bool IN_D, bool STAGED, bool GROUP = false>
-__device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store,
-                                             int grp = 0) {
+__device__ __forceinline__ void tile_fwd_regs(const Tile& r, int logP, bool red, double* sm, int t, double (&x)[16],
+                                              int grp = 0) {
     const PrimeInfo& pi = *r.pi;
     FCtx c;
     c.q = pi.qd;
@@ -325,13 +328,11 @@ __device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, 
     c.lt = reinterpret_cast<const double2*>(pi.fwd_lane);
     c.mt = reinterpret_cast<const double2*>(pi.fwd_mid);
     c.lazy = fwd_lazy(pi);
-    const int logP = rows.logP, hi = r.hi;
-    double x[16];
+    const int hi = r.hi;
 
     constexpr int L1 = K - 4;
     constexpr int L2 = (K - 8) > 0 ? (K - 8) : 0;
     constexpr int L3 = (K - 12) > 0 ? (K - 12) : 0;
-    const bool red = rows.reduce_input != 0;
     // each pass's twiddles are requested before the exchange that precedes the pass,
     // so their latency overlaps the barrier
     PassTw<L1, K - 1, L1> tw1;
@@ -370,40 +371,32 @@ __device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, 
             f_fwd_bits<K, 0, L3 - 1, 0>(x, tw4, c);
         }
     }
-    if (store) store16_canonical(r.dst + 16 * t, x, c.q, c.qinv, pi.q);
 }
 
-// Inverse transform of the low K bits of tile r.  FINAL (K == logP): P^-1 folded in,
-// canonical output; otherwise centred doubles for the column pass.  STAGED and store as
-// for tile_fwd_one.
-template <int K, bool FINAL, bool STAGED, bool GROUP = false>
-__device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store,
+template <int K, bool IN_D, bool STAGED, bool GROUP = false>
+__device__ __forceinline__ void tile_fwd_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store,
                                              int grp = 0) {
-    const PrimeInfo& pi = *r.pi;
+    double x[16];
+    tile_fwd_regs<K, IN_D, STAGED, GROUP>(r, rows.logP, rows.reduce_input != 0, sm, t, x, grp);
+    if (store) store16_canonical(r.dst + 16 * t, x, r.pi->qd, r.pi->qinv, r.pi->q);
+}
+
+// Inverse passes of the low K bits of one tile whose 16 residues per thread t are in x
+// (x[m] at index 16 t + m, |x| < q; the forward passes leave this layout).  FINAL
+// (K == logP): P^-1 folded in.  On return x[m] is at index own<K - 4>(t, m) of the tile.
+template <int K, bool FINAL, bool GROUP = false>
+__device__ __forceinline__ void tile_inv_regs(const PrimeInfo& pi, int logP, int hi, double* sm, int t,
+                                              double (&x)[16], int grp = 0) {
     FCtx c;
     c.q = pi.qd;
     c.qinv = pi.qinv;
     c.tw = reinterpret_cast<const double2*>(pi.inv_d);
     c.lt = reinterpret_cast<const double2*>(pi.inv_lane);
     c.mt = reinterpret_cast<const double2*>(pi.inv_mid);
-    const int logP = rows.logP, hi = r.hi;
-    double x[16];
 
     constexpr int F1 = 4 < (K - 4) ? 4 : (K - 4);
     constexpr int F2 = 8 < (K - 4) ? 8 : (K - 4);
     constexpr int F3 = 12 < (K - 4) ? 12 : (K - 4);
-    if (STAGED) {
-        const ulonglong2* in = reinterpret_cast<const ulonglong2*>(reinterpret_cast<const uint64_t*>(sm) + 16 * t);
-#pragma unroll
-        for (int m = 0; m < 16; m += 2) {
-            const ulonglong2 v = in[m / 2];
-            x[m] = f_from_u64(v.x);
-            x[m + 1] = f_from_u64(v.y);
-        }
-    } else {
-        load16_u64(x, r.src + 16 * t);
-    }
-    if (STAGED) tile_sync<K, GROUP>(grp);  // every input is in registers before the exchanges reuse the buffer
     PassTw<0, 0, 3> tw1;
     f_inv_tw<K, 0, 0, 3, false>(tw1, t, hi, logP, c);
     f_inv_bits<K, 0, 0, 3, false>(x, tw1, c, pi);
@@ -446,12 +439,35 @@ __device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, 
             f_inv_bits<K, F3, 12, K - 1, FINAL>(x, tw4, c, pi);
         }
     }
+}
+
+// Inverse transform of the low K bits of tile r.  FINAL (K == logP): P^-1 folded in,
+// canonical output; otherwise centred doubles for the column pass.  STAGED and store as
+// for tile_fwd_one.
+template <int K, bool FINAL, bool STAGED, bool GROUP = false>
+__device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, double* sm, int t, bool store,
+                                             int grp = 0) {
+    const PrimeInfo& pi = *r.pi;
+    double x[16];
+    if (STAGED) {
+        const ulonglong2* in = reinterpret_cast<const ulonglong2*>(reinterpret_cast<const uint64_t*>(sm) + 16 * t);
+#pragma unroll
+        for (int m = 0; m < 16; m += 2) {
+            const ulonglong2 v = in[m / 2];
+            x[m] = f_from_u64(v.x);
+            x[m + 1] = f_from_u64(v.y);
+        }
+    } else {
+        load16_u64(x, r.src + 16 * t);
+    }
+    if (STAGED) tile_sync<K, GROUP>(grp);  // every input is in registers before the exchanges reuse the buffer
+    tile_inv_regs<K, FINAL, GROUP>(pi, rows.logP, r.hi, sm, t, x, grp);
     constexpr int LAST = K - 4;
     if (!store) return;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
         uint64_t* p = r.dst + own<LAST>(t, m);
-        if (FINAL) *p = f_to_canonical(x[m], c.q, c.qinv, pi.q);
+        if (FINAL) *p = f_to_canonical(x[m], pi.qd, pi.qinv, pi.q);
         else *p = (uint64_t)__double_as_longlong(x[m]);
     }
 }
