@@ -617,12 +617,15 @@ def ntt_round_trip_leg(eng, reps: int = 20, cpu_budget: float = 3.0) -> dict:
             call()
         torch.cuda.synchronize()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        leg = "roundtrip" if split is None else "roundtrip_split1"
+        profile_range(None, leg, True)
         for e0, e1 in evs:
             flush.zero_()
             e0.record(stream)
             call()
             e1.record(stream)
         torch.cuda.synchronize()
+        profile_range(None, leg, False)
         ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
         # end to end from pinned host buffers
         hA = torch.from_numpy(ha.view(np.int64)).pin_memory()
@@ -1099,7 +1102,8 @@ def main() -> None:
     ap.add_argument("--ntt-schedule", action="append", default=[], metavar="LOGP:K,TPC,CPS",
                     help="override the tuned transform schedule of every row-count class of 2^LOGP-point rows "
                          "(vfhe_cuda_ntt_set_schedule), e.g. 14:10,2,-2 for the dataflow launch")
-    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist", "worklist_graph"],
+    ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist", "worklist_graph",
+                             "roundtrip", "roundtrip_split1"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()
     global PROFILE_LEG
