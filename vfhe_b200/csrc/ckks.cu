@@ -14,6 +14,7 @@
 //     inverse transform at the start of its rescale are both skipped: they are
 //     inverse bijections on canonical residues, so skipping them changes no bit.
 #include <cuda_runtime.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -24,6 +25,7 @@
 #include "bulk.cuh"
 #include "fp64mod.cuh"
 #include "keyswitch.cuh"
+#include "ntt_f64_dev.cuh"
 
 namespace vc {
 
@@ -364,6 +366,105 @@ __global__ void k_moddown(uint64_t* __restrict__ out, const uint64_t* __restrict
         }
     }
     (void)psp;
+}
+
+constexpr int kColdownThreads = 128;
+
+// The inverse transform's column pass (its last 2^K1-point stages, index bits KT..logP-1
+// of each 2^logP-point block) of the key-switch accumulators, fused with k_moddown's
+// FP64 form (k_moddown works coefficient by coefficient, so the split layout does not
+// matter to it): thread (block column cx,
+// ciphertext b, component c) finishes coefficients cx + m 2^KT of the special limb first
+// and keeps (t + p/2) mod p of them, then (rescaling) finishes and divides the top limb
+// and keeps its rounded value, then finishes, divides (and rescales) every output limb.
+// The accumulator rows hold the tile pass's centred doubles; they are read once and the
+// coefficient-domain accumulator never reaches HBM.  Per coefficient the operations are
+// k_moddown's, in the same order, so the residues are the same.
+template <int K1>
+__global__ void __launch_bounds__(kColdownThreads, 6) k_coldown(uint64_t* __restrict__ out, const uint64_t* __restrict__ acc,
+                                                 const uint64_t* __restrict__ pass, long long pass_stride,
+                                                 long long pass_off_a, long long pass_off_b, int use_pass_a,
+                                                 int use_pass_b, const __grid_constant__ ModDownConsts mc,
+                                                 const PrimeInfo* __restrict__ primes, int nl, int rescale, long long N,
+                                                 int logP, int KT) {
+    constexpr int R = 1 << K1;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // block g >> KT, column g mod 2^KT
+    if (g >= (N >> K1)) return;  // no barriers in this kernel
+    const long long cx = ((g >> KT) << logP) + (g & ((1LL << KT) - 1));
+    const int b = (int)(blockIdx.y >> 1), c = (int)(blockIdx.y & 1);
+    const int ne = nl + 1;
+    const int nout = rescale ? nl - 1 : nl;
+    const uint64_t* a = acc + ((long long)b * 2 + c) * ne * N + cx;
+    uint64_t* o = out + ((long long)b * 2 + c) * nout * N + cx;
+    const int use_pass = c == 0 ? use_pass_a : use_pass_b;
+    const uint64_t* ps = use_pass ? pass + (long long)b * pass_stride + (c == 0 ? pass_off_a : pass_off_b) + cx : nullptr;
+
+    // limb `row` of the accumulator in the coefficient domain: canonical residues as doubles
+    auto finish = [&](int row, const PrimeInfo& pi, double (&v)[R]) {
+#pragma unroll
+        for (int m = 0; m < R; ++m)
+            v[m] = __longlong_as_double((long long)__ldcs(a + (long long)row * N + ((long long)m << KT)));
+        col_inv_regs<K1>(v, pi, logP, KT);
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = f_from_u64(f_to_canonical(v[m], pi.qd, pi.qinv, pi.q));
+    };
+    // The special limb's (t + p/2) mod p and the rescale's rounded top limb stay in
+    // shared memory, entry m of this thread at [m][threadIdx.x] (conflict-free), so the
+    // registers hold one limb's column at a time.
+    __shared__ double td[R][kColdownThreads], sd[R][kColdownThreads];
+    const int tx = threadIdx.x;
+    // limb i after the special-prime division and the pass-through add, |v| < 7q/4
+    auto divide = [&](int i, double (&v)[R]) {
+        const PrimeInfo& pi = primes[mc.prime[i]];
+        finish(i, pi, v);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const double y = __dadd_rn(__dadd_rn(v[m], mc.half_sp_d[i]), -td[m][tx]);
+            v[m] = f_mulmod(y, mc.inv_sp_d[i], mc.inv_sp_dq[i], pi.qd);
+            if (ps) v[m] = __dadd_rn(v[m], f_from_u64(__ldcs(ps + (long long)i * N + ((long long)m << KT))));
+        }
+    };
+
+    double v[R];
+    {
+        const PrimeInfo& psp = primes[mc.special];
+        finish(nl, psp, v);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            uint64_t t = (uint64_t)v[m] + mc.half_p;
+            t -= t >= mc.p ? mc.p : 0;
+            td[m][tx] = f_from_u64(t);
+        }
+    }
+    if (!rescale) {
+        for (int i = 0; i < nl; ++i) {
+            const PrimeInfo& pi = primes[mc.prime[i]];
+            divide(i, v);
+#pragma unroll
+            for (int m = 0; m < R; ++m) o[(long long)i * N + ((long long)m << KT)] = f_to_canonical(v[m], pi.qd, pi.qinv, pi.q);
+        }
+        return;
+    }
+    {
+        const PrimeInfo& pt = primes[mc.prime[nl - 1]];
+        divide(nl - 1, v);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            uint64_t s = f_to_canonical(v[m], pt.qd, pt.qinv, pt.q) + mc.half_top;
+            s -= s >= mc.q_top ? mc.q_top : 0;
+            sd[m][tx] = f_from_u64(s);
+        }
+    }
+    for (int i = 0; i < nl - 1; ++i) {
+        const PrimeInfo& pi = primes[mc.prime[i]];
+        divide(i, v);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const double y = __dadd_rn(__dadd_rn(v[m], mc.half_r_d[i]), -sd[m][tx]);
+            o[(long long)i * N + ((long long)m << KT)] =
+                f_to_canonical(f_mulmod(y, mc.inv_r_d[i], mc.inv_r_dq[i], pi.qd), pi.qd, pi.qinv, pi.q);
+        }
+    }
 }
 
 // Galois permutation of both components, per-ciphertext generator (rns_polynomial.c:996-1035:
@@ -931,6 +1032,67 @@ uint64_t ckks_rot_ws_elems(uint64_t N, uint64_t B, uint64_t L) {
     return B * N * (2 * L + L * ne + 2 * ne) + 4 * B + 64;
 }
 
+namespace {
+// VFHE_CUDA_CKKS_UNFUSED=1: the whole inverse transform, then k_moddown (the fused and
+// unfused forms give the same residues; tests compare them)
+bool coldown_disabled() {
+    const char* s = getenv("VFHE_CUDA_CKKS_UNFUSED");
+    return s && atoi(s) != 0;
+}
+
+// Inverse transform of the key-switch accumulators [B][2][ne][N] (in place; limbs
+// ext[0..ne-1], the special prime last) and the special-prime division (+ pass-through,
+// + rescale by ext[ne-2]) into out.  Where every prime takes the FP64 form and the
+// transform's schedule is a tile pass plus a column pass of at most 16 points, the
+// column pass runs inside the division (k_coldown); otherwise the whole transform runs
+// and then k_moddown.
+int acc_inverse_moddown(IncNtt* t, uint64_t* out, uint64_t* acc, uint64_t B, const uint32_t* ext, int ne,
+                        const ModDownConsts& mc, const uint64_t* pass, long long pass_stride, long long off_a,
+                        long long off_b, int use_a, int use_b, int rescale, cudaStream_t st) {
+    const long long N = (long long)t->pub.N;
+    const int nl = ne - 1;
+    if (mc.fp64 && !coldown_disabled()) {
+        RowSet rs;
+        memset(&rs, 0, sizeof rs);
+        for (int i = 0; i < ne; ++i) {
+            rs.in[i] = acc + (long long)i * N;
+            rs.out[i] = acc + (long long)i * N;
+            rs.prime[i] = ext[i];
+        }
+        rs.nlimbs = ne;
+        rs.split = (int)t->pub.split_degree;
+        rs.logP = t->logP;
+        rs.batch = (int)(2 * B);
+        rs.batch_stride = (long long)ne * N;
+        rs.in_batch_stride = rs.batch_stride;
+        mark_fp64(rs, t);
+        int K1 = 0, KT = 0;
+        const int e = launch_ntt_f64_inverse_tiles(rs, t->d_info, 4, &K1, &KT, st);
+        if (e != kTilePassUnavailable) {
+            if (e) return e;
+            const dim3 g((unsigned)(((N >> K1) + kColdownThreads - 1) / kColdownThreads), (unsigned)(2 * B), 1);
+            note_launch();
+#define VC_COLDOWN(K1V)                                                                                          \
+    k_coldown<K1V><<<g, kColdownThreads, 0, st>>>(out, acc, pass, pass_stride, off_a, off_b, use_a, use_b, mc, t->d_info, nl, \
+                                      rescale, N, t->logP, KT)
+            switch (K1) {
+                case 1: VC_COLDOWN(1); break;
+                case 2: VC_COLDOWN(2); break;
+                case 3: VC_COLDOWN(3); break;
+                default: VC_COLDOWN(4); break;
+            }
+#undef VC_COLDOWN
+            return (int)cudaGetLastError();
+        }
+    }
+    const int e = blocks_transform(t, acc, 2 * B, ext, ne, true, st);
+    if (e) return e;
+    k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, pass, pass_stride, off_a, off_b, use_a,
+                                                                    use_b, mc, t->d_info, nl, rescale, N);
+    return (int)cudaGetLastError();
+}
+}  // namespace
+
 int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const uint64_t* ct2, uint64_t B,
                            const uint32_t* limbs, uint32_t L, uint32_t special, const uint64_t* rlk,
                            uint64_t* ws, cudaStream_t st) {
@@ -1008,12 +1170,13 @@ int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const 
     launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, nullptr, lpe, nl, ne, N, B, st, rlk_aligned,
                fold ? &fc : nullptr, d_pairs, npairs);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
-    if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
     const int use_pass = fold ? 0 : 1;
-    k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, T, 3LL * nl * N, (long long)nl * N,
-                                                            2LL * nl * N, use_pass, use_pass, mc, t->d_info, nl, 1, N);
-    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+    return check_cuda(acc_inverse_moddown(t, out, acc, B, ext, ne, mc, T, 3LL * nl * N, (long long)nl * N,
+                                          2LL * nl * N, use_pass, use_pass, 1, st),
+                      where)
+               ? 0
+               : 1;
 }
 
 // gens == nullptr: a plain key switch of every ciphertext (no automorphism); the
@@ -1087,11 +1250,11 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
     launch_mac(t, acc, D, (const uint64_t* const*)keyptrs, identity ? nullptr : d_order, lpe, nl, ne, N, B, st,
                keys_aligned, nullptr, d_pairs, npairs);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
-    if (!check_cuda(blocks_transform(t, acc, 2 * B, ext, ne, true, st), where)) return 1;
     const ModDownConsts mc = moddown_consts(t, limbs, nl, special);
-    k_moddown<<<grid_xy((N + 1) / 2, (long long)B * 2), 256, 0, st>>>(out, acc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1,
-                                                            mc, t->d_info, nl, 0, N);
-    return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+    return check_cuda(acc_inverse_moddown(t, out, acc, B, ext, ne, mc, src, 2LL * nl * N, 0, (long long)nl * N, 0, 1, 0, st),
+                      where)
+               ? 0
+               : 1;
 }
 
 namespace {

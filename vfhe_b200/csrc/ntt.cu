@@ -141,6 +141,25 @@ int g_force_generic = -1;
 int g_force_int = -1;
 }  // namespace
 
+namespace {
+void read_force_flags() {
+    if (g_force_generic < 0) {
+        const char* s = getenv("VFHE_CUDA_NTT_GENERIC");
+        g_force_generic = (s && atoi(s)) ? 1 : 0;
+    }
+    if (g_force_int < 0) {
+        const char* s = getenv("VFHE_CUDA_NTT_INT");
+        g_force_int = (s && atoi(s)) ? 1 : 0;
+    }
+}
+}  // namespace
+
+bool ntt_f64_eligible(const RowSet& rows) {
+    read_force_flags();
+    return !rows.table && rows.batch > 0 && rows.nlimbs > 0 && !g_force_generic && !g_force_int && rows.fp64 &&
+           rows.logP >= 8 && rows.logP <= 17 && rows_aligned16(rows);
+}
+
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream) {
     const int logP = rows.logP;
     if (rows.table) {
@@ -150,14 +169,7 @@ int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cuda
         return e == -1 ? (int)cudaErrorInvalidValue : e;
     }
     if (rows.batch <= 0 || rows.nlimbs <= 0) return 0;
-    if (g_force_generic < 0) {
-        const char* s = getenv("VFHE_CUDA_NTT_GENERIC");
-        g_force_generic = (s && atoi(s)) ? 1 : 0;
-    }
-    if (g_force_int < 0) {
-        const char* s = getenv("VFHE_CUDA_NTT_INT");
-        g_force_int = (s && atoi(s)) ? 1 : 0;
-    }
+    read_force_flags();
     if (!g_force_generic && logP >= 8 && logP <= 17 && rows_aligned16(rows)) {
         if (rows.fp64 && !g_force_int) {
             const int e = launch_ntt_f64(rows, d_primes, inverse, stream);

@@ -89,6 +89,16 @@ int sm_count();
 // Work is enqueued on `stream`; returns a cudaError_t code (0 on success).
 int launch_ntt(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, cudaStream_t stream);
 
+// Only the tile pass of an inverse FP64 transform (rows aligned, all primes below
+// 2^50) whose tuned schedule is a tile pass + a column pass of K1 <= max_k1 bits:
+// the rows are left as centred doubles, and *K1_out / *KT_out receive the column and
+// tile bits the caller's fused column pass must cover.  Returns kTilePassUnavailable,
+// having enqueued nothing, for any other schedule; else a cudaError_t code.
+constexpr int kTilePassUnavailable = -3;
+bool ntt_f64_eligible(const RowSet& rows);  // launch_ntt would take the FP64 kernels
+int launch_ntt_f64_inverse_tiles(const RowSet& rows, const PrimeInfo* d_primes, int max_k1, int* K1_out, int* KT_out,
+                                 cudaStream_t stream);
+
 // Count of kernels this engine has launched (vfhe_cuda_launch_count).  Kernels
 // recorded into a CUDA graph are counted at capture; the capturing code takes that
 // count back (forget_launches) and notes it again at every replay.

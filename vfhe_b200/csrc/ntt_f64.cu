@@ -652,4 +652,22 @@ int launch_ntt_f64(const RowSet& rows, const PrimeInfo* d_primes, bool inverse, 
     return col_dispatch(K1, second, d_primes, true, K, stream);
 }
 
+// The tile pass of an inverse transform whose schedule is a plain tile pass + column
+// pass with at most `max_k1` column bits: the rows are left as centred doubles for a
+// caller that fuses the column pass (and what follows it) into its own kernel.  Returns
+// kTilePassUnavailable, having enqueued nothing, for any other schedule.
+int launch_ntt_f64_inverse_tiles(const RowSet& rows, const PrimeInfo* d_primes, int max_k1, int* K1_out, int* KT_out,
+                                 cudaStream_t stream) {
+    const int logP = rows.logP;
+    if (!ntt_f64_eligible(rows)) return kTilePassUnavailable;
+    const NttSchedule sc = get_ntt_schedule(logP, rowset_rows(rows));
+    int K = sc.tile_bits ? sc.tile_bits : (logP <= 13 ? logP : 12);
+    if (K > logP || logP - K > 5) K = logP <= 13 ? logP : 12;
+    const int K1 = logP - K;
+    if (K1 < 1 || K1 > max_k1 || sc.ctas_per_sm < 0) return kTilePassUnavailable;
+    *K1_out = K1;
+    *KT_out = K;
+    return tile_dispatch(K, rows, d_primes, 3, 1 << K1, sc, stream);
+}
+
 }  // namespace vc

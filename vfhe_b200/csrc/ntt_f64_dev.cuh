@@ -472,6 +472,39 @@ __device__ __forceinline__ void tile_inv_one(const Tile& r, const RowSet& rows, 
     }
 }
 
+// The inverse column stages (index bits KT .. KT + K1 - 1, the transform's last, P^-1
+// folded into the final stage) of one column whose x[m] sits at index m 2^KT + column:
+// centred doubles from the tile pass in, centred values |x| < 2^51 out.
+template <int K1>
+__device__ __forceinline__ void col_inv_regs(double (&x)[1 << K1], const PrimeInfo& pi, int logP, int KT) {
+    constexpr int R = 1 << K1;
+    const double q = pi.qd, qinv = pi.qinv;
+    const double2* tw = reinterpret_cast<const double2*>(pi.inv_d);
+#pragma unroll
+    for (int bb = 0; bb < K1; ++bb) {
+        const int base = (1 << logP) >> (bb + KT + 1);
+        const bool last = bb == K1 - 1;
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            if (m & (1 << bb)) continue;
+            const double u = x[m], v = x[m | (1 << bb)];
+            if (last) {
+                x[m] = f_mulmod(__dadd_rn(u, v), pi.pinv_d, pi.pinv_q, q);
+                x[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), pi.ilast_d, pi.ilast_q, q);
+            } else {
+                const double2 w = __ldg(&tw[base + (m >> (bb + 1))]);
+                x[m] = __dadd_rn(u, v);
+                x[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), w.x, w.y, q);
+            }
+        }
+        if (!last && (bb & 1)) {
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                if (!(m & (1 << bb))) x[m] = f_reduce(x[m], q, qinv);
+        }
+    }
+}
+
 // Column-pass work of column gc (see k_col_f below).
 template <int K1, bool INV>
 __device__ __forceinline__ void col_one(const RowSet& rows, const PrimeInfo* __restrict__ primes, long long gc,
@@ -532,32 +565,9 @@ __device__ __forceinline__ void col_one(const RowSet& rows, const PrimeInfo* __r
         for (int m = 0; m < R; ++m)
             dst[(long long)m << KT] = (uint64_t)__double_as_longlong(lazy ? x[m] : f_reduce(x[m], q, qinv));
     } else {
-        const double2* tw = reinterpret_cast<const double2*>(pi.inv_d);
 #pragma unroll
         for (int m = 0; m < R; ++m) x[m] = __longlong_as_double((long long)src[(long long)m << KT]);
-#pragma unroll
-        for (int bb = 0; bb < K1; ++bb) {
-            const int base = (1 << logP) >> (bb + KT + 1);
-            const bool last = bb == K1 - 1;
-#pragma unroll
-            for (int m = 0; m < R; ++m) {
-                if (m & (1 << bb)) continue;
-                const double u = x[m], v = x[m | (1 << bb)];
-                if (last) {
-                    x[m] = f_mulmod(__dadd_rn(u, v), pi.pinv_d, pi.pinv_q, q);
-                    x[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), pi.ilast_d, pi.ilast_q, q);
-                } else {
-                    const double2 w = __ldg(&tw[base + (m >> (bb + 1))]);
-                    x[m] = __dadd_rn(u, v);
-                    x[m | (1 << bb)] = f_mulmod(__dsub_rn(u, v), w.x, w.y, q);
-                }
-            }
-            if (!last && (bb & 1)) {
-#pragma unroll
-                for (int m = 0; m < R; ++m)
-                    if (!(m & (1 << bb))) x[m] = f_reduce(x[m], q, qinv);
-            }
-        }
+        col_inv_regs<K1>(x, pi, logP, KT);
 #pragma unroll
         for (int m = 0; m < R; ++m) dst[(long long)m << KT] = f_to_canonical(x[m], q, qinv, pi.q);
     }
