@@ -50,30 +50,47 @@ CONFIG = {
     "special_primes": 1,
     "pairs_per_step": PAIRS,
     "l2_policy": "inputs larger than L2 (1.2 GB of ciphertexts per step)",
-    "parallelism": "replicas, ciphertext pairs sharded by rank (no data-path collective)",
+    "parallelism": "replicas, ciphertext pairs sharded by rank (no data-path collective): one job of "
+                   "world x 256 pairs from one seed, rank r takes pairs [256 r, 256 (r + 1))",
 }
 
 
 # ----------------------------------------------------------------------------- setup
-def build_workload(engine, pairs: int, seed: int, gk_steps=STEPS_SET):
-    """Keys and ciphertexts through the reference API mirror (seeded, engine-independent)."""
+def pair_share(rank: int, pairs_per_rank: int) -> range:
+    """Global indices of the ciphertext pairs one rank processes.  The job is
+    world x pairs_per_rank pairs drawn from one seed; rank r takes the r-th block of
+    pairs_per_rank, so the shares are disjoint and together are the whole job (weak
+    scaling: the per-rank share is fixed as ranks are added)."""
+    return range(rank * pairs_per_rank, (rank + 1) * pairs_per_rank)
+
+
+def build_workload(engine, pairs: int, seed: int, first_pair: int = 0, gk_steps=STEPS_SET, n: int = N_DEG,
+                   prime_sizes=PRIME_SIZES):
+    """Keys and ciphertexts through the reference API mirror (seeded, engine-independent).
+
+    The keys come from `seed` alone, so every rank holds the same ones; pair p of the job
+    (its two ciphertexts and its rotation step) comes from the seed sequence (seed, p),
+    so a pair is the same whichever rank draws it.  Returns pairs first_pair ..
+    first_pair + pairs - 1."""
     from vfhe_b200.arith import Ring
     from vfhe_b200.fhe import CKKS_Scheme
     from vfhe_b200.native import use_engine
 
     with use_engine(engine):
         rng = np.random.default_rng(seed)
-        R = Ring(N_DEG, prime_size=PRIME_SIZES, split_degree=1)
+        R = Ring(n, prime_size=prime_sizes, split_degree=1)
         s = CKKS_Scheme(R, scaling_factor=SCALE, special_primes=1)
         key = s.key_gen_uniform_ternary(3.2, rng)
         rlk = s.gen_rlk(key, key, lvl=0, rng=rng)
         gks = {k: s.gen_ksk_automorphism(key, key, s.galois_gen(k), lvl=1, rng=rng) for k in gk_steps}
-        steps = [int(v) for v in rng.choice(gk_steps, pairs)]
-        zs, cts = [], []
-        for _ in range(2 * pairs):
-            z = np.sqrt(rng.random(N_DEG // 2)) * np.exp(2j * np.pi * rng.random(N_DEG // 2))
-            zs.append(z)
-            cts.append(s.encrypt(s.encode(list(z)), key, rng=rng))
+        steps, zs, cts = [], [], []
+        for p in range(first_pair, first_pair + pairs):
+            prng = np.random.default_rng([seed, p])
+            steps.append(int(prng.choice(gk_steps)))
+            for _ in range(2):
+                z = np.sqrt(prng.random(n // 2)) * np.exp(2j * np.pi * prng.random(n // 2))
+                zs.append(z)
+                cts.append(s.encrypt(s.encode(list(z)), key, rng=prng))
         return s, key, rlk, gks, steps, zs, cts
 
 
@@ -801,7 +818,8 @@ def run_cuda_arm(args) -> None:
             if eng.lib.vfhe_cuda_ntt_set_schedule(int(lp), bucket, *sched) != 0:
                 raise SystemExit(f"--ntt-schedule {spec}: refused by the engine")
     PAIRS = args.pairs  # noqa: N806  (the workload's batch; 256 unless profiling a small case)
-    s, key, rlk, gks, rot_steps, zs, cts = build_workload(eng, PAIRS, SEED + rank)
+    share = pair_share(rank, PAIRS)
+    s, key, rlk, gks, rot_steps, zs, cts = build_workload(eng, PAIRS, SEED, first_pair=share.start)
     for c in cts:
         c.to_NTT()
     host1 = np.stack([ciphertext_rows(c) for c in cts[0::2]])
