@@ -219,6 +219,91 @@ def _ref_worker(args) -> dict:
     return {"elapsed": time.perf_counter() - t0, "pairs": pairs * done, "engine": name}
 
 
+def _ref_poly(R, rows):
+    from vfhe_b200.arith import Polynomial
+    from vfhe_b200.arith import repr as prepr
+
+    p = Polynomial(R)
+    p.set_rows(rows)
+    p.rns_mask = R.mask
+    p.repr = prepr.coeff
+    return p
+
+
+def _cpu_ntt_worker(args) -> dict:
+    """One host core: the reference library's forward transform of every limb of one
+    polynomial (polynomial_RNSc_to_RNS, rns_polynomial.c:582-614) at N = 2^logn with
+    `limbs` 50-bit primes, repeated for `seconds` after one warm-up call."""
+    logn, limbs, split, seconds, seed = args
+    from vfhe_b200.arith import Polynomial, Ring
+    from vfhe_b200.native import Engine
+
+    lib, name = _ref_library()
+    eng = Engine(lib)
+    R = Ring(2**logn, prime_size=[50] * limbs, split_degree=split, engine=eng)
+    rng = np.random.default_rng(seed)
+    src = _ref_poly(R, np.stack([rng.integers(0, q, R.N, dtype=np.uint64) for q in R.primes]))
+    out = Polynomial(R)
+    eng.lib.polynomial_RNSc_to_RNS(out.obj, src.obj)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        eng.lib.polynomial_RNSc_to_RNS(out.obj, src.obj)
+        done += 1
+    return {"units": done * limbs, "elapsed": time.perf_counter() - t0, "engine": name}
+
+
+def _cpu_roundtrip_worker(args) -> dict:
+    """One host core: the reference library's NTT -> incomplete product -> INTT chain of
+    one pair at N = 4096, L = 3 (polynomial_RNSc_to_RNS x 2, polynomial_mul_RNS_polynomial,
+    polynomial_RNS_to_RNSc), repeated for `seconds`."""
+    split, seconds, seed = args
+    from vfhe_b200.arith import Polynomial, Ring
+    from vfhe_b200.native import Engine
+
+    lib, name = _ref_library()
+    eng = Engine(lib)
+    R = Ring(4096, prime_size=[50] * 3, split_degree=split, engine=eng)
+    rng = np.random.default_rng(seed)
+    a, b = (_ref_poly(R, np.stack([rng.integers(0, q, R.N, dtype=np.uint64) for q in R.primes])) for _ in range(2))
+    P = [Polynomial(R) for _ in range(3)]
+    rl = eng.lib
+    done, t0 = -1, time.perf_counter()
+    while done < 0 or time.perf_counter() - t0 < seconds:
+        if done == 0:
+            t0 = time.perf_counter()  # the first chain is the warm-up
+        rl.polynomial_RNSc_to_RNS(P[0].obj, a.obj)
+        rl.polynomial_RNSc_to_RNS(P[1].obj, b.obj)
+        rl.polynomial_mul_RNS_polynomial(P[2].obj, P[0].obj, P[1].obj)
+        rl.polynomial_RNS_to_RNSc(P[2].obj, P[2].obj)
+        done += 1
+    return {"units": done, "elapsed": time.perf_counter() - t0, "engine": name}
+
+
+class CpuPool:
+    """Spawned processes, one per host core, for the reference's all-cores figures
+    (spawned, not forked: the parent holds a CUDA context)."""
+
+    def __init__(self):
+        self.cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        self.pool = None
+
+    def rate(self, worker, args: tuple, seed: int) -> dict:
+        """units/s over all cores: every process runs `worker` for the same time budget."""
+        import multiprocessing as mp
+
+        if self.pool is None:
+            self.pool = mp.get_context("spawn").Pool(self.cores)
+        res = self.pool.map(worker, [args + (seed + w,) for w in range(self.cores)])
+        return {"value": sum(r["units"] for r in res) / max(r["elapsed"] for r in res), "cores": self.cores,
+                "engine": res[0]["engine"]}
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.close()
+            self.pool.join()
+            self.pool = None
+
+
 def cpu_baseline(time_budget: float = 15.0) -> dict:
     """Reference library, one core, bounded sample of the same workload (pairs/s)."""
     lib, name = _ref_library()
@@ -295,7 +380,7 @@ def whole_job_rate(units_per_rank: int, world: int, ms: float) -> float:
 
 
 # ----------------------------------------------------------------------------- gpu arm
-def worklist_leg(eng, count: int, reps: int) -> dict:
+def worklist_leg(eng, count: int, reps: int, cpu_budget: float = 0.0) -> dict:
     """Uneven batch: `count` jobs, N in 2^12..2^16, L in 2..24, half NTT->product->INTT
     chains and half key switches, as one persistent work-list launch per run, beside
     the graph of per-pool launches and one call per job."""
@@ -349,6 +434,26 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
     ms_pc = ev0.elapsed_time(ev1) / reps
     exact = all(torch.equal(j.out, o) for j, o in zip(jobs, outs))
     moved = sum(j.bytes_moved() for j in jobs)
+    cpu = None
+    lib, name = _ref_library()
+    if cpu_budget > 0 and lib.exists():
+        # the reference library's one-op-per-call path over the first jobs of the same list,
+        # one host core, each output compared with the GPU work list's
+        from vfhe_b200.native import Engine
+        from vfhe_b200.worklist import run_job_on_engine
+
+        ref = Engine(lib)
+        done, same, t0 = 0, True, time.perf_counter()
+        for j in jobs:
+            got = run_job_on_engine(ref, j)
+            same = same and bool(np.array_equal(got, j.out.cpu().numpy().view(np.uint64).reshape(got.shape)))
+            done += 1
+            if time.perf_counter() - t0 > cpu_budget:
+                break
+        el = time.perf_counter() - t0
+        cpu = {"jobs_per_s": done / el, "cores": 1, "kind": "reference", "bit_exact_vs_work_list": same,
+               "sample": f"the first {done} of the {len(jobs)} jobs, one at a time through the reference's "
+                         f"{name} engine's cdef calls, one thread, {el:.1f} s"}
     res = {
         "jobs": count, "jobs_per_s": count / (ms_wl * 1e-3), "ms_per_run": ms_wl,
         "per_call_jobs_per_s": count / (ms_pc * 1e-3), "per_call_ms": ms_pc, "per_call_calls": calls,
@@ -360,6 +465,8 @@ def worklist_leg(eng, count: int, reps: int) -> dict:
         "algorithmic_gb_per_s": moved / (ms_wl * 1e-3) / 1e9,
         "mix": {"chain": sum(j.kind == "chain" for j in jobs), "keyswitch": sum(j.kind == "keyswitch" for j in jobs)},
     }
+    if cpu is not None:
+        res["cpu_reference"] = cpu
     wl.close()
     del jobs, outs, ws
     torch.cuda.empty_cache()
@@ -588,7 +695,7 @@ def rns_cggi_leg(eng, count: int = 1024, cpu_bootstraps: int = 2) -> dict:
     return res
 
 
-def ntt_round_trip_leg(eng, reps: int = 20, cpu_budget: float = 3.0) -> dict:
+def ntt_round_trip_leg(eng, reps: int = 20, cpu_budget: float = 3.0, pool=None) -> dict:
     """The plain RNS NTT round trip: 64 pairs (a, b) in Z_q[X]/(X^4096 + 1), L = 3 (the
     three largest 50-bit NTT primes of the reference's generator for the split), uniform
     residues; forward NTT of both, the incomplete product with the split twist, inverse
@@ -683,6 +790,12 @@ def ntt_round_trip_leg(eng, reps: int = 20, cpu_budget: float = 3.0) -> dict:
             el = time.perf_counter() - t0
             res[key]["cpu_reference"] = {"pairs_per_s": done / el, "cores": 1, "kind": "reference",
                                          "sample": f"{done} pairs on the reference's {name} engine, one thread"}
+            if pool is not None:
+                allc = pool.rate(_cpu_roundtrip_worker, (split, cpu_budget), SEED + 40)
+                res[key]["cpu_reference_all_cores"] = {
+                    "pairs_per_s": allc["value"], "cores": allc["cores"], "kind": "reference",
+                    "sample": f"one process per host core, {cpu_budget:.0f} s of chains each, the reference's "
+                              f"{allc['engine']} engine"}
         del a, b, out
     del flush
     return res
@@ -1016,10 +1129,25 @@ def run_cuda_arm(args) -> None:
     # the reference's default split for 50-bit primes: four 2^14-point blocks per limb
     ms16s4, limbs16s4 = ntt16_rate(4, False)
     eng.check("bench")
+    # the reference's CPU figures (rank 0 at one GPU only): one core in this process and
+    # all host cores in spawned processes
+    pool = CpuPool() if (world == 1 and not args.no_cpu_baseline and _ref_library()[0].exists()) else None
+    ntt16_cpu = {}
+    if pool is not None:
+        for split, tag in ((1, "split1"), (None, "split4")):
+            one = _cpu_ntt_worker((16, 24, split, 3.0, SEED + 50))
+            allc = pool.rate(_cpu_ntt_worker, (16, 24, split, 3.0), SEED + 51)
+            ntt16_cpu[tag] = {"limbs_per_s_one_core": one["units"] / one["elapsed"],
+                              "limbs_per_s_all_cores": allc["value"], "cores": allc["cores"], "kind": "reference",
+                              "sample": f"polynomial_RNSc_to_RNS of one 24-limb polynomial, repeated for 3 s per "
+                                        f"process, the reference's {one['engine']} engine"}
     encrypt = encrypt_leg(eng, s, key, d1[:, 1].contiguous(), reps=5)
-    round_trip = ntt_round_trip_leg(eng)
+    round_trip = ntt_round_trip_leg(eng, pool=pool)
 
-    uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)))
+    uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)),
+                                                        cpu_budget=10.0 if pool is not None else 0.0)
+    if pool is not None:
+        pool.close()
     serving = None if args.no_serving else serving_leg(eng, args.serving_requests)
     cggi_fft = None if args.no_cggi else cggi_fft_leg(eng, 4096, reps=3, million=not args.no_cggi_million)
     rns_cggi = None if args.no_cggi else rns_cggi_leg(eng)
@@ -1079,9 +1207,11 @@ def run_cuda_arm(args) -> None:
         "clocks": clocks.summary(),
         "decoded_max_error": err,
         "ntt_2p16_L24_split4": {"limbs_per_s": limbs16s4, "polys": NTT16_POLYS, "ms_per_launch": ms16s4,
-                                "frac_hbm": 16 * 2**16 * limbs16s4 / 1e9 / peak},
+                                "frac_hbm": 16 * 2**16 * limbs16s4 / 1e9 / peak,
+                                **({"cpu_reference": ntt16_cpu["split4"]} if "split4" in ntt16_cpu else {})},
         "ntt_2p16_L24": {"limbs_per_s": limbs16, "polys": NTT16_POLYS, "ms_per_launch": ms16,
-                         "frac_hbm": 16 * 2**16 * limbs16 / 1e9 / peak},
+                         "frac_hbm": 16 * 2**16 * limbs16 / 1e9 / peak,
+                         **({"cpu_reference": ntt16_cpu["split1"]} if "split1" in ntt16_cpu else {})},
     }
     if uneven is not None:
         line["uneven_worklist"] = uneven

@@ -41,36 +41,8 @@ def same(p1: Polynomial, p2: Polynomial, rows_only: bool = False) -> None:
 
 
 def job_on_engine(engine, job) -> np.ndarray:
-    """A work-list job recomputed through the cdef surface of `engine` (reference API):
-    chain  = polynomial_RNSc_to_RNS of both operands, polynomial_mul_RNS_polynomial,
-             polynomial_RNS_to_RNSc;
-    keyswitch = mlwe_RNSc_GHS_hybrid_keyswitch of the rank-1 sample with one key."""
-    from vfhe_b200.mlwe import MLWE, MLWE_Scheme, MLWE_Set
+    """A work-list job recomputed through the cdef surface of `engine`
+    (vfhe_b200.worklist.run_job_on_engine)."""
+    from vfhe_b200.worklist import run_job_on_engine
 
-    host = lambda t: t.cpu().numpy().view(np.uint64)  # noqa: E731
-    L = job.L
-    if job.kind == "chain":
-        R = Ring(job.N, prime_size=[50] * L, primes=job.ring.primes[:L], split_degree=job.ring.split_degree,
-                 engine=engine)
-        a = poly_from_rows(R, host(job.a))
-        b = poly_from_rows(R, host(job.b))
-        c = a * b
-        c.to_coeff()
-        return c.rows()
-    R = Ring(job.N, prime_size=[50] * (L + 1), primes=job.ring.primes[: L + 1], split_degree=job.ring.split_degree,
-             engine=engine)
-    s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
-    ct, ksk = host(job.a), host(job.ksk)
-    c = MLWE(s)
-    c.set_component_rows(0, ct[0])
-    c.set_component_rows(1, ct[1])
-    c.repr = repr.coeff
-    comps = []
-    for j in range(L):
-        k = MLWE(s, ring=s.special_rings[0])
-        k.set_component_rows(0, ksk[j][0])
-        k.set_component_rows(1, ksk[j][1])
-        k.repr = repr.ntt
-        comps.append(k)
-    out = s.keyswitch(c, MLWE_Set([comps]))
-    return np.stack([out.component_rows(0), out.component_rows(1)])
+    return run_job_on_engine(engine, job)

@@ -182,3 +182,52 @@ def uneven_jobs(engine: Engine, count: int = 512, seed: int = 3, logn: tuple[int
             ksk = uniform((L, 2, L + 1, n), 2, L + 1)
             jobs.append(Job("keyswitch", R, L, idx, R.prime_indices[L], torch.empty_like(ct), ct, ksk=ksk))
     return jobs
+
+
+def run_job_on_engine(engine: Engine, job: Job) -> np.ndarray:
+    """One job recomputed through the one-op-per-call cdef surface of `engine` (any
+    engine: the cuda engine, or a CPU library exporting the same cdef), as the
+    reference's callers would run it:
+    chain     = polynomial_RNSc_to_RNS of both operands, polynomial_mul_RNS_polynomial,
+                polynomial_RNS_to_RNSc (rns_polynomial.c:311-356, 582-614);
+    keyswitch = mlwe_RNSc_GHS_hybrid_keyswitch of the rank-1 sample with one key
+                (mlwe.c:557-598).
+    Inputs are read from the job's tensors; returns the output rows."""
+    from .arith import Polynomial
+    from .arith import repr as prepr
+    from .mlwe import MLWE, MLWE_Scheme, MLWE_Set
+
+    def host(t):
+        return t.cpu().numpy().view(np.uint64)
+
+    def poly(R, rows):
+        p = Polynomial(R)
+        p.set_rows(rows)
+        p.rns_mask = R.mask
+        p.repr = prepr.coeff
+        return p
+
+    L = job.L
+    if job.kind == "chain":
+        R = Ring(job.N, prime_size=[50] * L, primes=job.ring.primes[:L], split_degree=job.ring.split_degree,
+                 engine=engine)
+        c = poly(R, host(job.a)) * poly(R, host(job.b))
+        c.to_coeff()
+        return c.rows()
+    R = Ring(job.N, prime_size=[50] * (L + 1), primes=job.ring.primes[: L + 1], split_degree=job.ring.split_degree,
+             engine=engine)
+    s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
+    ct, ksk = host(job.a), host(job.ksk)
+    c = MLWE(s)
+    c.set_component_rows(0, ct[0])
+    c.set_component_rows(1, ct[1])
+    c.repr = prepr.coeff
+    comps = []
+    for j in range(L):
+        k = MLWE(s, ring=s.special_rings[0])
+        k.set_component_rows(0, ksk[j][0])
+        k.set_component_rows(1, ksk[j][1])
+        k.repr = prepr.ntt
+        comps.append(k)
+    out = s.keyswitch(c, MLWE_Set([comps]))
+    return np.stack([out.component_rows(0), out.component_rows(1)])
