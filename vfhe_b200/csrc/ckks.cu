@@ -9,7 +9,9 @@
 //   * the digit broadcast (limb j reduced modulo every extended prime) happens in
 //     the load of the forward transform, so the broadcast rows are never stored;
 //   * the special-prime round division, the pass-through additions and the CKKS
-//     rescale (division by the top prime) are one kernel per coefficient;
+//     rescale (division by the top prime) are one kernel per coefficient, which also
+//     runs the accumulators' inverse column pass (k_coldown) where the transform's
+//     schedule allows, so the coefficient-domain accumulators never reach HBM;
 //   * the forward transform at the end of the reference's mlwe_multiply and the
 //     inverse transform at the start of its rescale are both skipped: they are
 //     inverse bijections on canonical residues, so skipping them changes no bit.
