@@ -1052,6 +1052,57 @@ def run_cuda_arm(args) -> None:
     e2e_value_plain = whole_job_rate(PAIRS, world, e2e_ms_plain)
     e2e_ms = e2e_time(True)
     e2e_value = whole_job_rate(PAIRS, world, e2e_ms)
+
+    # the wire format with the sender's packing and the receiver's unpacking on the host
+    # inside the timed region (vfhe_cuda_pack_rows_host / _unpack_rows_host on every host
+    # thread): step i's inputs are packed while the GPU works on step i-1, and step i-1's
+    # results are unpacked into uint64 rows after step i is enqueued.  Host wall clock.
+    host_threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    h1n, h2n = h1.numpy(), h2.numpy()
+    hpk = [(torch.empty_like(h1p).pin_memory(), torch.empty_like(h2p).pin_memory()) for _ in range(2)]
+    res_rows = np.empty(tuple(rot.shape), dtype=np.int64)
+
+    def e2e_hostpack_run(count):
+        for i in range(count):
+            b = i % 2
+            if i >= 2:
+                ev_in[b].synchronize()  # step i-2's copy from these packed buffers is done
+            wf_in.pack_host(h1n, out=hpk[b][0].numpy(), nthreads=host_threads)
+            wf_in.pack_host(h2n, out=hpk[b][1].numpy(), nthreads=host_threads)
+            a1, a2 = din[b]
+            src1, src2 = dinp[b]
+            with torch.cuda.stream(s_in):
+                if i >= 2:
+                    s_in.wait_event(ev_comp[b])
+                src1.copy_(hpk[b][0], non_blocking=True)
+                src2.copy_(hpk[b][1], non_blocking=True)
+                ev_in[b].record(s_in)
+            stream.wait_event(ev_in[b])
+            if i >= 2:
+                stream.wait_event(ev_out[b])
+            wf_in.unpack(src1, a1.shape, out=a1, stream=stream)
+            wf_in.unpack(src2, a2.shape, out=a2, stream=stream)
+            mul.mul_relin_rescale(a1, a2, rlk_t, out=dprod[b], stream=stream)
+            rotb.rotate(dprod[b], gens, keys, out=drot[b], stream=stream)
+            wf_out.pack(drot[b], out=doutp[b], stream=stream)
+            ev_comp[b].record(stream)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_comp[b])
+                houtp[b].copy_(doutp[b], non_blocking=True)
+                ev_out[b].record(s_out)
+            if i >= 1:
+                ev_out[1 - b].synchronize()
+                wf_out.unpack_host(houtp[1 - b].numpy(), res_rows, nthreads=host_threads)
+        ev_out[(count - 1) % 2].synchronize()
+        wf_out.unpack_host(houtp[(count - 1) % 2].numpy(), res_rows, nthreads=host_threads)
+
+    e2e_hostpack_run(2)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_hostpack_run(e2e_steps)
+    barrier()
+    e2e_ms_hostpack = max_over_ranks(1e3 * (time.perf_counter() - t0) / e2e_steps, dist, "cuda")
+    hostpack_ok = bool(np.array_equal(res_rows, drot[(e2e_steps - 1) % 2].cpu().numpy()))
     # the packed transport delivers the same results: compare the last step's output
     hres = torch.empty_like(rot)
     wf_out.unpack(houtp[(e2e_steps - 1) % 2].cuda(), rot.shape, out=hres)
@@ -1198,7 +1249,14 @@ def run_cuda_arm(args) -> None:
                                 "transport": "compact wire format (residues at their primes' bit lengths) as a "
                                              "client would send it: packed by the sender before the timed region, "
                                              "unpacked and packed on the GPU inside the step",
-                                "packed_matches_plain": e2e_packed_ok}},
+                                "packed_matches_plain": e2e_packed_ok},
+                "wire_format_host_packed": {
+                    "value": whole_job_rate(PAIRS, world, e2e_ms_hostpack), "ms_per_step": e2e_ms_hostpack,
+                    "h2d_bytes_per_step": int(h1p.numel() + h2p.numel()),
+                    "d2h_bytes_per_step": int(houtp[0].numel()), "host_threads": host_threads,
+                    "transport": "compact wire format, packed from the uint64 rows and unpacked back into uint64 "
+                                 "rows on the host inside the timed region (host wall clock)",
+                    "unpacked_matches_device": hostpack_ok}},
         "roofline": {"bound": "hbm", "kernel": f"forward FP64 NTT, {kname} (digit transforms, {PAIRS * ne} rows x 2^14)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": MEASURED_TRAFFIC.get((kname, PAIRS * ne)), "launch_ms": ntt_ms,

@@ -399,6 +399,15 @@ int vfhe_cuda_pack_rows(void *d_packed, const uint64_t *d_rows, uint64_t N, cons
                         uint32_t rows_per_item, uint64_t items, void *stream);
 int vfhe_cuda_unpack_rows(uint64_t *d_rows, const void *d_packed, uint64_t N, const uint32_t *bits,
                           uint32_t rows_per_item, uint64_t items, void *stream);
+/* The same format packed and unpacked on the host, for a sender that holds plain uint64
+ * rows (h_rows, h_packed: host memory, pinned or not), on nthreads host threads (0 =
+ * every hardware thread); synchronous, no GPU needed.  Byte for byte what
+ * vfhe_cuda_pack_rows writes and vfhe_cuda_unpack_rows reads.  No counterpart in the
+ * reference. */
+int vfhe_cuda_pack_rows_host(void *h_packed, const uint64_t *h_rows, uint64_t N, const uint32_t *bits,
+                             uint32_t rows_per_item, uint64_t items, uint32_t nthreads);
+int vfhe_cuda_unpack_rows_host(uint64_t *h_rows, const void *h_packed, uint64_t N, const uint32_t *bits,
+                               uint32_t rows_per_item, uint64_t items, uint32_t nthreads);
 
 /* ChaCha20 keystream blocks counter0 .. counter0 + nblocks - 1 for a 256-bit key
  * (8 little-endian words) and a 64-bit nonce, in the original layout (64-bit block

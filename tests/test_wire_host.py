@@ -51,3 +51,30 @@ def test_host_packer_bit_order():
     assert pack_rows_host(rows, [8]).tolist() == [[1, 2, 3, 4, 5, 6, 7, 8]]
     rows = np.array([[[0b101] + [0] * 63]], dtype=np.uint64)
     assert pack_rows_host(rows, [3])[0, 0] == 0b101
+
+
+@pytest.mark.parametrize("bits,N,items,threads", [
+    ([50, 40, 40], 64, 3, 1),
+    ([1, 7, 13, 31, 33, 63, 64, 8], 64, 2, 3),
+    ([37, 41], 128, 5, 0),
+    ([50] + [40] * 8, 1024, 4, 4),  # one ciphertext component of the CKKS benchmark's chain
+])
+def test_native_host_packer_matches_format(lib_engine, bits, N, items, threads):
+    """vfhe_cuda_pack_rows_host / _unpack_rows_host (the sender's and receiver's side on
+    the host) write and read exactly the format the numpy restatement defines, for any
+    thread count, with residues wider than their field masked as the GPU packer does."""
+    from vfhe_b200.batch import WireFormat
+
+    rng = np.random.default_rng(N * items + len(bits))
+    rows = np.stack([np.stack([rng.integers(0, 2**63, N, dtype=np.uint64) for _ in bits]) for _ in range(items)])
+    masked = rows.copy()
+    for r, b in enumerate(bits):
+        if b < 64:
+            masked[:, r] &= np.uint64((1 << b) - 1)
+    wf = WireFormat(N, bits, engine=lib_engine)
+    packed = wf.pack_host(rows, nthreads=threads)
+    assert np.array_equal(packed, pack_rows_host(masked, bits))
+    back = np.empty_like(rows)
+    wf.unpack_host(packed, back, nthreads=threads)
+    assert np.array_equal(back, masked)
+    lib_engine.check("host packer")

@@ -290,6 +290,43 @@ class WireFormat:
             raise EngineError("pack_rows")
         return out
 
+    @staticmethod
+    def _host_ptr(ffi, a):
+        """Address of a contiguous host array (numpy array or CPU tensor)."""
+        if isinstance(a, torch.Tensor):
+            assert not a.is_cuda and a.is_contiguous()
+            return ffi.cast("void*", a.data_ptr())
+        assert a.flags["C_CONTIGUOUS"]
+        return ffi.cast("void*", a.ctypes.data)
+
+    def pack_host(self, rows, out=None, nthreads: int = 0):
+        """The sender's side on the host (vfhe_cuda_pack_rows_host): [B][rows...][N]
+        uint64 / int64 residues in host memory (numpy array or CPU tensor, e.g. pinned)
+        -> [B][item_bytes] uint8 in host memory, on `nthreads` threads (0: all)."""
+        B = rows.shape[0]
+        if out is None:
+            out = np.empty((B, self.item_bytes), dtype=np.uint8)
+        assert out.shape[0] * out.shape[1] == B * self.item_bytes
+        rc = self.lib.vfhe_cuda_pack_rows_host(self._host_ptr(self.ffi, out),
+                                               self.ffi.cast("uint64_t*", self._host_ptr(self.ffi, rows)), self.N,
+                                               self._bits, len(self.bits), B, int(nthreads))
+        if rc != 0:
+            self.engine.check("pack_rows_host")
+            raise EngineError("pack_rows_host")
+        return out
+
+    def unpack_host(self, packed, out, nthreads: int = 0):
+        """The receiver's side on the host (vfhe_cuda_unpack_rows_host): [B][item_bytes]
+        uint8 -> uint64 / int64 residues in `out` ([B][rows...][N], host memory)."""
+        B = packed.shape[0]
+        rc = self.lib.vfhe_cuda_unpack_rows_host(self.ffi.cast("uint64_t*", self._host_ptr(self.ffi, out)),
+                                                 self._host_ptr(self.ffi, packed), self.N, self._bits,
+                                                 len(self.bits), B, int(nthreads))
+        if rc != 0:
+            self.engine.check("unpack_rows_host")
+            raise EngineError("unpack_rows_host")
+        return out
+
     def unpack(self, packed: torch.Tensor, shape: tuple, out: torch.Tensor | None = None,
                stream=None) -> torch.Tensor:
         """[B][item_bytes] uint8 -> int64 residues of ``shape`` ([B][rows...][N])."""

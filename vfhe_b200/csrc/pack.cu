@@ -15,6 +15,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <thread>
+#include <vector>
 
 #include "abi_common.cuh"
 
@@ -98,6 +100,62 @@ bool make_layout(PackLayout& lay, uint64_t N, const uint32_t* bits, uint32_t row
     return true;
 }
 
+// Host form of k_pack for one row: N residues (masked to b bits) into N b / 64 words,
+// least significant bits first (the same stream k_pack writes).
+void pack_row_host(uint64_t* w, const uint64_t* src, uint64_t N, uint32_t b) {
+    const uint64_t mask = b >= 64 ? ~0ULL : ((1ULL << b) - 1);
+    uint64_t acc = 0;
+    uint32_t nb = 0;  // bits of acc in use, always < 64 here
+    for (uint64_t x = 0; x < N; ++x) {
+        const uint64_t v = src[x] & mask;
+        acc |= v << nb;
+        nb += b;
+        if (nb >= 64) {
+            *w++ = acc;
+            nb -= 64;
+            acc = nb ? v >> (b - nb) : 0;  // the bits of v that did not fit
+        }
+    }
+}
+
+// Host form of k_unpack for one row.
+void unpack_row_host(uint64_t* dst, const uint64_t* w, uint64_t N, uint32_t b) {
+    const uint64_t mask = b >= 64 ? ~0ULL : ((1ULL << b) - 1);
+    uint64_t cur = 0;
+    uint32_t avail = 0;  // unread low bits of cur
+    for (uint64_t x = 0; x < N; ++x) {
+        uint64_t v;
+        if (avail >= b) {
+            v = cur & mask;
+            cur = b >= 64 ? 0 : cur >> b;
+            avail -= b;
+        } else {
+            const uint64_t nxt = *w++;
+            v = (cur | (nxt << avail)) & mask;
+            const uint32_t used = b - avail;
+            cur = used >= 64 ? 0 : nxt >> used;
+            avail = 64 - used;
+        }
+        dst[x] = v;
+    }
+}
+
+// Run fn(item, row) over every (item, row) of a layout on nthreads host threads, each
+// taking a contiguous share.
+template <class F>
+void host_rows_parallel(const PackLayout& lay, uint64_t items, uint32_t nthreads, F fn) {
+    const uint64_t units = items * (uint64_t)lay.rows;
+    uint64_t nt = nthreads ? nthreads : std::max(1u, std::thread::hardware_concurrency());
+    nt = std::min<uint64_t>(nt, units);
+    auto work = [&](uint64_t t) {
+        for (uint64_t u = units * t / nt; u < units * (t + 1) / nt; ++u) fn(u / lay.rows, (int)(u % lay.rows));
+    };
+    std::vector<std::thread> pool;
+    for (uint64_t t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+}
+
 dim3 pack_grid(uint64_t per_row, uint64_t rows_total) {
     note_launch();
     uint64_t blocks = (per_row + 255) / 256;
@@ -150,6 +208,40 @@ int vfhe_cuda_unpack_rows(uint64_t* d_rows, const void* d_packed, uint64_t N, co
     k_unpack<<<pack_grid(N, items * rows_per_item), 256, 0, (cudaStream_t)stream>>>(
         d_rows, (const uint64_t*)d_packed, (long long)N, lay);
     return check_cuda(cudaGetLastError(), where) ? 0 : 1;
+}
+
+int vfhe_cuda_pack_rows_host(void* h_packed, const uint64_t* h_rows, uint64_t N, const uint32_t* bits,
+                             uint32_t rows_per_item, uint64_t items, uint32_t nthreads) {
+    const char* where = "vfhe_cuda_pack_rows_host";
+    PackLayout lay;
+    if (!make_layout(lay, N, bits, rows_per_item, where)) return 1;
+    if (!h_packed || !h_rows || items == 0) {
+        set_error(where, "null buffers or no items");
+        return 1;
+    }
+    uint64_t* out = (uint64_t*)h_packed;
+    host_rows_parallel(lay, items, nthreads, [&](uint64_t item, int r) {
+        pack_row_host(out + item * lay.item_words + lay.word_off[r], h_rows + (item * lay.rows + r) * N, N,
+                      lay.bits[r]);
+    });
+    return 0;
+}
+
+int vfhe_cuda_unpack_rows_host(uint64_t* h_rows, const void* h_packed, uint64_t N, const uint32_t* bits,
+                               uint32_t rows_per_item, uint64_t items, uint32_t nthreads) {
+    const char* where = "vfhe_cuda_unpack_rows_host";
+    PackLayout lay;
+    if (!make_layout(lay, N, bits, rows_per_item, where)) return 1;
+    if (!h_packed || !h_rows || items == 0) {
+        set_error(where, "null buffers or no items");
+        return 1;
+    }
+    const uint64_t* in = (const uint64_t*)h_packed;
+    host_rows_parallel(lay, items, nthreads, [&](uint64_t item, int r) {
+        unpack_row_host(h_rows + (item * lay.rows + r) * N, in + item * lay.item_words + lay.word_off[r], N,
+                        lay.bits[r]);
+    });
+    return 0;
 }
 
 }  // extern "C"
