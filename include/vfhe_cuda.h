@@ -272,6 +272,11 @@ void gp25_sub_a_mt(void *p0, uint64_t in_N, uint64_t *a, void *s_sign, uint64_t 
  * Part 2: batched device API (new; no reference counterpart)             *
  * ===================================================================== */
 
+/* An empty batch (batch = 0, or nsrc = 0 for key generation) is a successful no-op
+ * for the batched compute calls below once the pool and limb list check out: nothing
+ * is launched and no workspace is touched (vfhe_cuda_ntt_mul_intt_batch_noalloc keeps
+ * rejecting it, as documented there). */
+
 /* Engine status: 0 when no error has been recorded since the last clear. */
 int vfhe_cuda_status(void);
 const char *vfhe_cuda_last_error(void);

@@ -90,6 +90,22 @@ uint64_t* engine_workspace(size_t bytes, cudaStream_t st) {
     return (uint64_t*)b.p;
 }
 
+// An empty batch: a successful no-op (nothing is launched and no scratch is touched)
+// once the pool and the limb list check out; otherwise the call's usual error.
+int empty_batch(void* ntt, const uint32_t* limbs, uint32_t nlimbs, const char* where) {
+    IncNtt* t = as_ntt(ntt);
+    if (!t || !limbs || nlimbs == 0 || nlimbs > (uint32_t)kMaxLimbs) {
+        set_error(where, "bad pool or limb list");
+        return 1;
+    }
+    for (uint32_t k = 0; k < nlimbs; ++k)
+        if (limbs[k] >= t->pub.l) {
+            set_error(where, "limb index outside the pool");
+            return 1;
+        }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -107,6 +123,7 @@ int vfhe_cuda_ntt_batch(void* ntt, int inverse, uint64_t* d_out, const uint64_t*
 int vfhe_cuda_poly_mul_batch(void* ntt, uint64_t* d_out, const uint64_t* d_a, const uint64_t* d_b,
                              uint64_t batch, const uint32_t* limbs, uint32_t nlimbs, void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_poly_mul_batch");
     IncNtt* t = as_ntt(ntt);
     if (!t || !limbs || nlimbs == 0 || nlimbs > (uint32_t)kMaxLimbs) {
         set_error("vfhe_cuda_poly_mul_batch", "bad pool or limb list");
@@ -134,6 +151,7 @@ int vfhe_cuda_poly_mul_batch(void* ntt, uint64_t* d_out, const uint64_t* d_a, co
 int vfhe_cuda_ntt_mul_intt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_a, const uint64_t* d_b,
                                  uint64_t batch, const uint32_t* limbs, uint32_t nlimbs, void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_ntt_mul_intt_batch");
     IncNtt* t = as_ntt(ntt);
     if (!t) return 1;
     cudaStream_t st = (cudaStream_t)stream_;
@@ -161,6 +179,7 @@ int vfhe_cuda_ckks_mul_relin_rescale_batch(void* ntt, uint64_t* d_out, const uin
                                            uint32_t special, const uint64_t* d_rlk, void* workspace,
                                            void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_ckks_mul_relin_rescale_batch");
     IncNtt* t = as_ntt(ntt);
     cudaStream_t st = (cudaStream_t)stream_;
     uint64_t* ws = (uint64_t*)workspace;
@@ -173,6 +192,7 @@ int vfhe_cuda_rlwe_encrypt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_m
                                  const uint32_t* limbs, uint32_t nlimbs, const uint64_t* d_sk, double sigma,
                                  void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_rlwe_encrypt_batch");
     return rlwe_encrypt(as_ntt(ntt), d_out, d_msg, batch, limbs, nlimbs, d_sk, sigma, (cudaStream_t)stream_);
 }
 
@@ -180,6 +200,7 @@ int vfhe_cuda_gen_ksk_batch(void* ntt, uint64_t* d_out, const uint64_t* d_src, u
                             uint32_t nlimbs, const uint64_t* factors, const uint64_t* d_sk, double sigma,
                             void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (nsrc == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_gen_ksk_batch");
     return rlwe_gen_ksk(as_ntt(ntt), d_out, d_src, nsrc, limbs, nlimbs, factors, d_sk, sigma, (cudaStream_t)stream_);
 }
 
@@ -203,6 +224,7 @@ int vfhe_cuda_ckks_rotate_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct
                                 const uint32_t* limbs, uint32_t nlimbs, uint32_t special, const uint64_t* gens,
                                 const uint64_t* const* d_gks, void* workspace, void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_ckks_rotate_batch");
     IncNtt* t = as_ntt(ntt);
     cudaStream_t st = (cudaStream_t)stream_;
     uint64_t* ws = (uint64_t*)workspace;
@@ -221,6 +243,7 @@ int vfhe_cuda_cggi_bootstrap_batch(void* ntt, uint64_t* d_out_a, uint64_t* d_out
                                    uint32_t nlimbs, uint32_t special, const uint64_t* d_bk, const uint64_t* d_tv,
                                    uint64_t torus_base, void* workspace, void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_cggi_bootstrap_batch");
     IncNtt* t = as_ntt(ntt);
     cudaStream_t st = (cudaStream_t)stream_;
     uint64_t* ws = (uint64_t*)workspace;
@@ -238,6 +261,7 @@ int vfhe_cuda_keyswitch_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct, 
                               const uint32_t* limbs, uint32_t nlimbs, uint32_t special, const uint64_t* d_ksk,
                               void* workspace, void* stream_) {
     if (!vc::ensure_ready()) return 1;
+    if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_keyswitch_batch");
     IncNtt* t = as_ntt(ntt);
     cudaStream_t st = (cudaStream_t)stream_;
     uint64_t* ws = (uint64_t*)workspace;
