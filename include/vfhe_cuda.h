@@ -272,7 +272,11 @@ void gp25_sub_a_mt(void *p0, uint64_t in_N, uint64_t *a, void *s_sign, uint64_t 
  * Part 2: batched device API (new; no reference counterpart)             *
  * ===================================================================== */
 
-/* An empty batch (batch = 0, or nsrc = 0 for key generation) is a successful no-op
+/* The batched CKKS multiply, rotation and key switch take batches of any size: past
+ * 65535 / (2 (nlimbs + 1)) ciphertexts (one pass of their kernels' grids) they run as
+ * consecutive passes on the same stream, sharing one pass's workspace, with the same
+ * residues (a caller-supplied workspace sized for the whole batch also serves).
+ * An empty batch (batch = 0, or nsrc = 0 for key generation) is a successful no-op
  * for the batched compute calls below once the pool and limb list check out: nothing
  * is launched and no workspace is touched (vfhe_cuda_ntt_mul_intt_batch_noalloc keeps
  * rejecting it, as documented there). */

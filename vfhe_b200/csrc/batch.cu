@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -106,6 +107,11 @@ int empty_batch(void* ntt, const uint32_t* limbs, uint32_t nlimbs, const char* w
     return 0;
 }
 
+// Largest batch one pass of the CKKS and key-switch kernels takes: their grids' y
+// dimension (at most 65535) counts at most batch x 2 x (nlimbs + 1) rows.  Larger
+// batches run as consecutive chunks on the same stream, sharing the workspace.
+uint64_t ckks_max_chunk(uint32_t nlimbs) { return 65535 / (2 * ((uint64_t)nlimbs + 1)); }
+
 }  // namespace
 
 extern "C" {
@@ -181,11 +187,21 @@ int vfhe_cuda_ckks_mul_relin_rescale_batch(void* ntt, uint64_t* d_out, const uin
     if (!vc::ensure_ready()) return 1;
     if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_ckks_mul_relin_rescale_batch");
     IncNtt* t = as_ntt(ntt);
+    if (!t || nlimbs < 2) return ckks_mul_relin_rescale(t, d_out, d_ct1, d_ct2, batch, limbs, nlimbs, special, d_rlk,
+                                                        nullptr, (cudaStream_t)stream_);  // records the error
     cudaStream_t st = (cudaStream_t)stream_;
+    const uint64_t chunk = std::min<uint64_t>(batch, ckks_max_chunk(nlimbs));
     uint64_t* ws = (uint64_t*)workspace;
-    if (!ws) ws = engine_workspace(vfhe_cuda_ckks_mul_workspace_bytes(ntt, batch, nlimbs), st);
+    if (!ws) ws = engine_workspace(vfhe_cuda_ckks_mul_workspace_bytes(ntt, chunk, nlimbs), st);
     if (!ws) return 1;
-    return ckks_mul_relin_rescale(t, d_out, d_ct1, d_ct2, batch, limbs, nlimbs, special, d_rlk, ws, st);
+    const uint64_t N = t->pub.N;
+    for (uint64_t b0 = 0; b0 < batch; b0 += chunk) {
+        const uint64_t n = std::min(chunk, batch - b0);
+        const int rc = ckks_mul_relin_rescale(t, d_out + b0 * 2 * (nlimbs - 1) * N, d_ct1 + b0 * 2 * nlimbs * N,
+                                              d_ct2 + b0 * 2 * nlimbs * N, n, limbs, nlimbs, special, d_rlk, ws, st);
+        if (rc) return rc;
+    }
+    return 0;
 }
 
 int vfhe_cuda_rlwe_encrypt_batch(void* ntt, uint64_t* d_out, const uint64_t* d_msg, uint64_t batch,
@@ -226,11 +242,26 @@ int vfhe_cuda_ckks_rotate_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct
     if (!vc::ensure_ready()) return 1;
     if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_ckks_rotate_batch");
     IncNtt* t = as_ntt(ntt);
+    if (!t)
+        return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, gens, d_gks, nullptr,
+                           (cudaStream_t)stream_);  // records the error
+    if (!d_gks) {
+        set_error("vfhe_cuda_ckks_rotate_batch", "no key pointer array");
+        return 1;
+    }
     cudaStream_t st = (cudaStream_t)stream_;
+    const uint64_t chunk = std::min<uint64_t>(batch, ckks_max_chunk(nlimbs));
     uint64_t* ws = (uint64_t*)workspace;
-    if (!ws) ws = engine_workspace(vfhe_cuda_ckks_rotate_workspace_bytes(ntt, batch, nlimbs), st);
+    if (!ws) ws = engine_workspace(vfhe_cuda_ckks_rotate_workspace_bytes(ntt, chunk, nlimbs), st);
     if (!ws) return 1;
-    return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, gens, d_gks, ws, st);
+    const uint64_t N = t->pub.N;
+    for (uint64_t b0 = 0; b0 < batch; b0 += chunk) {
+        const uint64_t n = std::min(chunk, batch - b0);
+        const int rc = ckks_rotate(t, d_out + b0 * 2 * nlimbs * N, d_ct + b0 * 2 * nlimbs * N, n, limbs, nlimbs,
+                                   special, gens ? gens + b0 : nullptr, d_gks + b0, ws, st);
+        if (rc) return rc;
+    }
+    return 0;
 }
 
 uint64_t vfhe_cuda_cggi_workspace_bytes(void* ntt, uint64_t batch, uint32_t n, uint32_t nlimbs) {
@@ -264,11 +295,20 @@ int vfhe_cuda_keyswitch_batch(void* ntt, uint64_t* d_out, const uint64_t* d_ct, 
     if (batch == 0) return empty_batch(ntt, limbs, nlimbs, "vfhe_cuda_keyswitch_batch");
     IncNtt* t = as_ntt(ntt);
     cudaStream_t st = (cudaStream_t)stream_;
+    const uint64_t chunk = std::min<uint64_t>(batch, ckks_max_chunk(nlimbs));
+    std::vector<const uint64_t*> keys(chunk, d_ksk);
+    if (!t) return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, nullptr, keys.data(), nullptr, st);
     uint64_t* ws = (uint64_t*)workspace;
-    if (!ws) ws = engine_workspace(vfhe_cuda_keyswitch_workspace_bytes(ntt, batch, nlimbs), st);
+    if (!ws) ws = engine_workspace(vfhe_cuda_keyswitch_workspace_bytes(ntt, chunk, nlimbs), st);
     if (!ws) return 1;
-    std::vector<const uint64_t*> keys(batch, d_ksk);
-    return ckks_rotate(t, d_out, d_ct, batch, limbs, nlimbs, special, nullptr, keys.data(), ws, st);
+    const uint64_t N = t->pub.N;
+    for (uint64_t b0 = 0; b0 < batch; b0 += chunk) {
+        const uint64_t n = std::min(chunk, batch - b0);
+        const int rc = ckks_rotate(t, d_out + b0 * 2 * nlimbs * N, d_ct + b0 * 2 * nlimbs * N, n, limbs, nlimbs,
+                                   special, nullptr, keys.data(), ws, st);
+        if (rc) return rc;
+    }
+    return 0;
 }
 
 int vfhe_cuda_device_faults(void) {
