@@ -78,3 +78,25 @@ def test_native_host_packer_matches_format(lib_engine, bits, N, items, threads):
     wf.unpack_host(packed, back, nthreads=threads)
     assert np.array_equal(back, masked)
     lib_engine.check("host packer")
+
+
+def test_native_host_packer_refuses_bad_layouts(lib_engine):
+    """The host packer checks its layout and buffers like the GPU one and records an
+    error instead of writing anything."""
+    ffi, lib = lib_engine.ffi, lib_engine.lib
+    rows = np.zeros((1, 1, 64), dtype=np.uint64)
+    out = np.full(64, 7, dtype=np.uint8)
+    pr = ffi.cast("uint64_t*", rows.ctypes.data)
+    po = ffi.cast("void*", out.ctypes.data)
+    for bits, items, dst, src in (([33], 1, po, pr), ([0], 1, po, pr), ([40], 1, ffi.NULL, pr),
+                                  ([40], 1, po, ffi.NULL), ([40], 0, po, pr)):
+        lib.vfhe_cuda_clear_error()
+        b = ffi.new("uint32_t[]", bits)
+        N = 32 if bits == [33] else 64
+        assert lib.vfhe_cuda_pack_rows_host(dst, src, N, b, 1, items, 1) != 0
+        assert lib.vfhe_cuda_status() != 0
+        lib.vfhe_cuda_clear_error()
+        assert lib.vfhe_cuda_unpack_rows_host(ffi.cast("uint64_t*", src) if src != ffi.NULL else ffi.NULL,
+                                              dst, N, b, 1, items, 1) != 0
+        lib.vfhe_cuda_clear_error()
+    assert (out == 7).all()
