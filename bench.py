@@ -801,6 +801,116 @@ def ntt_round_trip_leg(eng, reps: int = 20, cpu_budget: float = 3.0, pool=None) 
     return res
 
 
+def composed_leg(eng, reps: int = 3) -> dict:
+    """The operations built by composing the engine's calls, timed through the cdef on the
+    cuda engine and on the reference's own library (one host core), same inputs:
+    mlwe_trace (mlwe.c:436-444: log2 N automorphism key switches) at N = 4096,
+    mlwe_full_packing_keyswitch (mlwe.c:343-430) of 16 LWEs at N = 1024, and the CKKS
+    rational rescale (ckks.py:150-202) of a ciphertext between levels sharing two primes
+    at N = 4096.  Random residues stand in for keys and ciphertexts (the calls are exact
+    modular arithmetic).  Per call: host-addressable rows in, results readable on return."""
+    from vfhe_b200.arith import Ring, reset_registries
+    from vfhe_b200.arith import repr as prepr
+    from vfhe_b200.fhe import CKKS_Ciphertext, CKKS_Scheme
+    from vfhe_b200.mlwe import LWE, MLWE, MLWE_Scheme, MLWE_Set
+    from vfhe_b200.native import Engine, use_engine
+
+    lib, name = _ref_library()
+    engines = [("cuda", eng)] + ([("reference", Engine(lib))] if lib.exists() else [])
+    rng = np.random.default_rng(SEED + 60)
+
+    def rows(primes, N):
+        return np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in primes])
+
+    def mlwe(s, ring, r0, r1, rep):
+        m = MLWE(s, ring=ring) if ring is not None else MLWE(s, lvl=0)
+        m.set_component_rows(0, r0)
+        m.set_component_rows(1, r1)
+        m.repr = rep
+        return m
+
+    def timed(fn):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return 1e3 * (time.perf_counter() - t0) / reps
+
+    res = {}
+    # trace at N = 4096 (12 automorphism key switches)
+    N, logN = 4096, 12
+    base = Ring(N, prime_size=[50, 50, 50], split_degree=1, engine=eng)
+    primes = base.primes
+    ct = [rows(primes[:2], N) for _ in range(2)]
+    keys = [[[rows(primes, N) for _ in range(2)] for _ in range(2)] for _ in range(logN)]
+    out = {}
+    for tag, e in engines:
+        reset_registries()
+        with use_engine(e):
+            R = Ring(N, prime_size=[50, 50, 50], primes=primes, split_degree=1, engine=e)
+            s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
+            c = mlwe(s, None, ct[0], ct[1], prepr.coeff)
+            sets = [MLWE_Set([[mlwe(s, s.special_rings[0], k[d][0], k[d][1], prepr.ntt) for d in range(2)]])
+                    for k in keys]
+            ksks = MLWE_Set.flatten_array(sets)
+            o = MLWE(s, lvl=0)
+            out[tag] = timed(lambda: R.lib.mlwe_trace(o.obj, c.obj, ksks.obj, 0))
+            e.check("mlwe_trace")
+    res["trace_n4096"] = out
+    # full packing key switch of 16 LWEs at N = 1024
+    N, size = 1024, 16
+    base = Ring(N, prime_size=[50, 50, 50], split_degree=1, engine=eng)
+    primes = base.primes
+    lwe_rows = [(rows(primes[:2], N), [int(rng.integers(0, q)) for q in primes[:2]]) for _ in range(size)]
+    krows = [[rows(primes, N) for _ in range(2)] for _ in range(2 * N)]
+    out = {}
+    for tag, e in engines:
+        reset_registries()
+        with use_engine(e):
+            R = Ring(N, prime_size=[50, 50, 50], primes=primes, split_degree=1, engine=e)
+            s = MLWE_Scheme(R, special_primes=1, module_rank=1, max_lvl=1)
+            lwes = []
+            for a, b in lwe_rows:
+                x = LWE(s.rings[0], n=N)
+                x.set_rows(a, b)
+                lwes.append(x)
+            ksk = MLWE_Set([[mlwe(s, s.special_rings[0], krows[2 * i + d][0], krows[2 * i + d][1], prepr.ntt)
+                             for d in range(2)] for i in range(N)])
+            o = MLWE(s, lvl=0)
+            arr = R.ffi.new("void*[]", [x.obj for x in lwes])
+            out[tag] = timed(lambda: R.lib.mlwe_full_packing_keyswitch(o.obj, arr, size, ksk.obj, 0))
+            e.check("mlwe_full_packing_keyswitch")
+    res["full_packing_keyswitch_16_n1024"] = out
+    # rational rescale between levels sharing two primes, N = 4096
+    N = 4096
+    base = Ring(N, split_degree=1, prime_size=[50, 50, 50, 30, 50], engine=eng)
+    primes = base.primes
+    ct = None
+    out = {}
+    for tag, e in engines:
+        reset_registries()
+        with use_engine(e):
+            Rq = Ring(N, split_degree=1, prime_size=[50, 50, 50, 30, 50], primes=primes, engine=e)
+            sub = lambda *ix: Rq.quotient_ring(mask=sum(1 << Rq.prime_indices[i] for i in ix))  # noqa: E731
+            s = CKKS_Scheme([sub(0, 1, 2), sub(0, 1, 3)], scaling_factor=2**50, special_primes=1,
+                            special_rings=[sub(0, 1, 2, 4), sub(0, 1, 3, 4)])
+            if ct is None:
+                ct = [rows(s.rings[0].primes, N) for _ in range(2)]
+            c = CKKS_Ciphertext(s, lvl=0)
+            c.set_component_rows(0, ct[0])
+            c.set_component_rows(1, ct[1])
+            c.repr = prepr.coeff
+            out[tag] = timed(lambda: s.rational_rescale(c))
+            e.check("rational_rescale")
+    res["rational_rescale_n4096"] = out
+    reset_registries()
+    for v in res.values():
+        v["unit"] = "ms per call"
+        if "reference" in v:
+            v["reference"] = {"ms": v["reference"], "cores": 1, "engine": name}
+    return res
+
+
 def encrypt_leg(eng, s, key, msgs, reps: int = 5, cpu_encryptions: int = 8) -> dict:
     """Batched CKKS encryption (vfhe_cuda_rlwe_encrypt_batch) of the workload's batch of
     coefficient-domain plaintexts at N = 2^14, L = 9, and the reference library's own
@@ -1193,6 +1303,7 @@ def run_cuda_arm(args) -> None:
                               "sample": f"polynomial_RNSc_to_RNS of one 24-limb polynomial, repeated for 3 s per "
                                         f"process, the reference's {one['engine']} engine"}
     encrypt = encrypt_leg(eng, s, key, d1[:, 1].contiguous(), reps=5)
+    composed = composed_leg(eng) if world == 1 else None
     round_trip = ntt_round_trip_leg(eng, pool=pool)
 
     uneven = None if args.no_worklist else worklist_leg(eng, args.worklist_jobs, reps=max(3, min(args.steps, 10)),
@@ -1278,6 +1389,8 @@ def run_cuda_arm(args) -> None:
     if cggi_fft is not None:
         line["cggi_fft_bootstrap"] = cggi_fft
     line["ckks_encrypt"] = encrypt
+    if composed is not None:
+        line["composed_ops"] = composed
     line["ntt_round_trip_n4096_L3"] = round_trip
     if rns_cggi is not None:
         line["cggi16_rns_bootstrap"] = rns_cggi

@@ -9,6 +9,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "abi_common.cuh"
 
 using namespace vc;
@@ -875,6 +878,161 @@ void mgsw_NCMUX(void* out, void* in1, void* in2, void* mgsw, void* ksk, uint64_t
 }
 
 // ------------------------------------------------------------------ packing (composite)
+// pool indices of the extended limbs, passed by value to the digit kernel
+struct PackPrimes {
+    uint32_t p[kMaxLimbs];
+};
+
+// The packing key switch's digits for digits d0 .. d0 + nd - 1, d = i lwe_l + l: row e of
+// digit d is the polynomial whose coefficient k < size is sample k's mask entry i of
+// limb l (M [in_n][lwe_l][size]) reduced modulo extended prime e, zero above `size`
+// (polynomial_RNSc_mod_reduce_lifted of the reference's tmp polynomial).
+__global__ void k_pack_digits(uint64_t* __restrict__ D, const uint64_t* __restrict__ M, long long d0, int nd,
+                              int lwe_l, int size, int ne, const __grid_constant__ PackPrimes lp,
+                              const PrimeInfo* __restrict__ primes, long long N) {
+    const int de = blockIdx.y;  // (digit, extended limb)
+    const int dd = de / ne, e = de - dd * ne;
+    const long long d = d0 + dd;
+    const PrimeInfo& pi = primes[lp.p[e]];
+    const uint64_t* src = M + d * size;  // [i][l] rows of `size` entries, d = i lwe_l + l
+    uint64_t* row = D + ((long long)dd * ne + e) * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x)
+        row[x] = x < size ? reduce64(src[x], pi) : 0;
+    (void)lwe_l;
+    (void)nd;
+}
+
+// Copy rows through a pointer table: rows[r] (N residues) -> dst + r N.
+__global__ void k_gather_rows(uint64_t* __restrict__ dst, const uint64_t* const* __restrict__ rows, long long N) {
+    const uint64_t* src = rows[blockIdx.y];
+    uint64_t* o = dst + (long long)blockIdx.y * N;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N; x += (long long)gridDim.x * blockDim.x)
+        o[x] = src[x];
+}
+
+// mlwe_full_packing_keyswitch's inner product over every (mask entry i, limb l) digit
+// at once: the mask entries are gathered on the host in one pass, the digit rows built,
+// transformed and multiplied into the key on the GPU in a few launches per chunk of
+// digits, instead of a host write of the digit polynomial and a synchronisation per
+// mask entry.  Digits of the target's limbs past the samples' lwe_l are zero and are
+// skipped (they add nothing).  Exact modular arithmetic throughout, so the result is
+// the sequential form's.  Writes -sum into out's a[0] and b rows of the extended limbs
+// and returns true; false (nothing written) where it does not apply: rank other than
+// 1, more than 64 extended limbs, or a failed allocation.
+static bool packing_inner_product_batched(RNS_MLWE o, LWE* lw, RNS_MLWE** K, uint64_t size, uint64_t in_n,
+                                          uint64_t lwe_l, uint64_t extended, const char* where) {
+    // VFHE_CUDA_PACKING_SEQUENTIAL=1: the sequential form below (same residues; tests compare)
+    const char* seq = getenv("VFHE_CUDA_PACKING_SEQUENTIAL");
+    if (seq && atoi(seq) != 0) return false;
+    if (o->r != 1 || K[0][0]->r != 1) return false;
+    IncNtt* t = pool(o);
+    const uint64_t N = o->b->ntt->N;
+    std::vector<uint32_t> ext;
+    for (uint32_t j = 0; j < 64; ++j)
+        if ((extended >> j) & 1) ext.push_back(j);
+    const int ne = (int)ext.size();
+    if (ne == 0 || ne > kMaxLimbs || size > N || in_n == 0 || lwe_l == 0) return false;
+    // the samples' mask entries, M[i][l][k] = sample k's entry i of limb l
+    std::vector<uint64_t> M(in_n * lwe_l * size);
+    for (uint64_t k = 0; k < size; ++k)
+        for (uint64_t l = 0; l < lwe_l; ++l)
+            for (uint64_t i = 0; i < in_n; ++i) M[(i * lwe_l + l) * size + k] = lw[k]->a[l][i];
+    const uint64_t ndig = in_n * lwe_l;
+    // digits per chunk: D and the gathered keys within ~256 MB
+    const uint64_t per_digit = 3ULL * ne * N * sizeof(uint64_t);
+    uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(ndig, (256ULL << 20) / per_digit));
+    chunk = std::min<uint64_t>(chunk, 65535 / (2 * (uint64_t)ne));  // the gather grid's y dimension
+    uint64_t *dM = nullptr, *dD = nullptr, *dK = nullptr, *dacc = nullptr, *dtmp = nullptr, *dptr = nullptr;
+    const uint64_t** drows = nullptr;
+    auto release = [&]() {
+        cudaFree(dM);
+        cudaFree(dD);
+        cudaFree(dK);
+        cudaFree(dacc);
+        cudaFree(dtmp);
+        cudaFree(dptr);
+        cudaFree(drows);
+    };
+    if (cudaMalloc(&dM, M.size() * 8) != cudaSuccess || cudaMalloc(&dD, chunk * ne * N * 8) != cudaSuccess ||
+        cudaMalloc(&dK, chunk * 2 * ne * N * 8) != cudaSuccess || cudaMalloc(&dacc, 2 * ne * N * 8) != cudaSuccess ||
+        cudaMalloc(&dtmp, 2 * ne * N * 8) != cudaSuccess || cudaMalloc(&dptr, 8) != cudaSuccess ||
+        cudaMalloc(&drows, chunk * 2 * ne * sizeof(uint64_t*)) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return false;
+    }
+    cudaStream_t st = stream();
+    bool ok = check_cuda(cudaMemcpy(dM, M.data(), M.size() * 8, cudaMemcpyHostToDevice), where);
+    PackPrimes lp;
+    memset(&lp, 0, sizeof lp);
+    for (int e = 0; e < ne; ++e) lp.p[e] = ext[e];
+    std::vector<const uint64_t*> rows(chunk * 2 * ne);
+    for (uint64_t d0 = 0; ok && d0 < ndig; d0 += chunk) {
+        const int nd = (int)std::min(chunk, ndig - d0);
+        // keys of these digits, [dd][component][e][N]
+        for (int dd = 0; dd < nd; ++dd) {
+            const uint64_t d = d0 + dd, i = d / lwe_l, l = d % lwe_l;
+            RNS_MLWE k = K[i][l];
+            for (int e = 0; e < ne; ++e) {
+                rows[((size_t)dd * 2 + 0) * ne + e] = k->a[0]->coeffs[ext[e]];
+                rows[((size_t)dd * 2 + 1) * ne + e] = k->b->coeffs[ext[e]];
+            }
+        }
+        ok = check_cuda(cudaMemcpyAsync(drows, rows.data(), (size_t)nd * 2 * ne * sizeof(uint64_t*),
+                                        cudaMemcpyHostToDevice, st), where);
+        if (!ok) break;
+        const unsigned gx = (unsigned)std::min<uint64_t>(64, (N + 255) / 256);
+        k_gather_rows<<<dim3(gx, (unsigned)(nd * 2 * ne)), 256, 0, st>>>(dK, drows, (long long)N);
+        k_pack_digits<<<dim3(gx, (unsigned)(nd * ne)), 256, 0, st>>>(dD, dM, (long long)d0, nd, (int)lwe_l, (int)size,
+                                                                     ne, lp, t->d_info, (long long)N);
+        ok = check_cuda(cudaGetLastError(), where);
+        if (!ok) break;
+        RowSet rs;
+        memset(&rs, 0, sizeof rs);
+        for (int e = 0; e < ne; ++e) {
+            rs.in[e] = dD + (size_t)e * N;
+            rs.out[e] = dD + (size_t)e * N;
+            rs.prime[e] = ext[e];
+        }
+        rs.nlimbs = ne;
+        rs.split = (int)t->pub.split_degree;
+        rs.logP = t->logP;
+        rs.batch = nd;
+        rs.batch_stride = (long long)ne * N;
+        rs.in_batch_stride = rs.batch_stride;
+        mark_fp64(rs, t);
+        ok = check_cuda(launch_ntt(rs, t->d_info, false, st), where) &&
+             check_cuda(mac_one_sample(t, d0 ? dtmp : dacc, dD, dK, dptr, ext.data(), nd, ne, st), where);
+        if (ok && d0) {
+            // acc += tmp, row by row (both components)
+            EwSet es = empty_set((long long)N);
+            for (int c = 0; c < 2 && ok; ++c) {
+                for (int e = 0; e < ne; ++e) {
+                    es.out[e] = dacc + ((size_t)c * ne + e) * N;
+                    es.a[e] = dacc + ((size_t)c * ne + e) * N;
+                    es.b[e] = dtmp + ((size_t)c * ne + e) * N;
+                    es.prime[e] = ext[e];
+                }
+                es.nlimbs = ne;
+                ok = check_cuda(launch_ew(EW_ADD, es, t->d_info, st), where);
+            }
+        }
+        // the host rewrites `rows` for the next chunk only after this chunk's copy of it
+        if (ok && d0 + chunk < ndig) ok = check_cuda(cudaStreamSynchronize(st), where);
+    }
+    if (ok) {
+        for (int e = 0; e < ne && ok; ++e) {
+            ok = check_cuda(cudaMemcpyAsync(o->a[0]->coeffs[ext[e]], dacc + (size_t)e * N, N * 8,
+                                            cudaMemcpyDeviceToDevice, st), where) &&
+                 check_cuda(cudaMemcpyAsync(o->b->coeffs[ext[e]], dacc + ((size_t)ne + e) * N, N * 8,
+                                            cudaMemcpyDeviceToDevice, st), where);
+        }
+    }
+    check_cuda(cudaStreamSynchronize(st), where);
+    release();
+    return ok;
+}
+
 // Packing of `size` LWE samples into one MLWE (mlwe_full_packing_keyswitch, mlwe.c:343-430):
 // out = sum over mask coefficients i of -(the polynomial of the samples' i-th mask
 // entries, one coefficient per sample) lifted per limb and times ksk[i][limb], computed
@@ -914,7 +1072,8 @@ void mlwe_full_packing_keyswitch(void* out, void* in, uint64_t size, void* ksk, 
     void* tmp_red = polynomial_new_RNS_polynomial(N, extended, t);
     void* tmp_rns = polynomial_new_RNS_polynomial(N, extended, t);
     RNS_Polynomial tp = (RNS_Polynomial)tmp;
-    for (uint64_t i = 0; i < in_n; ++i) {
+    const bool batched = packing_inner_product_batched(o, lw, K, size, in_n, lwe_l, extended, vc_where_);
+    for (uint64_t i = 0; i < in_n && !batched; ++i) {
         vc::sync(vc_where_);  // the rows are written from the host below
         for (uint64_t j : active) memset(tp->coeffs[j], 0, N * sizeof(uint64_t));
         for (uint64_t limb = 0; limb < lwe_l; ++limb)

@@ -1095,6 +1095,20 @@ int acc_inverse_moddown(IncNtt* t, uint64_t* out, uint64_t* acc, uint64_t B, con
 }
 }  // namespace
 
+int mac_one_sample(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* keys, uint64_t* keyptr,
+                   const uint32_t* ext, int nd, int ne, cudaStream_t st) {
+    LimbPrimes lpe;
+    memset(&lpe, 0, sizeof lpe);
+    for (int i = 0; i < ne; ++i) lpe.p[i] = ext[i];
+    const uint64_t kp = (uint64_t)(uintptr_t)keys;
+    const int e = upload_small(keyptr, &kp, 1, st);
+    if (e) return e;
+    const bool aligned = (reinterpret_cast<uintptr_t>(keys) & 15) == 0;
+    launch_mac(t, acc, D, (const uint64_t* const*)keyptr, nullptr, lpe, nd, ne, (long long)t->pub.N, 1, st, aligned,
+               nullptr, nullptr, 0);
+    return (int)cudaGetLastError();
+}
+
 int ckks_mul_relin_rescale(IncNtt* t, uint64_t* out, const uint64_t* ct1, const uint64_t* ct2, uint64_t B,
                            const uint32_t* limbs, uint32_t L, uint32_t special, const uint64_t* rlk,
                            uint64_t* ws, cudaStream_t st) {

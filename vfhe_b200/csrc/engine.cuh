@@ -171,6 +171,13 @@ int launch_chain(IncNtt* t, uint64_t* out, const uint64_t* a, const uint64_t* b,
 // Shared-memory attributes of the chain kernels, set once outside any stream capture.
 int prepare_chain_kernels();
 
+// The packing key switch's inner product for one sample over nd digits (ckks.cu):
+// acc [2][ne][N] = -sum_d D_d (*) K_d, D [nd][ne][N] and keys [nd][2][ne][N] contiguous,
+// NTT domain, (*) the ring's incomplete product; ext: the ne limbs' pool indices;
+// keyptr: device scratch for one pointer.
+int mac_one_sample(IncNtt* t, uint64_t* acc, const uint64_t* D, const uint64_t* keys, uint64_t* keyptr,
+                   const uint32_t* ext, int nd, int ne, cudaStream_t st);
+
 // Galois permutation x -> x^gen (rns_polynomial.c:996-1035).
 int launch_permute(const EwSet& set, uint64_t N, int split, uint64_t gen, const PrimeInfo* d_primes,
                    cudaStream_t st);
