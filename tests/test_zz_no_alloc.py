@@ -65,3 +65,41 @@ def test_noalloc_rejects_oversized_batches(cuda):
     assert rc != 0
     assert "static scratch" in ffi.string(cuda.lib.vfhe_cuda_last_error()).decode()
     cuda.lib.vfhe_cuda_clear_error()
+
+
+def test_noalloc_call_captures_into_a_cuda_graph(cuda):
+    """The property the entry point exists for: after one warm call, a call captured by
+    stream capture (global mode, where a cudaMalloc, cudaFree or synchronisation
+    invalidates the capture) records and replays, and the replay's output equals the
+    allocating entry's."""
+    import torch
+
+    from vfhe_b200.arith import Ring
+    from vfhe_b200.batch import to_device
+
+    N, batch = 4096, 16
+    ring = Ring(N, prime_size=[50, 50, 50], split_degree=None, engine=cuda)
+    rng = np.random.default_rng(5)
+    a = np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in ring.primes]) for _ in range(batch)])
+    b = np.stack([np.stack([rng.integers(0, q, N, dtype=np.uint64) for q in ring.primes]) for _ in range(batch)])
+    ta, tb = to_device(a), to_device(b)
+    ref = _run(cuda, "vfhe_cuda_ntt_mul_intt_batch", ring, ta, tb)
+    _run(cuda, "vfhe_cuda_ntt_mul_intt_batch_noalloc", ring, ta, tb)  # warm: kernel attributes, scratch address
+
+    ffi = cuda.ffi
+    out = torch.zeros_like(ta)
+    limbs = ffi.new("uint32_t[]", ring.prime_indices)
+    p = lambda t: ffi.cast("uint64_t*", t.data_ptr())  # noqa: E731
+    g = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.graph(g):
+        st = ffi.cast("void*", torch.cuda.current_stream().cuda_stream)
+        rcs.append(cuda.lib.vfhe_cuda_ntt_mul_intt_batch_noalloc(ring.NTT, p(out), p(ta), p(tb), batch, limbs,
+                                                                ring.ell, st))
+    assert rcs == [0], ffi.string(cuda.lib.vfhe_cuda_last_error()).decode()
+    torch.cuda.synchronize()
+    assert not out.any()  # captured, not run
+    g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), ref)
+    del g
