@@ -811,12 +811,26 @@ int strided_transform(IncNtt* t, uint64_t* data, uint64_t count, long long strid
 
 // ---- batched RLWE encryption (mlwe_RNSc_sample, modules/mlwe/c/src/mlwe.c:190-241)
 //
-// out [B][2][L][N]: the a rows are drawn uniform directly in the NTT domain (the
-// transform is a bijection, so that is the same distribution as the reference's
-// coefficient-domain draw followed by a transform) and the b rows receive the rounded
-// Gaussian integer of each coefficient reduced into every limb
-// (polynomial_gen_gaussian_RNSc_polynomial, rns_polynomial.c:255-271).  ChaCha20
-// blocks: Gaussian g0 + b ceil(N/4) + j, uniform u0 + (b L + i) ceil(N/4) + j.
+// Four rounded Gaussians of width sigma from ChaCha20 block `ctr` of the Gaussian stream
+// (Box-Muller on two 53-bit uniforms each, rounded: generate_normal_random and
+// polynomial_gen_gaussian_RNSc_polynomial, misc_tp.c:26-33, rns_polynomial.c:255-271).
+__device__ __forceinline__ void gaussian4(const PrngKey& key, uint64_t ctr, double sigma, int64_t ev[4]) {
+    uint32_t blk[16];
+    chacha20_block(key, ctr, kStreamGaussian, blk);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        ev[k] = (int64_t)llrint(sigma * sqrt(-2.0 * log(unit_open_low(block_u64(blk, 2 * k)))) *
+                                cospi(2.0 * unit_closed_low(block_u64(blk, 2 * k + 1))));
+}
+
+// out [B][2][L][N]: the a rows are drawn uniform (polynomial_gen_random_RNSc_polynomial,
+// rns_polynomial.c:242-253) and, with E, the b rows receive the rounded Gaussian integer
+// of each coefficient reduced into every limb (polynomial_gen_gaussian_RNSc_polynomial,
+// rns_polynomial.c:255-271).  ChaCha20 blocks: Gaussian g0 + b ceil(N/4) + j, uniform
+// u0 + (b L + i) ceil(N/4) + j.  Uniform residues are uniform in either domain (the
+// transform is a bijection), so the same draw serves as a's coefficients or as its
+// transform.
+template <bool E>
 __global__ void k_encrypt_sample(uint64_t* __restrict__ out, const __grid_constant__ LimbPrimes lp,
                                  const PrimeInfo* __restrict__ primes, int L, long long N, double sigma,
                                  const __grid_constant__ PrngKey key, uint64_t g0, uint64_t u0) {
@@ -827,12 +841,8 @@ __global__ void k_encrypt_sample(uint64_t* __restrict__ out, const __grid_consta
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per;
          j += (long long)gridDim.x * blockDim.x) {
         uint32_t blk[16];
-        chacha20_block(key, g0 + (uint64_t)(b * per + j), kStreamGaussian, blk);
         int64_t ev[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            ev[k] = (int64_t)llrint(sigma * sqrt(-2.0 * log(unit_open_low(block_u64(blk, 2 * k)))) *
-                                    cospi(2.0 * unit_closed_low(block_u64(blk, 2 * k + 1))));
+        if (E) gaussian4(key, g0 + (uint64_t)(b * per + j), sigma, ev);
         for (int i = 0; i < L; ++i) {
             const PrimeInfo& pi = primes[lp.p[i]];
             chacha20_block(key, u0 + (uint64_t)((b * L + i) * per + j), kStreamUniform, blk);
@@ -841,7 +851,7 @@ __global__ void k_encrypt_sample(uint64_t* __restrict__ out, const __grid_consta
                 const long long x = 4 * j + k;
                 if (x >= N) break;
                 a[(long long)i * N + x] = uniform_mod(block_u64(blk, 2 * k), block_u64(blk, 2 * k + 1), pi.q);
-                e[(long long)i * N + x] = reduce_signed(ev[k], pi);
+                if (E) e[(long long)i * N + x] = reduce_signed(ev[k], pi);
             }
         }
     }
@@ -849,7 +859,10 @@ __global__ void k_encrypt_sample(uint64_t* __restrict__ out, const __grid_consta
 
 // b = e + s a in the NTT domain: the ring's incomplete product over S blocks of P
 // slots (rns_polynomial.c:358-396), with the key broadcast to every ciphertext.
-template <int S>
+// NOISE: b <- b + a s, with a in the a rows and b holding the transformed noise.
+// Otherwise b <- b s in place, with b holding a's transform: each thread reads the S
+// residues of its position x in every block before it writes them.
+template <int S, bool NOISE>
 __global__ void k_encrypt_combine(uint64_t* __restrict__ out, const uint64_t* __restrict__ sk,
                                   const __grid_constant__ LimbPrimes lp, const PrimeInfo* __restrict__ primes, int L,
                                   long long N) {
@@ -858,8 +871,8 @@ __global__ void k_encrypt_combine(uint64_t* __restrict__ out, const uint64_t* __
     const PrimeInfo pi = primes[lp.p[i]];
     const uint64_t q = pi.q;
     const long long P = N / S;
-    const uint64_t* a = out + (b * 2 * L + i) * N;
     uint64_t* eb = out + (b * 2 * L + L + i) * N;
+    const uint64_t* a = NOISE ? out + (b * 2 * L + i) * N : eb;
     const uint64_t* s = sk + (long long)i * N;
     const ulonglong2* tw = reinterpret_cast<const ulonglong2*>(pi.twist);
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < P;
@@ -882,23 +895,37 @@ __global__ void k_encrypt_combine(uint64_t* __restrict__ out, const uint64_t* __
                 const ulonglong2 w = tw[x];
                 acc = add_mod(acc, shoup(wrap, w.x, w.y, q), q);
             }
-            eb[o * P + x] = add_mod(eb[o * P + x], acc, q);
+            eb[o * P + x] = NOISE ? add_mod(eb[o * P + x], acc, q) : acc;
         }
     }
 }
 
-// b += m (coefficient domain); msg: [B][L][N].
-__global__ void k_encrypt_add_msg(uint64_t* __restrict__ out, const uint64_t* __restrict__ msg,
-                                  const __grid_constant__ LimbPrimes lp, const PrimeInfo* __restrict__ primes, int L,
-                                  long long N) {
-    const long long b = blockIdx.y / L;
-    const int i = blockIdx.y - (int)(b * L);
-    const uint64_t q = primes[lp.p[i]].q;
-    uint64_t* eb = out + (b * 2 * L + L + i) * N;
-    const uint64_t* m = msg + (b * L + i) * N;
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < N;
-         x += (long long)gridDim.x * blockDim.x)
-        eb[x] = add_mod(eb[x], m[x], q);
+// b <- b + e + m in the coefficient domain: the four rounded Gaussians of block j
+// (the same stream positions k_encrypt_sample<true> uses) reduced into every limb, and
+// the message rows when given.
+__global__ void k_encrypt_noise_msg(uint64_t* __restrict__ out, const uint64_t* __restrict__ msg,
+                                    const __grid_constant__ LimbPrimes lp, const PrimeInfo* __restrict__ primes, int L,
+                                    long long N, double sigma, const __grid_constant__ PrngKey key, uint64_t g0) {
+    const long long b = blockIdx.y;
+    const long long per = (N + 3) / 4;
+    uint64_t* eb = out + (b * 2 * L + L) * N;
+    const uint64_t* m = msg ? msg + b * L * N : nullptr;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per;
+         j += (long long)gridDim.x * blockDim.x) {
+        int64_t ev[4];
+        gaussian4(key, g0 + (uint64_t)(b * per + j), sigma, ev);
+        for (int i = 0; i < L; ++i) {
+            const PrimeInfo& pi = primes[lp.p[i]];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const long long x = 4 * j + k;
+                if (x >= N) break;
+                uint64_t v = add_mod(eb[(long long)i * N + x], reduce_signed(ev[k], pi), pi.q);
+                if (m) v = add_mod(v, m[(long long)i * N + x], pi.q);
+                eb[(long long)i * N + x] = v;
+            }
+        }
+    }
 }
 
 // Gadget messages of a key-switching key, added in the NTT domain: digit d = j L + i of
@@ -1275,6 +1302,19 @@ int ckks_rotate(IncNtt* t, uint64_t* out, const uint64_t* ct, uint64_t B, const 
 
 namespace {
 // ntt_out: leave both components in the NTT domain (msg must then be null).
+template <bool NOISE>
+int launch_encrypt_combine(const IncNtt* t, dim3 g, uint64_t* out, const uint64_t* sk, const LimbPrimes& lp, int nl,
+                           long long N, cudaStream_t st) {
+    switch (t->pub.split_degree) {
+        case 1: k_encrypt_combine<1, NOISE><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        case 2: k_encrypt_combine<2, NOISE><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        case 4: k_encrypt_combine<4, NOISE><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        case 8: k_encrypt_combine<8, NOISE><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+        default: k_encrypt_combine<16, NOISE><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
+    }
+    return (int)cudaGetLastError();
+}
+
 int rlwe_encrypt_impl(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B, const uint32_t* limbs, uint32_t L,
                       const uint64_t* sk, double sigma, bool ntt_out, const char* where, cudaStream_t st) {
     if (!t || !limbs || L == 0 || L > (uint32_t)kMaxLimbs || !out || !sk || B == 0 || B > 65535 / L ||
@@ -1295,14 +1335,12 @@ int rlwe_encrypt_impl(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B,
     const uint64_t per = (uint64_t)((N + 3) / 4);
     const uint64_t g0 = prng_advance(B * per * (1 + (uint64_t)L));
     const uint64_t u0 = g0 + B * per;
-    k_encrypt_sample<<<grid_xy((long long)per, (long long)B), 256, 0, st>>>(out, lp, t->d_info, nl, N, sigma,
-                                                                            prng_key(), g0, u0);
-    if (!check_cuda(cudaGetLastError(), where)) return 1;
-    // forward transforms of the noise rows (b components)
+    const dim3 gs = grid_xy((long long)per, (long long)B);
+    // rows: a component (limb i) at b 2L N + i N, b component at b 2L N + (L + i) N
     RowSet rs;
     memset(&rs, 0, sizeof rs);
     for (int i = 0; i < nl; ++i) {
-        rs.in[i] = out + ((long long)nl + i) * N;
+        rs.in[i] = out + ((long long)(ntt_out ? nl : 0) + i) * N;
         rs.out[i] = out + ((long long)nl + i) * N;
         rs.prime[i] = limbs[i];
     }
@@ -1313,24 +1351,26 @@ int rlwe_encrypt_impl(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B,
     rs.batch_stride = 2LL * nl * N;
     rs.in_batch_stride = rs.batch_stride;
     mark_fp64(rs, t);
-    if (!check_cuda(launch_ntt(rs, t->d_info, false, st), where)) return 1;
     const dim3 g = grid_xy(N / (long long)t->pub.split_degree, (long long)B * nl);
-    switch (t->pub.split_degree) {
-        case 1: k_encrypt_combine<1><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
-        case 2: k_encrypt_combine<2><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
-        case 4: k_encrypt_combine<4><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
-        case 8: k_encrypt_combine<8><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
-        default: k_encrypt_combine<16><<<g, 256, 0, st>>>(out, sk, lp, t->d_info, nl, N); break;
-    }
-    if (!check_cuda(cudaGetLastError(), where)) return 1;
-    // a was drawn in the NTT domain: a key wants both components there already
-    if (ntt_out) return 0;
-    // both components back to the coefficient domain
-    if (!check_cuda(blocks_transform(t, out, 2 * B, limbs, nl, true, st), where)) return 1;
-    if (msg) {
-        k_encrypt_add_msg<<<grid_xy(N, (long long)B * nl), 256, 0, st>>>(out, msg, lp, t->d_info, nl, N);
+    if (ntt_out) {
+        // keys stay in the NTT domain: a drawn there, the noise transformed, b = e + a s
+        k_encrypt_sample<true><<<gs, 256, 0, st>>>(out, lp, t->d_info, nl, N, sigma, prng_key(), g0, u0);
         if (!check_cuda(cudaGetLastError(), where)) return 1;
+        if (!check_cuda(launch_ntt(rs, t->d_info, false, st), where)) return 1;
+        if (!check_cuda(launch_encrypt_combine<true>(t, g, out, sk, lp, nl, N, st), where)) return 1;
+        return 0;
     }
+    // ciphertexts in the coefficient domain: a drawn as coefficients, then
+    // b = INTT(NTT(a) s) + e + m, two transforms of B L rows where the reference's
+    // order (transform e and a, multiply, inverse-transform a and b) takes four
+    k_encrypt_sample<false><<<gs, 256, 0, st>>>(out, lp, t->d_info, nl, N, sigma, prng_key(), g0, u0);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
+    if (!check_cuda(launch_ntt(rs, t->d_info, false, st), where)) return 1;  // b rows <- NTT(a)
+    if (!check_cuda(launch_encrypt_combine<false>(t, g, out, sk, lp, nl, N, st), where)) return 1;
+    for (int i = 0; i < nl; ++i) rs.in[i] = rs.out[i];
+    if (!check_cuda(launch_ntt(rs, t->d_info, true, st), where)) return 1;
+    k_encrypt_noise_msg<<<gs, 256, 0, st>>>(out, msg, lp, t->d_info, nl, N, sigma, prng_key(), g0);
+    if (!check_cuda(cudaGetLastError(), where)) return 1;
     return 0;
 }
 
