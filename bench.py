@@ -924,11 +924,13 @@ def encrypt_leg(eng, s, key, msgs, reps: int = 5, cpu_encryptions: int = 8) -> d
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    profile_range(None, "encrypt", True)
     e0.record(stream)
     for _ in range(reps):
         enc.encrypt(key, msgs, out=out)
     e1.record(stream)
     torch.cuda.synchronize()
+    profile_range(None, "encrypt", False)
     ms = e0.elapsed_time(e1) / reps
     B = msgs.shape[0]
     res = {"workload": f"{B} ciphertexts, N=2^14, L=9, ternary key, sigma 3.2, ChaCha20 randomness",
@@ -1422,7 +1424,7 @@ def main() -> None:
                     help="override the tuned transform schedule of every row-count class of 2^LOGP-point rows "
                          "(vfhe_cuda_ntt_set_schedule), e.g. 14:10,2,-2 for the dataflow launch")
     ap.add_argument("--profile-leg", default="ckks", choices=["ckks", "digits", "ntt16", "cggi_fft", "cggi_rns", "worklist", "worklist_graph",
-                             "roundtrip", "roundtrip_split1"],
+                             "roundtrip", "roundtrip_split1", "encrypt"],
                     help="leg whose timed region is the profiler capture range (ncu --profile-from-start off)")
     args = ap.parse_args()
     global PROFILE_LEG

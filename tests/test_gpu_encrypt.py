@@ -68,7 +68,7 @@ def _noise(oracle_engine, R, key, out, msgs):
     return np.stack(es)
 
 
-@pytest.mark.parametrize("N,n_mid,split", [(2**12, 3, 1), (2**12, 2, 2), (2**13, 1, 4)])
+@pytest.mark.parametrize("N,n_mid,split", [(2**12, 3, 1), (2**12, 2, 2), (2**13, 1, 4), (2**12, 1, 8), (2**13, 1, 16)])
 def test_encryptions_decrypt_to_message_plus_small_noise(cuda, oracle_engine, N, n_mid, split):
     import torch
 
