@@ -82,6 +82,16 @@ VC_HD uint64_t uniform_mod(uint64_t lo, uint64_t hi, uint64_t q) {
     return (uint64_t)(t >> 64);
 }
 
+// Lemire's multiply-shift with rejection ("Fast random integer generation in an
+// interval", ACM TOMACS 29(1), 2019): for a uniform 64-bit r and m = r q, hi(m) is
+// exactly uniform on [0, q) once the draws with lo(m) < 2^64 mod q (`thresh`) are
+// rejected; a draw is rejected with probability below q / 2^64.  Returns acceptance.
+VC_HD bool uniform_mod64(uint64_t r, uint64_t q, uint64_t thresh, uint64_t& out) {
+    const unsigned __int128 m = (unsigned __int128)r * q;
+    out = (uint64_t)(m >> 64);
+    return (uint64_t)m >= thresh;
+}
+
 // Uniform double in (0, 1] and [0, 1) from 53 bits of a 64-bit word.
 VC_HD double unit_open_low(uint64_t r) { return ((double)(r >> 11) + 1.0) * (1.0 / 9007199254740992.0); }
 VC_HD double unit_closed_low(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
@@ -92,6 +102,7 @@ enum PrngStream : uint64_t {
     kStreamGaussian = 2,
     kStreamInteger = 3,
     kStreamTernary = 4,
+    kStreamUniformRedraw = 5,  // replacements for rejected uniform_mod64 draws
 };
 
 }  // namespace vc

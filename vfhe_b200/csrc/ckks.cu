@@ -826,31 +826,59 @@ __device__ __forceinline__ void gaussian4(const PrngKey& key, uint64_t ctr, doub
 // out [B][2][L][N]: the a rows are drawn uniform (polynomial_gen_random_RNSc_polynomial,
 // rns_polynomial.c:242-253) and, with E, the b rows receive the rounded Gaussian integer
 // of each coefficient reduced into every limb (polynomial_gen_gaussian_RNSc_polynomial,
-// rns_polynomial.c:255-271).  ChaCha20 blocks: Gaussian g0 + b ceil(N/4) + j, uniform
-// u0 + (b L + i) ceil(N/4) + j.  Uniform residues are uniform in either domain (the
+// rns_polynomial.c:255-271).  Uniform residues are uniform in either domain (the
 // transform is a bijection), so the same draw serves as a's coefficients or as its
-// transform.
+// transform.  The reference reduces one 64-bit word per residue with a small bias;
+// here the reduction is exact (uniform_mod64 with redraws).
+//
+// Replacement for a rejected uniform_mod64 draw: the first accepted of the eight 64-bit
+// words of redraw-stream block `ctr`.  If all eight are rejected (probability below
+// 2^-112 for the primes here) the first draw's hi(r q), `first`, which is in [0, q), is
+// kept.  Out of line, so that the common path keeps its draws in registers.
+__device__ __noinline__ uint64_t uniform_redraw(const PrngKey& key, uint64_t ctr, uint64_t q, uint64_t thresh,
+                                                uint64_t first) {
+    uint32_t blk[16];
+    chacha20_block(key, ctr, kStreamUniformRedraw, blk);
+    for (int w = 0; w < 8; ++w) {
+        uint64_t r;
+        if (uniform_mod64(block_u64(blk, w), q, thresh, r)) return r;
+    }
+    return first;
+}
+
+// ChaCha20 blocks: Gaussian g0 + b ceil(N/4) + c for coefficients 4c..4c+3 (the layout
+// k_encrypt_noise_msg reads), uniform u0 + (b L + i) ceil(N/8) + j for coefficients
+// 8j..8j+7 of limb i (one 64-bit word each), and the redraw of coefficient 8j + k at
+// counter u0 + 8 ((b L + i) ceil(N/8) + j) + k of the redraw stream.
 template <bool E>
 __global__ void k_encrypt_sample(uint64_t* __restrict__ out, const __grid_constant__ LimbPrimes lp,
                                  const PrimeInfo* __restrict__ primes, int L, long long N, double sigma,
                                  const __grid_constant__ PrngKey key, uint64_t g0, uint64_t u0) {
     const long long b = blockIdx.y;
-    const long long per = (N + 3) / 4;
+    const long long per4 = (N + 3) / 4, per8 = (N + 7) / 8;
     uint64_t* a = out + b * 2 * L * N;
     uint64_t* e = a + (long long)L * N;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < per8;
          j += (long long)gridDim.x * blockDim.x) {
-        uint32_t blk[16];
-        int64_t ev[4];
-        if (E) gaussian4(key, g0 + (uint64_t)(b * per + j), sigma, ev);
+        int64_t ev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (E) {
+            gaussian4(key, g0 + (uint64_t)(b * per4 + 2 * j), sigma, ev);
+            if (2 * j + 1 < per4) gaussian4(key, g0 + (uint64_t)(b * per4 + 2 * j + 1), sigma, ev + 4);
+        }
         for (int i = 0; i < L; ++i) {
             const PrimeInfo& pi = primes[lp.p[i]];
-            chacha20_block(key, u0 + (uint64_t)((b * L + i) * per + j), kStreamUniform, blk);
+            const uint64_t thresh = reduce64((uint64_t)0 - pi.q, pi);  // 2^64 mod q
+            const uint64_t idx = (uint64_t)((b * L + i) * per8 + j);
+            uint32_t blk[16];
+            chacha20_block(key, u0 + idx, kStreamUniform, blk);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const long long x = 4 * j + k;
+            for (int k = 0; k < 8; ++k) {
+                const long long x = 8 * j + k;
                 if (x >= N) break;
-                a[(long long)i * N + x] = uniform_mod(block_u64(blk, 2 * k), block_u64(blk, 2 * k + 1), pi.q);
+                uint64_t v;
+                if (!uniform_mod64(block_u64(blk, k), pi.q, thresh, v))
+                    v = uniform_redraw(key, u0 + 8 * idx + (uint64_t)k, pi.q, thresh, v);
+                a[(long long)i * N + x] = v;
                 if (E) e[(long long)i * N + x] = reduce_signed(ev[k], pi);
             }
         }
@@ -874,6 +902,31 @@ __global__ void k_encrypt_combine(uint64_t* __restrict__ out, const uint64_t* __
     uint64_t* eb = out + (b * 2 * L + L + i) * N;
     const uint64_t* a = NOISE ? out + (b * 2 * L + i) * N : eb;
     const uint64_t* s = sk + (long long)i * N;
+    if (S == 1 && pi.fp64 && (N & 1) == 0 &&
+        ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(eb) | reinterpret_cast<uintptr_t>(s)) & 15) ==
+            0) {
+        // exact FP64 products (canonical operands below 2^50, uncentred multiplier s with
+        // fl(s qinv) as its quotient estimate: |a s - n q| < q), two residues per thread
+        const double qd = pi.qd, qinv = pi.qinv;
+        for (long long x = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x); x < N;
+             x += 2 * (long long)gridDim.x * blockDim.x) {
+            const ulonglong2 ua = *reinterpret_cast<const ulonglong2*>(a + x);
+            const ulonglong2 us = __ldg(reinterpret_cast<const ulonglong2*>(s + x));
+            const double s0 = f_from_u64(us.x), s1 = f_from_u64(us.y);
+            double t0 = f_mulmod(f_from_u64(ua.x), s0, __dmul_rn(s0, qinv), qd);
+            double t1 = f_mulmod(f_from_u64(ua.y), s1, __dmul_rn(s1, qinv), qd);
+            if (NOISE) {
+                const ulonglong2 ue = *reinterpret_cast<const ulonglong2*>(eb + x);
+                t0 = __dadd_rn(t0, f_from_u64(ue.x));
+                t1 = __dadd_rn(t1, f_from_u64(ue.y));
+            }
+            ulonglong2 r;
+            r.x = f_to_canonical(t0, qd, qinv, pi.q);
+            r.y = f_to_canonical(t1, qd, qinv, pi.q);
+            *reinterpret_cast<ulonglong2*>(eb + x) = r;
+        }
+        return;
+    }
     const ulonglong2* tw = reinterpret_cast<const ulonglong2*>(pi.twist);
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < P;
          x += (long long)gridDim.x * blockDim.x) {
@@ -1332,10 +1385,13 @@ int rlwe_encrypt_impl(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B,
     LimbPrimes lp;
     memset(&lp, 0, sizeof lp);
     for (int i = 0; i < nl; ++i) lp.p[i] = limbs[i];
-    const uint64_t per = (uint64_t)((N + 3) / 4);
-    const uint64_t g0 = prng_advance(B * per * (1 + (uint64_t)L));
-    const uint64_t u0 = g0 + B * per;
-    const dim3 gs = grid_xy((long long)per, (long long)B);
+    const uint64_t per4 = (uint64_t)((N + 3) / 4), per8 = (uint64_t)((N + 7) / 8);
+    // counters: the Gaussian blocks, then the uniform blocks and their redraws (two streams
+    // over the same range)
+    const uint64_t g0 = prng_advance(B * per4 + B * L * per8 * 8);
+    const uint64_t u0 = g0 + B * per4;
+    const dim3 gs = grid_xy((long long)per8, (long long)B);   // k_encrypt_sample: 8 coefficients a thread
+    const dim3 gn = grid_xy((long long)per4, (long long)B);   // k_encrypt_noise_msg: 4 a thread
     // rows: a component (limb i) at b 2L N + i N, b component at b 2L N + (L + i) N
     RowSet rs;
     memset(&rs, 0, sizeof rs);
@@ -1369,7 +1425,7 @@ int rlwe_encrypt_impl(IncNtt* t, uint64_t* out, const uint64_t* msg, uint64_t B,
     if (!check_cuda(launch_encrypt_combine<false>(t, g, out, sk, lp, nl, N, st), where)) return 1;
     for (int i = 0; i < nl; ++i) rs.in[i] = rs.out[i];
     if (!check_cuda(launch_ntt(rs, t->d_info, true, st), where)) return 1;
-    k_encrypt_noise_msg<<<gs, 256, 0, st>>>(out, msg, lp, t->d_info, nl, N, sigma, prng_key(), g0);
+    k_encrypt_noise_msg<<<gn, 256, 0, st>>>(out, msg, lp, t->d_info, nl, N, sigma, prng_key(), g0);
     if (!check_cuda(cudaGetLastError(), where)) return 1;
     return 0;
 }
