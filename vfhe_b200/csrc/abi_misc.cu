@@ -106,7 +106,8 @@ void* init_base_conversion_params(void* ntt, uint64_t in_mask, uint64_t out_mask
     std::vector<uint64_t> srcp(bc->D.begin(), bc->D.end());
     tab.insert(tab.end(), srcp.begin(), srcp.end());
     if (!VC_CHECK(cudaMalloc(&bc->d_tab, tab.size() * 8)) ||
-        !VC_CHECK(cudaMemcpy(bc->d_tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice))) {
+        !VC_CHECK(cudaMemcpy(bc->d_tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice)) ||
+        !VC_CHECK(cudaStreamSynchronize(0))) {  // the upload has landed before engine-stream kernels read it
         delete bc;
         return nullptr;
     }

@@ -962,7 +962,8 @@ static bool packing_inner_product_batched(RNS_MLWE o, LWE* lw, RNS_MLWE** K, uin
         return false;
     }
     cudaStream_t st = stream();
-    bool ok = check_cuda(cudaMemcpy(dM, M.data(), M.size() * 8, cudaMemcpyHostToDevice), where);
+    // on the engine stream, so that the digit kernels below are ordered after it
+    bool ok = check_cuda(cudaMemcpyAsync(dM, M.data(), M.size() * 8, cudaMemcpyHostToDevice, st), where);
     PackPrimes lp;
     memset(&lp, 0, sizeof lp);
     for (int e = 0; e < ne; ++e) lp.p[e] = ext[e];

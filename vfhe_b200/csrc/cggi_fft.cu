@@ -75,7 +75,8 @@ const FourierTables* fourier_tables(int N) {
     if (cudaMalloc(&t.d_tw, sizeof(double2) * M) != cudaSuccess ||
         cudaMalloc(&t.d_twist, sizeof(double2) * M) != cudaSuccess ||
         cudaMemcpy(t.d_tw, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(t.d_twist, twist.data(), sizeof(double2) * M, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(t.d_twist, twist.data(), sizeof(double2) * M, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess)  // the uploads have landed before other streams read them
         return nullptr;
     g_ft.push_back(t);
     return &g_ft.back();

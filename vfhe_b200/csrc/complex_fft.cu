@@ -163,7 +163,8 @@ RouTable* load_rous(const double* re, const double* im, uint64_t size, const cha
     t->size = size;
     if (cudaMalloc(&t->d_re, size * 8) != cudaSuccess || cudaMalloc(&t->d_im, size * 8) != cudaSuccess ||
         cudaMemcpy(t->d_re, re, size * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(t->d_im, im, size * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(t->d_im, im, size * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess) {  // the uploads have landed before engine-stream kernels read them
         cudaFree(t->d_re);
         cudaFree(t->d_im);
         delete t;

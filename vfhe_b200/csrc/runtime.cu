@@ -430,8 +430,13 @@ bool upload_prime_info(IncNtt* t) {
         t->d_info = d;
         t->d_info_cap = cap;
     }
-    return check_cuda(cudaMemcpy(t->d_info, t->info.data(), n * sizeof(PrimeInfo), cudaMemcpyHostToDevice),
-                      "prime info upload");
+    if (!check_cuda(cudaMemcpy(t->d_info, t->info.data(), n * sizeof(PrimeInfo), cudaMemcpyHostToDevice),
+                    "prime info upload"))
+        return false;
+    // the last of a pool's uploads (tables of every added prime, then this one):
+    // a pageable upload on the legacy stream may return before its DMA lands, and the
+    // kernels that read it run on non-blocking streams: wait for the legacy stream
+    return check_cuda(cudaStreamSynchronize(0), "prime info upload");
 }
 
 static bool add_primes(IncNtt* t, const uint64_t* primes, uint64_t count) {

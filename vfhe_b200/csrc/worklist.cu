@@ -620,6 +620,9 @@ int compile(WorkList& w) {
                                                        cudaMemcpyHostToDevice), kWhere)))
             return 1;
     }
+    // a pageable upload on the legacy stream may return before its DMA lands, and the
+    // kernels that read it run on non-blocking streams: wait for the legacy stream
+    if (!check_cuda(cudaStreamSynchronize(0), kWhere)) return 1;
 
     if (persist) {
         // the group plans and the barrier words sit at the end of the buffer
@@ -669,6 +672,7 @@ int compile(WorkList& w) {
         int nb = 0;
         int err = (int)cudaMemcpy(d_plans, plans.data(), plans.size() * sizeof(WlGroupPlan), cudaMemcpyHostToDevice);
         if (!err) err = (int)cudaMemset(d_bar, 0, 256);
+        if (!err) err = (int)cudaStreamSynchronize(0);  // the plans and barrier words are in place
         int nbp[3] = {0, 0, 0};
         if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp[0], k_wl_persistent<0>, kWlPThreads, kWlPSmem);
         if (!err) err = (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbp[1], k_wl_persistent<1>, kWlPThreads, kWlPSmem);
