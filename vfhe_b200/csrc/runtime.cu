@@ -147,15 +147,16 @@ void device_free(void* p) { cache_free(device_cache(), p); }
 // every prefetch off.
 void prefetch_to_device(const void* p, size_t bytes) {
     if (!p || bytes == 0) return;
-    static int enabled = -1;
-    static size_t min_bytes = 0;
-    if (enabled < 0) {
+    struct Policy {
+        bool enabled;
+        size_t min_bytes;
+    };
+    static const Policy policy = [] {  // read once; a function-local static initialises thread-safely
         const char* s = getenv("VFHE_CUDA_PREFETCH");
         const char* m = getenv("VFHE_CUDA_PREFETCH_MIN_BYTES");
-        min_bytes = m ? (size_t)strtoull(m, nullptr, 10) : ((size_t)2 << 20);
-        enabled = (s == nullptr || atoi(s) != 0) ? 1 : 0;
-    }
-    if (!enabled || bytes < min_bytes) return;
+        return Policy{s == nullptr || atoi(s) != 0, m ? (size_t)strtoull(m, nullptr, 10) : ((size_t)2 << 20)};
+    }();
+    if (!policy.enabled || bytes < policy.min_bytes) return;
     cudaMemPrefetchAsync(p, bytes, ctx().device, ctx().stream);
     cudaGetLastError();  // a refused prefetch only costs speed
 }
