@@ -90,3 +90,21 @@ def test_sums_of_products_and_residues_stay_exact(q):
         assert f_to_canonical(d1, qd, qinv, q) == (a1 * b2 + b1 * a2) % q
         t = dadd(f_mulmod(float(a2), fa1, qa1, qd), float(e))
         assert f_to_canonical(t, qd, qinv, q) == (a1 * a2 + e) % q
+
+
+@pytest.mark.parametrize("q", [(1 << 50) - 27, (1 << 49) + 1, (1 << 40) - 87])
+def test_centred_twiddle_with_lazy_input(q):
+    """The butterflies' case: a centred twiddle |w| <= q/2 with wq = fl(w / q) (the
+    tables' quotient, a correctly rounded division) and a lazily reduced input
+    |y| < 2^52 give |t| <= 3q/4 with t = y w mod q."""
+    rng = np.random.default_rng(11)
+    qd = float(q)
+    ws = [0, 1, -1, q // 2, -(q // 2)] + [int(v) - q // 2 for v in rng.integers(0, q, 20, dtype=np.uint64)]
+    ys = [0, 1, -1, (1 << 52) - 1, -((1 << 52) - 1)] + [int(v) for v in rng.integers(-(1 << 52) + 1, 1 << 52, 40)]
+    for w in ws:
+        fw = float(w)
+        wq = _rn(Fraction(w, q))
+        for y in ys:
+            t = f_mulmod(float(y), fw, wq, qd)
+            assert t == int(t) and abs(t) <= 0.75 * q, (y, w)
+            assert (int(t) - y * w) % q == 0, (y, w)
