@@ -191,13 +191,31 @@ def _ref_library() -> tuple[Path, str]:
     return ROOT / "oracle" / "_ref" / f"libvfhe_ref_{name}.so", name
 
 
+def _cpu_library() -> tuple[Path, str, str]:
+    """(library, engine name, kind) of the CPU implementation that the reference arm and
+    the one-core baseline time: the reference's own library compiled from its sources
+    (oracle/_ref, kind "reference"), else the oracle's C restatement of the same path
+    (kind "port"), compiled here if needed."""
+    lib, name = _ref_library()
+    if lib.exists():
+        return lib, name, "reference"
+    port = ROOT / "oracle" / "_build" / "libvfhe_oracle.so"
+    src = ROOT / "oracle" / "vfhe_oracle.c"
+    if not port.exists() or port.stat().st_mtime < src.stat().st_mtime:
+        port.parent.mkdir(exist_ok=True)
+        subprocess.run(["gcc", "-O2", "-std=gnu11", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(port),
+                        str(src), "-lm"], check=True)
+    return port, "oracle", "port"
+
+
 def _ref_worker(args) -> dict:
-    """One host core: reference library, a bounded number of pairs, warmup + timed steps."""
+    """One host core: the CPU implementation (_cpu_library), a bounded number of pairs,
+    warmup + timed steps."""
     pairs, warmup, steps, seed, time_budget = args
     from vfhe_b200.native import Engine
 
-    lib, name = _ref_library()
-    eng = Engine(lib)
+    lib, name, kind = _cpu_library()
+    eng = Engine(lib, name if kind == "port" else None)
     s, key, rlk, gks, rot, zs, cts = build_workload(eng, pairs, seed, gk_steps=sorted(set(STEPS_SET[:2])))
 
     def one_step():
@@ -305,24 +323,19 @@ class CpuPool:
 
 
 def cpu_baseline(time_budget: float = 15.0) -> dict:
-    """Reference library, one core, bounded sample of the same workload (pairs/s)."""
-    lib, name = _ref_library()
-    if not lib.exists():
-        return {"value": None, "unit": "pairs/s", "cores": 1, "kind": "reference",
-                "sample": "unavailable: oracle/_ref not built"}
+    """The CPU implementation (_cpu_library), one core, bounded sample of the same
+    workload (pairs/s)."""
+    lib, name, kind = _cpu_library()
     r = _ref_worker((1, 1, 100000, SEED + 7, time_budget))
-    return {"value": r["pairs"] / r["elapsed"], "unit": "pairs/s", "cores": 1, "kind": "reference",
-            "sample": f"{r['pairs']} pairs of the same workload on the reference's {name} engine, "
-                      f"one thread, {r['elapsed']:.1f} s"}
+    what = f"the reference's {name} engine" if kind == "reference" else "the oracle port"
+    return {"value": r["pairs"] / r["elapsed"], "unit": "pairs/s", "cores": 1, "kind": kind,
+            "sample": f"{r['pairs']} pairs of the same workload on {what}, one thread, {r['elapsed']:.1f} s"}
 
 
 def run_reference_arm(args) -> None:
     import multiprocessing as mp
 
-    lib, name = _ref_library()
-    if not lib.exists():
-        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/build_ref.sh)"}))
-        return
+    lib, name, kind = _cpu_library()
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     workers = max(1, min(cores, 96))
     ctx = mp.get_context("spawn")
@@ -337,8 +350,9 @@ def run_reference_arm(args) -> None:
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (RNS residues < 2^50)",
         "data": "synthetic (seeded)", "config": dict(CONFIG, pairs_per_step=workers),
-        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": workers, "kind": "reference",
-                         "sample": f"{workers} processes x 1 pair per step on the reference's {name} engine"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": workers, "kind": kind,
+                         "sample": f"{workers} processes x 1 pair per step on "
+                                   + (f"the reference's {name} engine" if kind == "reference" else "the oracle port")},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
