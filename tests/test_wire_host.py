@@ -100,3 +100,26 @@ def test_native_host_packer_refuses_bad_layouts(lib_engine):
                                               dst, N, b, 1, items, 1) != 0
         lib.vfhe_cuda_clear_error()
     assert (out == 7).all()
+
+
+def test_native_host_packer_every_fixed_width(lib_engine):
+    """Every field width the host packer has a fixed-width form for (24..62), and its
+    neighbours on either side that take the general loop, against the numpy restatement:
+    several periods of each width, several items, one and four threads."""
+    from vfhe_b200.batch import WireFormat
+
+    rng = np.random.default_rng(23)
+    N = 256  # a multiple of every width's period (64 / gcd(64, b) divides 64)
+    for b in range(22, 65):
+        bits = [b, b]
+        rows = np.stack([np.stack([rng.integers(0, 2**64 - 1, N, dtype=np.uint64, endpoint=True) for _ in bits])
+                         for _ in range(3)])
+        masked = rows & np.uint64((1 << b) - 1) if b < 64 else rows.copy()
+        wf = WireFormat(N, bits, engine=lib_engine)
+        for threads in (1, 4):
+            packed = wf.pack_host(rows, nthreads=threads)
+            assert np.array_equal(packed, pack_rows_host(masked, bits)), (b, threads)
+            back = np.empty_like(rows)
+            wf.unpack_host(packed, back, nthreads=threads)
+            assert np.array_equal(back, masked), (b, threads)
+    lib_engine.check("host packer")

@@ -15,7 +15,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
+#include <numeric>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "abi_common.cuh"
@@ -140,6 +143,92 @@ void unpack_row_host(uint64_t* dst, const uint64_t* w, uint64_t N, uint32_t b) {
     }
 }
 
+// The same two transforms for one field width B fixed at compile time.  A row falls into
+// periods of G = 64 / gcd(64, B) residues that fill W = B G / 64 words exactly (N B being
+// a multiple of 64 makes N a multiple of G).  Within a period every word is an OR of the
+// at most ceil(64 / B) + 1 residues that overlap it, at constant shifts, and every
+// residue comes from at most two words, so neither direction carries a bit counter from
+// one residue to the next.  Same bits as pack_row_host / unpack_row_host.
+template <int B, int J, int POS>
+inline uint64_t fixed_tail_bits(const uint64_t* v) {
+    if constexpr (POS >= 64) {
+        return 0;
+    } else {
+        return (v[J] << POS) | fixed_tail_bits<B, J + 1, POS + B>(v);
+    }
+}
+template <int B, int K>
+inline uint64_t fixed_word(const uint64_t* v) {
+    constexpr int i0 = 64 * K / B, s0 = 64 * K % B;  // first residue overlapping word K
+    return (v[i0] >> s0) | fixed_tail_bits<B, i0 + 1, B - s0>(v);
+}
+template <int B, int... K>
+inline void fixed_pack_period(uint64_t* o, const uint64_t* v, std::integer_sequence<int, K...>) {
+    ((o[K] = fixed_word<B, K>(v)), ...);
+}
+template <int B, int X>
+inline uint64_t fixed_value(const uint64_t* w) {
+    constexpr uint64_t mask = B >= 64 ? ~0ULL : ((1ULL << B) - 1);
+    constexpr int k0 = X * B / 64, off = X * B % 64;
+    if constexpr (off + B <= 64) {
+        return (w[k0] >> off) & mask;
+    } else {
+        return ((w[k0] >> off) | (w[k0 + 1] << (64 - off))) & mask;
+    }
+}
+template <int B, int... X>
+inline void fixed_unpack_period(uint64_t* d, const uint64_t* w, std::integer_sequence<int, X...>) {
+    ((d[X] = fixed_value<B, X>(w)), ...);
+}
+template <int B>
+struct FixedPeriod {
+    static constexpr int G = 64 / std::gcd(64, B);
+    static constexpr int W = B * G / 64;
+};
+template <int B>
+void pack_row_fixed(uint64_t* w, const uint64_t* src, uint64_t N) {
+    constexpr int G = FixedPeriod<B>::G, W = FixedPeriod<B>::W;
+    constexpr uint64_t mask = B >= 64 ? ~0ULL : ((1ULL << B) - 1);
+    const uint64_t periods = N / G;
+    for (uint64_t p = 0; p < periods; ++p) {
+        uint64_t v[G];
+        for (int j = 0; j < G; ++j) v[j] = src[p * G + j] & mask;
+        fixed_pack_period<B>(w + p * W, v, std::make_integer_sequence<int, W>{});
+    }
+    if (periods * G < N) pack_row_host(w + periods * W, src + periods * G, N - periods * G, B);
+}
+template <int B>
+void unpack_row_fixed(uint64_t* dst, const uint64_t* w, uint64_t N) {
+    constexpr int G = FixedPeriod<B>::G, W = FixedPeriod<B>::W;
+    const uint64_t periods = N / G;
+    for (uint64_t p = 0; p < periods; ++p)
+        fixed_unpack_period<B>(dst + p * G, w + p * W, std::make_integer_sequence<int, G>{});
+    if (periods * G < N) unpack_row_host(dst + periods * G, w + periods * W, N - periods * G, B);
+}
+
+// Fixed-width forms for the widths of the engine's primes; other widths use the loops above.
+constexpr int kFixedLo = 24, kFixedHi = 62;
+using PackRowFn = void (*)(uint64_t*, const uint64_t*, uint64_t);
+template <int... I>
+constexpr std::array<PackRowFn, sizeof...(I)> fixed_pack_table(std::integer_sequence<int, I...>) {
+    return {{&pack_row_fixed<kFixedLo + I>...}};
+}
+template <int... I>
+constexpr std::array<PackRowFn, sizeof...(I)> fixed_unpack_table(std::integer_sequence<int, I...>) {
+    return {{&unpack_row_fixed<kFixedLo + I>...}};
+}
+constexpr auto kPackFixed = fixed_pack_table(std::make_integer_sequence<int, kFixedHi - kFixedLo + 1>{});
+constexpr auto kUnpackFixed = fixed_unpack_table(std::make_integer_sequence<int, kFixedHi - kFixedLo + 1>{});
+
+void pack_row_best(uint64_t* w, const uint64_t* src, uint64_t N, uint32_t b) {
+    if (b >= (uint32_t)kFixedLo && b <= (uint32_t)kFixedHi) return kPackFixed[b - kFixedLo](w, src, N);
+    pack_row_host(w, src, N, b);
+}
+void unpack_row_best(uint64_t* dst, const uint64_t* w, uint64_t N, uint32_t b) {
+    if (b >= (uint32_t)kFixedLo && b <= (uint32_t)kFixedHi) return kUnpackFixed[b - kFixedLo](dst, w, N);
+    unpack_row_host(dst, w, N, b);
+}
+
 // Run fn(item, row) over every (item, row) of a layout on nthreads host threads, each
 // taking a contiguous share.
 template <class F>
@@ -221,7 +310,7 @@ int vfhe_cuda_pack_rows_host(void* h_packed, const uint64_t* h_rows, uint64_t N,
     }
     uint64_t* out = (uint64_t*)h_packed;
     host_rows_parallel(lay, items, nthreads, [&](uint64_t item, int r) {
-        pack_row_host(out + item * lay.item_words + lay.word_off[r], h_rows + (item * lay.rows + r) * N, N,
+        pack_row_best(out + item * lay.item_words + lay.word_off[r], h_rows + (item * lay.rows + r) * N, N,
                       lay.bits[r]);
     });
     return 0;
@@ -238,7 +327,7 @@ int vfhe_cuda_unpack_rows_host(uint64_t* h_rows, const void* h_packed, uint64_t 
     }
     const uint64_t* in = (const uint64_t*)h_packed;
     host_rows_parallel(lay, items, nthreads, [&](uint64_t item, int r) {
-        unpack_row_host(h_rows + (item * lay.rows + r) * N, in + item * lay.item_words + lay.word_off[r], N,
+        unpack_row_best(h_rows + (item * lay.rows + r) * N, in + item * lay.item_words + lay.word_off[r], N,
                         lay.bits[r]);
     });
     return 0;
